@@ -1,0 +1,415 @@
+#!/usr/bin/env python
+"""SA+ISA+LCP build throughput on B200 (Gsym/s), one JSON line.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload plain100m|plain4m|batched]
+
+A step is one complete build of the workload: seed sort, doubling rounds,
+ISA, PHI LCP and packing.  ``value`` uses a device-resident text and device
+output planes and the device time of each build (CUDA events recorded by the
+library on its own stream, first to last); L2 is flushed (256 MiB write)
+between steps.  ``e2e`` is the same build through the C ABI with pinned host
+buffers, host<->device copies included.  With N > 1 (torchrun) every rank
+builds its own replica (no collective: the path does not shard) and the
+slowest rank's time counts.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "SA+LCP build Gsym/s on 1 B200 (batched vs plain, bit-exact); % of HBM peak"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="plain100m",
+                    choices=["plain100m", "plain4m", "batched"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        data = json.loads(path.read_text())
+        return float(data["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# Workloads
+# ---------------------------------------------------------------------------
+def workload(name: str):
+    from sufkit_b200 import synth
+    if name == "plain4m":
+        ref = synth.plain_4mbp()
+        desc = ("plain 4 Mbp build: 4 contigs (1.5/1.2/0.8/0.5 Mbp), uniform ACGT, "
+                "0.1% N runs; Fast profile SA+ISA+raw LCP32, 32-bit storage")
+        return [ref.logical_text()], desc
+    if name == "batched":
+        refs = synth.uneven_collection(count=64)
+        desc = ("batched uneven collection sample: 64 bacterial-like references "
+                "(log-normal, median 4 Mbp), SA+raw LCP32 per reference, one batch")
+        return [r.logical_text() for r in refs], desc
+    ref = synth.repeat_rich_100mbp()
+    desc = ("repeat-rich 100 Mbp plain build: 24 contigs, GC 41%, 25% interspersed "
+            "repeats (500 families, 5-15% divergence), 3% tandem repeats, 0.5% N runs; "
+            "Fast profile SA+ISA+raw LCP32, 32-bit construction and storage")
+    return [ref.logical_text()], desc
+
+
+# ---------------------------------------------------------------------------
+# Clock sampling during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, sm_max, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                sm_max.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(sm_max) if sm_max else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# Algorithmic-byte model of one build (per-unit figures in DESIGN.md)
+# ---------------------------------------------------------------------------
+def build_bytes(text: np.ndarray, sa: np.ndarray, isa: np.ndarray, lcp: np.ndarray,
+                w_sa: int = 4, w_isa: int = 4, w_lcp: int = 4, seed: int = 21) -> int:
+    n = int(text.size)
+    W = 4 if n - 1 <= 0xFFFFFFFF else 8
+    lcp64 = lcp.astype(np.int64)
+    nxt = np.append(lcp64[1:], 0)
+    row = isa.astype(np.int64)
+    m = np.maximum(lcp64[row], nxt[row])
+    rounds_bytes = 0
+    k = 1
+    while True:
+        a_k = int(np.count_nonzero(m >= seed * (1 << (k - 1))))
+        if a_k == 0:
+            break
+        rounds_bytes += 8 * W * a_k
+        k += 1
+    plcp = np.empty(n, np.int64)
+    plcp[sa.astype(np.int64)] = lcp64
+    prev = np.concatenate([[0], np.maximum(plcp[:-1] - 1, 0)])
+    compares = int(np.sum(plcp - prev + 1))
+    b = n * (1 + 2 * (8 + W) + W)
+    b += rounds_bytes
+    b += n * (W + w_isa)
+    b += n * 6 * W + 2 * compares
+    b += n * (W + w_sa)
+    b += n * w_lcp
+    return int(b)
+
+
+def load_traffic(kernel: str):
+    """ncu DRAM bytes per algorithmic byte for `kernel` from profiles/, if any."""
+    path = ROOT / "profiles" / "traffic.json"
+    if not path.exists():
+        return None
+    data = json.loads(path.read_text())
+    return data.get(kernel)
+
+
+# ---------------------------------------------------------------------------
+# Reference arm and CPU baseline (the reference's own CPU build path)
+# ---------------------------------------------------------------------------
+def cpu_reference_step(text: np.ndarray, threads: int) -> float:
+    import oracle
+    t0 = time.perf_counter()
+    oracle.ref_adapter(text, 64, threads)
+    return time.perf_counter() - t0
+
+
+def cpu_sample(texts: list[np.ndarray], symbols: int) -> np.ndarray:
+    """A bounded prefix of the workload, re-terminated with the sentinel."""
+    body = texts[0][: max(1, symbols - 1)]
+    return np.concatenate([body[body != 0], np.zeros(1, np.uint8)])
+
+
+def run_reference(args, texts, desc):
+    import oracle
+    if oracle.ref() is None:
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/libsufref.so was not built"}))
+        return
+    threads = os.cpu_count() or 1
+    sample = cpu_sample(texts, 20_000_000)
+    for _ in range(args.warmup):
+        cpu_reference_step(sample, threads)
+    times = [cpu_reference_step(sample, threads) for _ in range(args.steps)]
+    sec = sum(times) / len(times)
+    value = sample.size / sec / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Gsym/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+        "config": {"workload": desc, "symbols_per_step": int(sample.size)},
+        "cpu_baseline": {"value": value, "unit": "Gsym/s", "cores": threads,
+                         "kind": "reference",
+                         "sample": f"first {sample.size} symbols of the workload text; "
+                                   "libdivsufsort64 + ISA + Kasai LCP through "
+                                   "detail::BuildDivsufsort64 (threads=%d)" % threads},
+        "e2e": {"value": value, "unit": "Gsym/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# Our arm
+# ---------------------------------------------------------------------------
+def main():
+    args = parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    texts, desc = workload(args.workload)
+
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args, texts, desc)
+        return
+
+    import torch
+    import sufkit_b200 as sg
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    ctx = sg.Context(local)
+    lcp_enc = sg.LcpEncoding.RAW32
+    isa_bits = 0 if args.workload == "batched" else 32
+
+    # Device-resident inputs and outputs.
+    n_total = sum(int(t.size) for t in texts)
+    d_texts = [torch.from_numpy(t).to(dev) for t in texts]
+    d_out = [{"sa_low": torch.empty(t.size, dtype=torch.int32, device=dev),
+              "isa_low": torch.empty(t.size, dtype=torch.int32, device=dev) if isa_bits else None,
+              "lcp": torch.empty(t.size, dtype=torch.int32, device=dev)} for t in texts]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def device_step():
+        if len(texts) == 1:
+            st = ctx.build_device(d_texts[0].data_ptr(), int(texts[0].size),
+                                  {k: (v.data_ptr() if v is not None else None)
+                                   for k, v in d_out[0].items()},
+                                  sa_bits=32, isa_bits=isa_bits, lcp=lcp_enc)
+        else:
+            st = ctx.build_batch_device([(d.data_ptr(), int(t.size)) for d, t in zip(d_texts, texts)],
+                                        [{k: (v.data_ptr() if v is not None else None)
+                                          for k, v in o.items()} for o in d_out],
+                                        sa_bits=32, isa_bits=isa_bits, lcp=lcp_enc)
+        return st
+
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        device_step()
+
+    # Timed region: K builds, L2 flushed between them, profile on.
+    ctx.set_profiling(True)
+    clocks = ClockSampler(local)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    device_seconds = 0.0
+    launches = 0
+    wall0 = time.perf_counter()
+    for k in range(args.steps):
+        flush.fill_(k & 0xff)
+        torch.cuda.synchronize()
+        st = device_step()
+        device_seconds += st["device_seconds"]
+        launches += st["kernel_launches"]
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
+    clock_info = clocks.stop()
+    if dist is not None:
+        dist.barrier()
+    profile = ctx.profile()
+    ctx.set_profiling(False)
+
+    step_seconds = device_seconds / args.steps
+    if dist is not None:
+        t = torch.tensor([step_seconds], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        step_seconds = float(t.item())
+    value = world * n_total / step_seconds / 1e9
+
+    # End to end through the C ABI with pinned host buffers.
+    e2e = None
+    if not args.no_e2e:
+        pinned_text = [sg.pinned_array(int(t.size)) for t in texts]
+        for src, dst in zip(texts, pinned_text):
+            dst[:] = src
+        host_out = []
+        keep = []
+        d2h = 0
+        for t in texts:
+            planes = {}
+            for key, on in (("sa_low", True), ("isa_low", bool(isa_bits)), ("lcp", True)):
+                if not on:
+                    continue
+                arr = sg.pinned_array(int(t.size), np.uint32)
+                keep.append(arr)
+                planes[key] = arr.ctypes.data
+                d2h += arr.nbytes
+            host_out.append(planes)
+        for _ in range(2):
+            e2e_step(ctx, pinned_text, host_out, isa_bits, lcp_enc)
+        if dist is not None:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step(ctx, pinned_text, host_out, isa_bits, lcp_enc)
+        e2e_sec = (time.perf_counter() - t0) / args.steps
+        if dist is not None:
+            t = torch.tensor([e2e_sec], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_sec = float(t.item())
+        e2e = {"value": world * n_total / e2e_sec / 1e9, "unit": "Gsym/s",
+               "h2d_bytes_per_step": n_total, "d2h_bytes_per_step": d2h,
+               "ms_per_step": e2e_sec * 1e3}
+
+    # Roofline of the dominant kernel and of the whole build.
+    peak, peak_kind = peaks()
+    top = max(profile, key=lambda k: k["seconds"])
+    achieved = top["bytes"] / top["seconds"] / 1e9 if top["seconds"] > 0 else 0.0
+    traffic_ratio = load_traffic(top["kernel"])
+    roofline = {"bound": "hbm", "kernel": top["kernel"], "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                "launches_per_step": top["launches"] / args.steps,
+                "share_of_kernel_time": top["seconds"] / sum(k["seconds"] for k in profile),
+                "traffic": (traffic_ratio * top["bytes"] / top["launches"])
+                if traffic_ratio else None}
+    kernels = sorted(({"kernel": k["kernel"], "ms_per_step": k["seconds"] * 1e3 / args.steps,
+                       "launches_per_step": k["launches"] / args.steps,
+                       "GBps": (k["bytes"] / k["seconds"] / 1e9) if k["seconds"] else None}
+                      for k in profile), key=lambda k: -k["ms_per_step"])
+
+    whole = None
+    if rank == 0 and len(texts) == 1:
+        # Algorithmic bytes of the whole build from this build's own exact
+        # outputs (A_k, C depend only on the text).
+        sa = d_out[0]["sa_low"].cpu().numpy().view(np.uint32)
+        isa = d_out[0]["isa_low"].cpu().numpy().view(np.uint32)
+        lcp = d_out[0]["lcp"].cpu().numpy().view(np.uint32)
+        b = build_bytes(texts[0], sa, isa, lcp)
+        whole = {"algorithmic_bytes": b, "achieved_GBps": b / step_seconds / 1e9,
+                 "frac": b / step_seconds / 1e9 / peak}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+        if oracle.ref() is not None:
+            sample = cpu_sample(texts, 50_000_000)
+            sec = cpu_reference_step(sample, 1)
+            cpu = {"value": sample.size / sec / 1e9, "unit": "Gsym/s", "cores": 1,
+                   "kind": "reference",
+                   "sample": f"first {sample.size} symbols of the workload text, "
+                             "libdivsufsort64 + Kasai LCP via detail::BuildDivsufsort64, "
+                             "1 thread (divsufsort is serial)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "Gsym/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_seconds * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u32", "data": "synthetic",
+            "config": {"workload": desc, "symbols": n_total,
+                       "l2": "flushed between steps (256 MiB device write)",
+                       "parallelism": f"{world} independent replica(s)",
+                       "timing": "device time per build (library CUDA events), "
+                                 "max over ranks", "wall_s": wall,
+                       "build_roofline": whole, "kernels": kernels},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "clocks": clock_info, "gpu_launches": launches,
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def e2e_step(ctx, pinned_text, host_out, isa_bits, lcp_enc):
+    import sufkit_b200 as sg
+    if len(pinned_text) == 1:
+        t = pinned_text[0]
+        return ctx.build_device(t.ctypes.data, int(t.size), host_out[0], sa_bits=32,
+                                isa_bits=isa_bits, lcp=lcp_enc)
+    return ctx.build_batch_device([(t.ctypes.data, int(t.size)) for t in pinned_text], host_out,
+                                  sa_bits=32, isa_bits=isa_bits, lcp=lcp_enc)
+
+
+if __name__ == "__main__":
+    main()

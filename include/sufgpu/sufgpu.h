@@ -1,0 +1,198 @@
+/* sufgpu: B200 construction engine for sufkit's SA + ISA + LCP build path.
+ *
+ * Plain C ABI: opaque context, plain pointers and sizes, status codes, no C++
+ * exceptions and no torch types across the boundary.  A context owns one CUDA
+ * device, one stream and the device buffers it grows as builds need them; it
+ * is thread-compatible (one thread at a time per context).
+ *
+ * Every build sorts all suffixes of the given byte string exactly as
+ * libdivsufsort does (unsigned byte order, a proper prefix first), so the SA,
+ * ISA and LCP equal the reference's divsufsort64 build word for word.  Inside
+ * the device all coordinates are 32-bit, which bounds one instance (and one
+ * batch) to 2^32 - 1 symbols; outputs are written in any stored width.
+ *
+ * Citations name files of the sufkit project (malabz/sufkit).
+ */
+#ifndef SUFGPU_SUFGPU_H
+#define SUFGPU_SUFGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SUFGPU_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define SUFGPU_API __attribute__((visibility("default")))
+#else
+#define SUFGPU_API
+#endif
+
+/* Status codes.  Non-zero values are sufkit::ErrorCode + 1
+ * (include/sufkit/types.hpp:708-721), so an adapter maps them one to one. */
+typedef enum sufgpu_status {
+  SUFGPU_OK = 0,
+  SUFGPU_INVALID_INPUT = 1,    /* ErrorCode::kInvalidInput */
+  SUFGPU_IO_ERROR = 2,         /* ErrorCode::kIoError */
+  SUFGPU_UNSUPPORTED = 3,      /* ErrorCode::kUnsupportedBackend */
+  SUFGPU_CORRUPT_INDEX = 4,    /* ErrorCode::kCorruptIndex */
+  SUFGPU_VERSION_MISMATCH = 5, /* ErrorCode::kVersionMismatch */
+  SUFGPU_BUILD_FAILURE = 6     /* ErrorCode::kBuildFailure (CUDA errors, OOM) */
+} sufgpu_status;
+
+/* LCP layouts; values equal detail::LcpEncoding (src/lcp_storage.hpp:53-59). */
+typedef enum sufgpu_lcp_encoding {
+  SUFGPU_LCP_NONE = 0,
+  SUFGPU_LCP_RAW32 = 1,   /* uint32 per row */
+  SUFGPU_LCP_RAW64 = 2,   /* uint64 per row */
+  SUFGPU_LCP_BYTE32 = 3,  /* uint8 primary + uint32 anchors */
+  SUFGPU_LCP_BYTE64 = 4   /* uint8 primary + uint64 anchors */
+} sufgpu_lcp_encoding;
+
+/* Build flags. */
+#define SUFGPU_FLAG_VALIDATE 1u /* check the SA is a permutation (device) */
+
+/* What to build.  Stored widths follow CoordinateStorageWidth
+ * (include/sufkit/types.hpp:100-111): 32 native, 40 split low32+high8,
+ * 48 split low32+high16, 64 native. */
+typedef struct sufgpu_build_desc {
+  uint32_t sa_storage_bits;  /* 32, 40, 48 or 64 */
+  uint32_t isa_storage_bits; /* 0 = no ISA output, else 32, 40, 48 or 64 */
+  uint32_t lcp_encoding;     /* sufgpu_lcp_encoding */
+  uint32_t flags;            /* SUFGPU_FLAG_* */
+} sufgpu_build_desc;
+
+/* Caller-owned output planes of one instance (n rows each).  Each pointer may
+ * be host memory (pageable or pinned) or device memory of the context's
+ * device; NULL skips that plane.
+ *   sa_low/isa_low: uint32 rows for 32/40/48-bit widths, uint64 for 64;
+ *   sa_high/isa_high: uint8 (40) or uint16 (48) rows, unused otherwise;
+ *   lcp: uint32 / uint64 rows (raw) or uint8 primary bytes (byte-coded). */
+typedef struct sufgpu_outputs {
+  void *sa_low;
+  void *sa_high;
+  void *isa_low;
+  void *isa_high;
+  void *lcp;
+} sufgpu_outputs;
+
+/* Byte-coded overflow anchors (text-ordered positions with their LCP values,
+ * coordinates of 32 or 64 bits per the encoding).  Library-owned host memory,
+ * valid until the next build on the same context or sufgpu_destroy. */
+typedef struct sufgpu_anchors {
+  const void *positions;
+  const void *values;
+  uint64_t count;
+  uint32_t coordinate_bits;
+} sufgpu_anchors;
+
+/* Phase timings (CUDA events, seconds) and work counters of one build. */
+typedef struct sufgpu_build_stats {
+  double h2d_seconds;    /* text upload */
+  double sa_seconds;     /* seed sort + doubling rounds (SA and ISA final) */
+  double isa_seconds;    /* ISA packing */
+  double lcp_seconds;    /* PHI, PLCP, row gather / byte coding */
+  double storage_seconds;/* SA packing + validation */
+  double d2h_seconds;    /* output download (not overlapped part) */
+  double total_seconds;  /* whole call, wall clock */
+  double device_seconds; /* first to last device event of the call */
+  uint64_t symbols;
+  uint32_t rounds;            /* doubling rounds after the seed */
+  uint32_t seed_symbols;      /* symbols packed per seed key */
+  uint64_t active_rows;       /* sum over rounds of still-unsorted rows */
+  uint64_t irreducible_long;  /* PLCP positions finished by a warp */
+  uint64_t anchors;
+  uint32_t kernel_launches;   /* kernels launched by this call */
+  uint32_t reserved;
+} sufgpu_build_stats;
+
+typedef struct sufgpu_ctx sufgpu_ctx;
+
+/* Context lifetime.  device is a CUDA ordinal. */
+SUFGPU_API sufgpu_status sufgpu_create(sufgpu_ctx **ctx, int device);
+SUFGPU_API void sufgpu_destroy(sufgpu_ctx *ctx);
+
+/* Last error message of the context (or of a failed sufgpu_create when ctx is
+ * NULL). */
+SUFGPU_API const char *sufgpu_last_error(const sufgpu_ctx *ctx);
+
+/* Largest text (symbols, sentinel included) one build accepts. */
+SUFGPU_API uint64_t sufgpu_max_symbols(void);
+
+/* Device bytes one build of n symbols needs with this descriptor. */
+SUFGPU_API uint64_t sufgpu_device_bytes(uint64_t n, const sufgpu_build_desc *desc);
+
+/* One complete build of text[0..n) (the logical text with its sentinel, as
+ * SuffixArray::Build hands it to the constructor, src/suffix_array.cpp:
+ * 4113-4117).  Replaces detail::BuildDivsufsort32/64
+ * (src/divsufsort_backend.hpp:27-33, src/divsufsort_backend.cpp:24-157)
+ * followed by RepackSuffixArray (src/suffix_array.cpp:852-910), BuildIsa
+ * (src/suffix_array.cpp:1025-1047) and BuildLcp / BuildByteCodedLcpDirect /
+ * FinalizeLcpStorage (src/suffix_array.cpp:1073-1170).
+ * text may be host or device memory.  anchors may be NULL unless the encoding
+ * is byte-coded.  stats may be NULL. */
+SUFGPU_API sufgpu_status sufgpu_build(sufgpu_ctx *ctx, const uint8_t *text, uint64_t n,
+                           const sufgpu_build_desc *desc,
+                           const sufgpu_outputs *out, sufgpu_anchors *anchors,
+                           sufgpu_build_stats *stats);
+
+/* Drop-in for the libdivsufsort C entry point
+ * saint_t divsufsort64(const sauchar_t *T, saidx64_t *SA, saidx64_t n)
+ * (third_party/libdivsufsort/include/divsufsort64.h; divsufsort.c:331-358):
+ * same arguments, same return codes (0 ok, -1 bad arguments, -2 failure). */
+SUFGPU_API int sufgpu_divsufsort64(sufgpu_ctx *ctx, const uint8_t *T, int64_t *SA,
+                        int64_t n);
+
+/* Same for the 32-bit entry point divsufsort (divsufsort.h). */
+SUFGPU_API int sufgpu_divsufsort(sufgpu_ctx *ctx, const uint8_t *T, int32_t *SA,
+                      int32_t n);
+
+/* One independent reference of a batch. */
+typedef struct sufgpu_instance {
+  const uint8_t *text; /* host or device */
+  uint64_t n;
+  sufgpu_outputs out;
+  sufgpu_anchors anchors; /* filled for byte-coded encodings */
+} sufgpu_instance;
+
+/* Batched build: many references of uneven size sorted by the same launches
+ * (per-instance segment offsets; rounds continue only while some instance has
+ * unsorted groups).  Each instance's outputs equal its own sufgpu_build.
+ * The sum of the sizes must not exceed sufgpu_max_symbols().  The reference
+ * has no counterpart; it builds one reference per SuffixArray::Build call. */
+SUFGPU_API sufgpu_status sufgpu_build_batch(sufgpu_ctx *ctx, sufgpu_instance *instances,
+                                 uint32_t count, const sufgpu_build_desc *desc,
+                                 sufgpu_build_stats *stats);
+
+/* Per-kernel profile: when enabled, every launch is bracketed by CUDA events
+ * on the context stream and accumulated per kernel name with its algorithmic
+ * bytes (the minimum it must read and write).  Enabling resets the totals. */
+SUFGPU_API void sufgpu_set_profiling(sufgpu_ctx *ctx, int enable);
+SUFGPU_API uint32_t sufgpu_profile_count(const sufgpu_ctx *ctx);
+SUFGPU_API sufgpu_status sufgpu_profile_entry(const sufgpu_ctx *ctx, uint32_t index,
+                                              const char **name, uint64_t *launches,
+                                              double *seconds, uint64_t *bytes);
+
+/* Pinned host memory helpers (fast transfers for callers that can use them). */
+SUFGPU_API void *sufgpu_host_alloc(uint64_t bytes);
+SUFGPU_API void sufgpu_host_free(void *ptr);
+
+/* Normalizes FASTA (plain or gzip) exactly like GenomeReference::FromFasta
+ * (src/genome_reference.cpp:30-57, 131-156, 222-268): A/C/G/T (any case) ->
+ * 2..5, every other byte -> 6, a 1 after every record.  Writes at most cap
+ * bytes to out (no sentinel) and stores the full size in *size; returns
+ * SUFGPU_INVALID_INPUT for malformed input, SUFGPU_IO_ERROR if unreadable.
+ * fingerprint (FNV-1a 64 of the bytes, src/genome_reference.cpp:125-129) and
+ * records may be NULL. */
+SUFGPU_API sufgpu_status sufgpu_encode_fasta(const char *path, uint8_t *out, uint64_t cap,
+                                  uint64_t *size, uint64_t *fingerprint,
+                                  uint64_t *records);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SUFGPU_SUFGPU_H */

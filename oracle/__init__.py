@@ -1,0 +1,260 @@
+"""Test infrastructure only: ctypes loaders for the CPU oracle.
+
+* ``port()``  -> liboracle.so, our C restatement (oracle/sa_oracle.c).
+* ``ref()``   -> _ref/libsufref.so, the reference's own sources compiled by
+  oracle/Makefile (None when it has not been built).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+package, and only as the checker or the timed CPU baseline.
+"""
+from __future__ import annotations
+
+import ctypes
+import subprocess
+from pathlib import Path
+from typing import Optional
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+PORT_PATH = HERE / "liboracle.so"
+REF_PATH = HERE / "_ref" / "libsufref.so"
+
+P = ctypes.c_void_p
+U64 = ctypes.c_uint64
+
+
+def build(reference: Optional[str] = None) -> None:
+    """Compiles liboracle.so, and _ref/libsufref.so when the reference tree is
+    available (make -C oracle)."""
+    cmd = ["make", "-C", str(HERE), "-j8", "-s"]
+    if reference:
+        cmd.append(f"REF={reference}")
+    subprocess.run(cmd, check=True)
+
+
+_port = None
+_ref = None
+
+
+def port() -> ctypes.CDLL:
+    global _port
+    if _port is None:
+        if not PORT_PATH.exists():
+            build()
+        lib = ctypes.CDLL(str(PORT_PATH))
+        lib.oracle_suffix_sort.argtypes = [P, U64, P]
+        lib.oracle_isa.argtypes = [P, U64, P]
+        lib.oracle_kasai_lcp.argtypes = [P, U64, P, P, P]
+        lib.oracle_kasai_lcp.restype = None
+        lib.oracle_bytecode_lcp.argtypes = [P, U64, P, P, ctypes.c_int, P, P, P, U64]
+        lib.oracle_bytecode_lcp.restype = ctypes.c_int64
+        lib.oracle_bytecode_guide.argtypes = [P, U64, U64, P]
+        lib.oracle_bytecode_guide.restype = U64
+        lib.oracle_bytecode_exact.argtypes = [P, P, P, U64, U64, U64]
+        lib.oracle_bytecode_exact.restype = U64
+        lib.oracle_pack.argtypes = [P, U64, U64, ctypes.c_int, P, P, P]
+        lib.oracle_is_permutation.argtypes = [P, U64]
+        _port = lib
+    return _port
+
+
+def ref() -> Optional[ctypes.CDLL]:
+    global _ref
+    if _ref is None:
+        if not REF_PATH.exists():
+            return None
+        lib = ctypes.CDLL(str(REF_PATH))
+        lib.sufref_last_error.restype = ctypes.c_char_p
+        lib.sufref_divsufsort64.argtypes = [P, P, ctypes.c_int64]
+        lib.sufref_divsufsort32.argtypes = [P, P, ctypes.c_int32]
+        lib.sufref_adapter_build.argtypes = [ctypes.c_int, P, U64, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_uint32, P, P, P, P]
+        lib.sufref_pack.argtypes = [P, U64, U64, ctypes.c_int, P, P, P, P]
+        lib.sufref_bytecoded_direct.argtypes = [P, U64, P, P, ctypes.c_int, P, P, P, U64, P]
+        lib.sufref_bytecoded_from_raw.argtypes = [P, P, U64, ctypes.c_int, P, P, P, U64, P]
+        lib.sufref_bytecoded_exact.argtypes = [P, U64, P, P, U64, P, P, U64, P]
+        lib.sufref_encode_fasta.argtypes = [ctypes.c_char_p, P, U64, P, P]
+        lib.sufref_encode_fasta.restype = ctypes.c_int64
+        lib.sufref_suffix_array_build.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                                                  ctypes.c_int, ctypes.c_int, ctypes.c_uint32,
+                                                  ctypes.c_char_p, P, P]
+        lib.sufref_suffix_array_rows.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                                                 ctypes.c_int, P, U64]
+        _ref = lib
+    return _ref
+
+
+def _p(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+# --------------------------------------------------------------------------
+# Port (C restatement)
+# --------------------------------------------------------------------------
+def suffix_array(text: np.ndarray) -> np.ndarray:
+    t = np.ascontiguousarray(text, np.uint8)
+    sa = np.empty(t.size, np.uint64)
+    if port().oracle_suffix_sort(_p(t), t.size, _p(sa)) != 0:
+        raise MemoryError("oracle suffix sort failed")
+    return sa
+
+
+def inverse(sa: np.ndarray) -> np.ndarray:
+    sa = np.ascontiguousarray(sa, np.uint64)
+    isa = np.empty(sa.size, np.uint64)
+    if port().oracle_isa(_p(sa), sa.size, _p(isa)) != 0:
+        raise ValueError("not a permutation")
+    return isa
+
+
+def kasai(text: np.ndarray, sa: np.ndarray, isa: np.ndarray) -> np.ndarray:
+    t = np.ascontiguousarray(text, np.uint8)
+    sa = np.ascontiguousarray(sa, np.uint64)
+    isa = np.ascontiguousarray(isa, np.uint64)
+    lcp = np.empty(t.size, np.uint64)
+    port().oracle_kasai_lcp(_p(t), t.size, _p(sa), _p(isa), _p(lcp))
+    return lcp
+
+
+def bytecode(text: np.ndarray, sa: np.ndarray, isa: np.ndarray, width: int = 32):
+    """(primary, anchor_positions, anchor_values) as uint8 / uint64 arrays."""
+    t = np.ascontiguousarray(text, np.uint8)
+    sa = np.ascontiguousarray(sa, np.uint64)
+    isa = np.ascontiguousarray(isa, np.uint64)
+    primary = np.empty(t.size, np.uint8)
+    cap = max(16, t.size)
+    pos = np.empty(cap, np.uint64)
+    val = np.empty(cap, np.uint64)
+    k = port().oracle_bytecode_lcp(_p(t), t.size, _p(sa), _p(isa), width, _p(primary),
+                                   _p(pos), _p(val), cap)
+    if k < 0:
+        raise ValueError("byte coding failed")
+    return primary, pos[:k].copy(), val[:k].copy()
+
+
+def guide(anchor_positions: np.ndarray, n: int) -> np.ndarray:
+    a = np.ascontiguousarray(anchor_positions, np.uint64)
+    out = np.empty(2 + max(n, 1) // 4096 + 1, np.uint64)
+    k = port().oracle_bytecode_guide(_p(a), a.size, n, _p(out))
+    return out[:k].copy()
+
+
+def pack(values: np.ndarray, symbol_count: int, bits: int):
+    """(width, low32 or native64, high or None)."""
+    v = np.ascontiguousarray(values, np.uint64)
+    low = np.empty(v.size, np.uint32)
+    high8 = np.empty(v.size, np.uint8)
+    high16 = np.empty(v.size, np.uint16)
+    native = np.empty(v.size, np.uint64)
+    width = bits
+    resolved = port().oracle_pack(_p(v), v.size, symbol_count, bits, _p(low),
+                                  _p(high16 if bits == 48 else high8), _p(native))
+    if resolved < 0:
+        raise ValueError("coordinate out of range for the storage width")
+    width = resolved
+    if width == 64:
+        return width, native, None
+    if width == 40:
+        return width, low, high8
+    if width == 48:
+        return width, low, high16
+    return width, low, None
+
+
+def full_build(text: np.ndarray):
+    """(sa, isa, lcp) from the port."""
+    sa = suffix_array(text)
+    isa = inverse(sa)
+    return sa, isa, kasai(text, sa, isa)
+
+
+# --------------------------------------------------------------------------
+# Reference (compiled sufkit sources)
+# --------------------------------------------------------------------------
+def _check(lib, rc):
+    if rc != 0:
+        raise RuntimeError(f"reference call failed ({rc}): {lib.sufref_last_error().decode()}")
+
+
+def ref_adapter(text: np.ndarray, width: int = 64, threads: int = 1):
+    """detail::BuildDivsufsort{width}: (sa, isa, lcp, seconds[3])."""
+    lib = ref()
+    t = np.ascontiguousarray(text, np.uint8)
+    sa = np.empty(t.size, np.uint64)
+    isa = np.empty(t.size, np.uint64)
+    lcp = np.empty(t.size, np.uint64)
+    sec = (ctypes.c_double * 3)()
+    _check(lib, lib.sufref_adapter_build(width, _p(t), t.size, 1, 1, threads, _p(sa), _p(isa),
+                                         _p(lcp), sec))
+    return sa, isa, lcp, list(sec)
+
+
+def ref_divsufsort64(text: np.ndarray) -> np.ndarray:
+    lib = ref()
+    t = np.ascontiguousarray(text, np.uint8)
+    sa = np.empty(t.size, np.int64)
+    _check(lib, lib.sufref_divsufsort64(_p(t), _p(sa), t.size))
+    return sa
+
+
+def ref_bytecode(text: np.ndarray, sa: np.ndarray, isa: np.ndarray, width: int = 32):
+    lib = ref()
+    t = np.ascontiguousarray(text, np.uint8)
+    sa = np.ascontiguousarray(sa, np.uint64)
+    isa = np.ascontiguousarray(isa, np.uint64)
+    primary = np.empty(t.size, np.uint8)
+    cap = max(16, t.size)
+    pos = np.empty(cap, np.uint64)
+    val = np.empty(cap, np.uint64)
+    count = U64()
+    _check(lib, lib.sufref_bytecoded_direct(_p(t), t.size, _p(sa), _p(isa), width, _p(primary),
+                                            _p(pos), _p(val), cap, ctypes.addressof(count)))
+    k = count.value
+    return primary, pos[:k].copy(), val[:k].copy()
+
+
+def ref_bytecode_from_raw(lcp: np.ndarray, isa: np.ndarray, width: int = 32):
+    lib = ref()
+    lcp = np.ascontiguousarray(lcp, np.uint64)
+    isa = np.ascontiguousarray(isa, np.uint64)
+    primary = np.empty(lcp.size, np.uint8)
+    cap = max(16, lcp.size)
+    pos = np.empty(cap, np.uint64)
+    val = np.empty(cap, np.uint64)
+    count = U64()
+    _check(lib, lib.sufref_bytecoded_from_raw(_p(lcp), _p(isa), lcp.size, width, _p(primary),
+                                              _p(pos), _p(val), cap, ctypes.addressof(count)))
+    k = count.value
+    return primary, pos[:k].copy(), val[:k].copy()
+
+
+def ref_pack(values: np.ndarray, symbol_count: int, bits: int):
+    lib = ref()
+    v = np.ascontiguousarray(values, np.uint64)
+    low = np.empty(v.size, np.uint32)
+    high = np.empty(v.size, np.uint16 if bits == 48 else np.uint8)
+    native = np.empty(v.size, np.uint64)
+    width = ctypes.c_int()
+    _check(lib, lib.sufref_pack(_p(v), v.size, symbol_count, bits, _p(low), _p(high),
+                                _p(native), ctypes.addressof(width)))
+    w = width.value
+    if w == 64:
+        return w, native, None
+    return w, low, (high if w in (40, 48) else None)
+
+
+def ref_encode_fasta(path) -> tuple[np.ndarray, int]:
+    lib = ref()
+    need = U64()
+    fp = U64()
+    raw = str(path).encode()
+    rc = lib.sufref_encode_fasta(raw, None, 0, ctypes.addressof(need), ctypes.addressof(fp))
+    if rc == -1:
+        raise ValueError(lib.sufref_last_error().decode())
+    out = np.empty(need.value, np.uint8)
+    rc = lib.sufref_encode_fasta(raw, _p(out), need.value, ctypes.addressof(need),
+                                 ctypes.addressof(fp))
+    if rc < 0:
+        raise ValueError(lib.sufref_last_error().decode())
+    return out, fp.value

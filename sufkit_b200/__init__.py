@@ -1,0 +1,504 @@
+"""sufkit_b200: Python host side of the sufgpu B200 construction engine.
+
+Every call goes through the C ABI of ``libsufgpu.so`` (include/sufgpu/sufgpu.h)
+with ctypes; the arrays live in numpy (host) or in any object exposing a device
+pointer.  The names mirror the reference's constructor interface
+(``detail::BuildDivsufsort32/64``, src/divsufsort_backend.hpp:13-33 in sufkit):
+``build_cuda32`` / ``build_cuda64`` return the same fields (suffix_array, isa,
+lcp and per-phase seconds) and raise :class:`SufkitError` with the reference's
+``ErrorCode`` categories.
+
+There is no CPU fallback: importing works anywhere, but every build needs the
+compiled library and a CUDA device, and fails loudly without them.
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+from dataclasses import dataclass, field
+from pathlib import Path
+from typing import Optional, Sequence
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+LIBRARY_PATH = _HERE / "libsufgpu.so"
+
+
+class ErrorCode(enum.IntEnum):
+    """sufkit::ErrorCode (include/sufkit/types.hpp:708-721)."""
+
+    INVALID_INPUT = 0
+    IO_ERROR = 1
+    UNSUPPORTED_BACKEND = 2
+    CORRUPT_INDEX = 3
+    VERSION_MISMATCH = 4
+    BUILD_FAILURE = 5
+
+
+class SufkitError(RuntimeError):
+    """Mirror of sufkit::Error: a stable category plus a message."""
+
+    def __init__(self, code: ErrorCode, message: str):
+        super().__init__(message)
+        self.code = ErrorCode(code)
+
+
+class LcpEncoding(enum.IntEnum):
+    """detail::LcpEncoding (src/lcp_storage.hpp:53-59)."""
+
+    NONE = 0
+    RAW32 = 1
+    RAW64 = 2
+    BYTE32 = 3
+    BYTE64 = 4
+
+
+FLAG_VALIDATE = 1
+
+
+class _Desc(ctypes.Structure):
+    _fields_ = [("sa_storage_bits", ctypes.c_uint32),
+                ("isa_storage_bits", ctypes.c_uint32),
+                ("lcp_encoding", ctypes.c_uint32),
+                ("flags", ctypes.c_uint32)]
+
+
+class _Outputs(ctypes.Structure):
+    _fields_ = [("sa_low", ctypes.c_void_p), ("sa_high", ctypes.c_void_p),
+                ("isa_low", ctypes.c_void_p), ("isa_high", ctypes.c_void_p),
+                ("lcp", ctypes.c_void_p)]
+
+
+class _Anchors(ctypes.Structure):
+    _fields_ = [("positions", ctypes.c_void_p), ("values", ctypes.c_void_p),
+                ("count", ctypes.c_uint64), ("coordinate_bits", ctypes.c_uint32)]
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [("h2d_seconds", ctypes.c_double), ("sa_seconds", ctypes.c_double),
+                ("isa_seconds", ctypes.c_double), ("lcp_seconds", ctypes.c_double),
+                ("storage_seconds", ctypes.c_double), ("d2h_seconds", ctypes.c_double),
+                ("total_seconds", ctypes.c_double), ("device_seconds", ctypes.c_double),
+                ("symbols", ctypes.c_uint64),
+                ("rounds", ctypes.c_uint32), ("seed_symbols", ctypes.c_uint32),
+                ("active_rows", ctypes.c_uint64), ("irreducible_long", ctypes.c_uint64),
+                ("anchors", ctypes.c_uint64), ("kernel_launches", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
+
+
+class _Instance(ctypes.Structure):
+    _fields_ = [("text", ctypes.c_void_p), ("n", ctypes.c_uint64),
+                ("out", _Outputs), ("anchors", _Anchors)]
+
+
+_lib: Optional[ctypes.CDLL] = None
+
+# Exported symbols of the C ABI with their ctypes signatures.
+_SIGNATURES = {
+    "sufgpu_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int]),
+    "sufgpu_destroy": (None, [ctypes.c_void_p]),
+    "sufgpu_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "sufgpu_max_symbols": (ctypes.c_uint64, []),
+    "sufgpu_device_bytes": (ctypes.c_uint64, [ctypes.c_uint64, ctypes.c_void_p]),
+    "sufgpu_build": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                    ctypes.POINTER(_Desc), ctypes.POINTER(_Outputs),
+                                    ctypes.POINTER(_Anchors), ctypes.POINTER(_Stats)]),
+    "sufgpu_divsufsort64": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.c_void_p, ctypes.c_int64]),
+    "sufgpu_divsufsort": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_void_p, ctypes.c_int32]),
+    "sufgpu_build_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(_Instance),
+                                          ctypes.c_uint32, ctypes.POINTER(_Desc),
+                                          ctypes.POINTER(_Stats)]),
+    "sufgpu_set_profiling": (None, [ctypes.c_void_p, ctypes.c_int]),
+    "sufgpu_profile_count": (ctypes.c_uint32, [ctypes.c_void_p]),
+    "sufgpu_profile_entry": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32,
+                                            ctypes.POINTER(ctypes.c_char_p),
+                                            ctypes.POINTER(ctypes.c_uint64),
+                                            ctypes.POINTER(ctypes.c_double),
+                                            ctypes.POINTER(ctypes.c_uint64)]),
+    "sufgpu_host_alloc": (ctypes.c_void_p, [ctypes.c_uint64]),
+    "sufgpu_host_free": (None, [ctypes.c_void_p]),
+    "sufgpu_encode_fasta": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_uint64,
+                                           ctypes.POINTER(ctypes.c_uint64),
+                                           ctypes.POINTER(ctypes.c_uint64),
+                                           ctypes.POINTER(ctypes.c_uint64)]),
+}
+
+
+def library() -> ctypes.CDLL:
+    """Loads libsufgpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIBRARY_PATH.exists():
+            raise SufkitError(ErrorCode.UNSUPPORTED_BACKEND,
+                              f"{LIBRARY_PATH} is missing: run python -m sufkit_b200.build")
+        lib = ctypes.CDLL(str(LIBRARY_PATH))
+        for name, (restype, argtypes) in _SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = restype
+            fn.argtypes = argtypes
+        _lib = lib
+    return _lib
+
+
+def exported_symbols() -> list[str]:
+    return list(_SIGNATURES)
+
+
+def _ptr(a: Optional[np.ndarray]) -> Optional[int]:
+    if a is None:
+        return None
+    return a.ctypes.data
+
+
+def _raise(status: int, message: str):
+    raise SufkitError(ErrorCode(status - 1), message)
+
+
+def _as_text(text) -> np.ndarray:
+    if isinstance(text, (bytes, bytearray, memoryview)):
+        return np.frombuffer(bytes(text), dtype=np.uint8)
+    arr = np.ascontiguousarray(text)
+    if arr.dtype != np.uint8:
+        raise SufkitError(ErrorCode.INVALID_INPUT, "text must be uint8")
+    return arr
+
+
+def _plane_dtype(bits: int):
+    return np.uint64 if bits == 64 else np.uint32
+
+
+def _high_dtype(bits: int):
+    return {40: np.uint8, 48: np.uint16}.get(bits)
+
+
+def compose(low: np.ndarray, high: Optional[np.ndarray]) -> np.ndarray:
+    """Decodes a (low, high) coordinate plane pair to uint64 values."""
+    out = low.astype(np.uint64)
+    if high is not None:
+        out |= high.astype(np.uint64) << np.uint64(32)
+    return out
+
+
+@dataclass
+class BuildResult:
+    """Planes of one build (host numpy arrays)."""
+
+    sa_low: np.ndarray
+    sa_high: Optional[np.ndarray] = None
+    isa_low: Optional[np.ndarray] = None
+    isa_high: Optional[np.ndarray] = None
+    lcp: Optional[np.ndarray] = None
+    anchor_positions: Optional[np.ndarray] = None
+    anchor_values: Optional[np.ndarray] = None
+    stats: dict = field(default_factory=dict)
+
+    @property
+    def sa(self) -> np.ndarray:
+        return compose(self.sa_low, self.sa_high)
+
+    @property
+    def isa(self) -> Optional[np.ndarray]:
+        return None if self.isa_low is None else compose(self.isa_low, self.isa_high)
+
+
+class Context:
+    """One CUDA device with its stream and grown device buffers."""
+
+    def __init__(self, device: int = 0):
+        lib = library()
+        handle = ctypes.c_void_p()
+        status = lib.sufgpu_create(ctypes.byref(handle), device)
+        if status != 0:
+            _raise(status, lib.sufgpu_last_error(None).decode())
+        self._lib = lib
+        self._h = handle
+        self.last_stats: dict = {}
+
+    def close(self):
+        if self._h:
+            self._lib.sufgpu_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _error(self) -> str:
+        return self._lib.sufgpu_last_error(self._h).decode()
+
+    def _alloc_outputs(self, n: int, sa_bits: int, isa_bits: int, lcp: LcpEncoding):
+        planes = {"sa_low": np.empty(n, _plane_dtype(sa_bits))}
+        if _high_dtype(sa_bits):
+            planes["sa_high"] = np.empty(n, _high_dtype(sa_bits))
+        if isa_bits:
+            planes["isa_low"] = np.empty(n, _plane_dtype(isa_bits))
+            if _high_dtype(isa_bits):
+                planes["isa_high"] = np.empty(n, _high_dtype(isa_bits))
+        if lcp in (LcpEncoding.RAW32, LcpEncoding.RAW64):
+            planes["lcp"] = np.empty(n, np.uint32 if lcp == LcpEncoding.RAW32 else np.uint64)
+        elif lcp in (LcpEncoding.BYTE32, LcpEncoding.BYTE64):
+            planes["lcp"] = np.empty(n, np.uint8)
+        return planes
+
+    @staticmethod
+    def _outputs(planes: dict) -> _Outputs:
+        return _Outputs(*(_ptr(planes.get(k)) for k in
+                          ("sa_low", "sa_high", "isa_low", "isa_high", "lcp")))
+
+    @staticmethod
+    def _anchors(a: _Anchors, lcp: LcpEncoding):
+        if lcp not in (LcpEncoding.BYTE32, LcpEncoding.BYTE64):
+            return None, None
+        dtype = np.uint32 if a.coordinate_bits == 32 else np.uint64
+        if a.count == 0 or not a.positions:
+            return np.empty(0, dtype), np.empty(0, dtype)
+        size = int(a.count) * np.dtype(dtype).itemsize
+        pos = np.frombuffer(ctypes.string_at(a.positions, size), dtype=dtype).copy()
+        val = np.frombuffer(ctypes.string_at(a.values, size), dtype=dtype).copy()
+        return pos, val
+
+    def build(self, text, sa_bits: int = 32, isa_bits: int = 32,
+              lcp: LcpEncoding = LcpEncoding.RAW32, validate: bool = False) -> BuildResult:
+        """One complete build of ``text`` (the logical text including its
+        sentinel).  Returns host planes; see include/sufgpu/sufgpu.h."""
+        t = _as_text(text)
+        n = int(t.size)
+        lcp = LcpEncoding(lcp)
+        planes = self._alloc_outputs(n, sa_bits, isa_bits, lcp)
+        desc = _Desc(sa_bits, isa_bits, int(lcp), FLAG_VALIDATE if validate else 0)
+        out = self._outputs(planes)
+        anchors = _Anchors()
+        stats = _Stats()
+        status = self._lib.sufgpu_build(self._h, _ptr(t), n, ctypes.byref(desc),
+                                        ctypes.byref(out), ctypes.byref(anchors),
+                                        ctypes.byref(stats))
+        if status != 0:
+            _raise(status, self._error())
+        pos, val = self._anchors(anchors, lcp)
+        self.last_stats = stats.as_dict()
+        return BuildResult(anchor_positions=pos, anchor_values=val,
+                           stats=self.last_stats, **planes)
+
+    def build_batch(self, texts: Sequence, sa_bits: int = 32, isa_bits: int = 0,
+                    lcp: LcpEncoding = LcpEncoding.RAW32,
+                    validate: bool = False) -> list[BuildResult]:
+        """Builds many independent references with the same launches."""
+        ts = [_as_text(t) for t in texts]
+        lcp = LcpEncoding(lcp)
+        all_planes = [self._alloc_outputs(int(t.size), sa_bits, isa_bits, lcp) for t in ts]
+        arr = (_Instance * len(ts))()
+        for j, (t, planes) in enumerate(zip(ts, all_planes)):
+            arr[j].text = _ptr(t)
+            arr[j].n = int(t.size)
+            arr[j].out = self._outputs(planes)
+        desc = _Desc(sa_bits, isa_bits, int(lcp), FLAG_VALIDATE if validate else 0)
+        stats = _Stats()
+        status = self._lib.sufgpu_build_batch(self._h, arr, len(ts), ctypes.byref(desc),
+                                              ctypes.byref(stats))
+        if status != 0:
+            _raise(status, self._error())
+        self.last_stats = stats.as_dict()
+        results = []
+        for j, planes in enumerate(all_planes):
+            pos, val = self._anchors(arr[j].anchors, lcp)
+            results.append(BuildResult(anchor_positions=pos, anchor_values=val,
+                                       stats=self.last_stats, **planes))
+        return results
+
+    def set_profiling(self, enable: bool = True) -> None:
+        self._lib.sufgpu_set_profiling(self._h, int(enable))
+
+    def profile(self) -> list[dict]:
+        """Per-kernel totals since profiling was enabled."""
+        out = []
+        for i in range(self._lib.sufgpu_profile_count(self._h)):
+            name = ctypes.c_char_p()
+            launches = ctypes.c_uint64()
+            seconds = ctypes.c_double()
+            nbytes = ctypes.c_uint64()
+            self._lib.sufgpu_profile_entry(self._h, i, ctypes.byref(name), ctypes.byref(launches),
+                                           ctypes.byref(seconds), ctypes.byref(nbytes))
+            out.append({"kernel": name.value.decode(), "launches": launches.value,
+                        "seconds": seconds.value, "bytes": nbytes.value})
+        return out
+
+    def build_device(self, text_ptr: int, n: int, out_ptrs: dict, sa_bits: int = 32,
+                     isa_bits: int = 32, lcp: LcpEncoding = LcpEncoding.RAW32,
+                     validate: bool = False) -> dict:
+        """Build from a device-resident text into device-resident planes
+        (raw pointers, e.g. from torch tensors).  Returns the stats."""
+        desc = _Desc(sa_bits, isa_bits, int(LcpEncoding(lcp)), FLAG_VALIDATE if validate else 0)
+        out = _Outputs(*(out_ptrs.get(k) for k in ("sa_low", "sa_high", "isa_low", "isa_high", "lcp")))
+        anchors = _Anchors()
+        stats = _Stats()
+        status = self._lib.sufgpu_build(self._h, text_ptr, n, ctypes.byref(desc), ctypes.byref(out),
+                                        ctypes.byref(anchors), ctypes.byref(stats))
+        if status != 0:
+            _raise(status, self._error())
+        self.last_stats = stats.as_dict()
+        return self.last_stats
+
+    def build_batch_device(self, texts: Sequence[tuple[int, int]], outs: Sequence[dict],
+                           sa_bits: int = 32, isa_bits: int = 0,
+                           lcp: LcpEncoding = LcpEncoding.RAW32, validate: bool = False) -> dict:
+        """Batched build from (pointer, length) texts into raw output pointers."""
+        arr = (_Instance * len(texts))()
+        for j, ((ptr, n), o) in enumerate(zip(texts, outs)):
+            arr[j].text = ptr
+            arr[j].n = n
+            arr[j].out = _Outputs(*(o.get(k) for k in ("sa_low", "sa_high", "isa_low",
+                                                       "isa_high", "lcp")))
+        desc = _Desc(sa_bits, isa_bits, int(LcpEncoding(lcp)), FLAG_VALIDATE if validate else 0)
+        stats = _Stats()
+        status = self._lib.sufgpu_build_batch(self._h, arr, len(texts), ctypes.byref(desc),
+                                              ctypes.byref(stats))
+        if status != 0:
+            _raise(status, self._error())
+        self.last_stats = stats.as_dict()
+        return self.last_stats
+
+    def divsufsort64(self, text) -> np.ndarray:
+        """Drop-in for libdivsufsort's divsufsort64 (returns the int64 SA)."""
+        t = _as_text(text)
+        sa = np.empty(t.size, np.int64)
+        rc = self._lib.sufgpu_divsufsort64(self._h, _ptr(t), _ptr(sa), int(t.size))
+        if rc != 0:
+            raise SufkitError(ErrorCode.BUILD_FAILURE, f"divsufsort64 returned {rc}: {self._error()}")
+        return sa
+
+    def divsufsort(self, text) -> np.ndarray:
+        t = _as_text(text)
+        sa = np.empty(t.size, np.int32)
+        rc = self._lib.sufgpu_divsufsort(self._h, _ptr(t), _ptr(sa), int(t.size))
+        if rc != 0:
+            raise SufkitError(ErrorCode.BUILD_FAILURE, f"divsufsort returned {rc}: {self._error()}")
+        return sa
+
+
+@dataclass
+class CudaBuildResult:
+    """Field-for-field mirror of detail::DivSufsortBuildResult<Index>
+    (src/divsufsort_backend.hpp:13-25)."""
+
+    suffix_array: np.ndarray
+    isa: np.ndarray
+    lcp: np.ndarray
+    sa_seconds: float = 0.0
+    isa_seconds: float = 0.0
+    lcp_seconds: float = 0.0
+
+
+_default_ctx: Optional[Context] = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+def _build_cuda(width: int, text, sampling_rate: int, retain_lcp: bool, retain_isa: bool,
+                threads: int) -> CudaBuildResult:
+    """Same contract as BuildDivsufsort<Index> (src/divsufsort_backend.cpp:24-157)
+    for sampling_rate 1: SA in Index, ISA/LCP as uint64 when retained."""
+    t = _as_text(text)
+    if sampling_rate != 1:
+        raise SufkitError(ErrorCode.UNSUPPORTED_BACKEND,
+                          "the GPU constructor builds complete suffix arrays (K=1)")
+    if threads == 0:
+        raise SufkitError(ErrorCode.INVALID_INPUT, "thread count must be greater than zero")
+    limit = np.iinfo(np.int32).max if width == 32 else np.iinfo(np.int64).max
+    if t.size > limit:
+        raise SufkitError(ErrorCode.INVALID_INPUT,
+                          f"reference is too large for divsufsort{width}")
+    ctx = default_context()
+    r = ctx.build(t, sa_bits=64 if width == 64 else 32,
+                  isa_bits=64 if (retain_isa or retain_lcp) else 0,
+                  lcp=LcpEncoding.RAW64 if retain_lcp else LcpEncoding.NONE)
+    sa = r.sa_low.astype(np.int32 if width == 32 else np.int64, copy=False)
+    st = r.stats
+    return CudaBuildResult(
+        suffix_array=sa,
+        isa=r.isa_low if retain_isa else np.empty(0, np.uint64),
+        lcp=r.lcp if retain_lcp else np.empty(0, np.uint64),
+        sa_seconds=st["sa_seconds"], isa_seconds=st["isa_seconds"],
+        lcp_seconds=st["lcp_seconds"])
+
+
+def build_cuda32(text, sampling_rate: int = 1, retain_lcp: bool = False,
+                 retain_isa: bool = False, threads: int = 1) -> CudaBuildResult:
+    return _build_cuda(32, text, sampling_rate, retain_lcp, retain_isa, threads)
+
+
+def build_cuda64(text, sampling_rate: int = 1, retain_lcp: bool = False,
+                 retain_isa: bool = False, threads: int = 1) -> CudaBuildResult:
+    return _build_cuda(64, text, sampling_rate, retain_lcp, retain_isa, threads)
+
+
+class _Pinned:
+    def __init__(self, nbytes: int):
+        self.addr = library().sufgpu_host_alloc(max(1, nbytes))
+        if not self.addr:
+            raise SufkitError(ErrorCode.BUILD_FAILURE, "cannot allocate pinned host memory")
+
+    def __del__(self):
+        try:
+            library().sufgpu_host_free(self.addr)
+        except Exception:
+            pass
+
+
+def pinned_array(count: int, dtype=np.uint8) -> np.ndarray:
+    """A numpy array in page-locked host memory (freed with the array)."""
+    dtype = np.dtype(dtype)
+    holder = _Pinned(count * dtype.itemsize)
+    buf = (ctypes.c_uint8 * max(1, count * dtype.itemsize)).from_address(holder.addr)
+    arr = np.frombuffer(buf, dtype=np.uint8)[: count * dtype.itemsize].view(dtype)
+    arr.flags.writeable = True
+    _PINNED_OWNERS[id(arr)] = holder
+    import weakref
+    weakref.finalize(arr, _PINNED_OWNERS.pop, id(arr), None)
+    return arr
+
+
+_PINNED_OWNERS: dict = {}
+
+
+def encode_fasta(path) -> tuple[np.ndarray, int, int]:
+    """GenomeReference::FromFasta normalization: (encoded bytes without the
+    sentinel, FNV-1a fingerprint, record count)."""
+    lib = library()
+    size = ctypes.c_uint64()
+    fp = ctypes.c_uint64()
+    recs = ctypes.c_uint64()
+    raw = str(path).encode()
+    status = lib.sufgpu_encode_fasta(raw, None, 0, ctypes.byref(size), ctypes.byref(fp),
+                                     ctypes.byref(recs))
+    if status not in (0,):
+        _raise(status, f"cannot normalize FASTA {path}")
+    out = np.empty(size.value, np.uint8)
+    status = lib.sufgpu_encode_fasta(raw, _ptr(out), size.value, ctypes.byref(size),
+                                     ctypes.byref(fp), ctypes.byref(recs))
+    if status != 0:
+        _raise(status, f"cannot normalize FASTA {path}")
+    return out, fp.value, recs.value
+
+
+def logical_text(encoded: np.ndarray) -> np.ndarray:
+    """Appends the unique 0 sentinel (src/suffix_array.cpp:4113-4117)."""
+    return np.concatenate([np.asarray(encoded, np.uint8), np.zeros(1, np.uint8)])

@@ -1,0 +1,49 @@
+"""Build recipe for the sufgpu shared library (sm_100a, built in-tree).
+
+``python -m sufkit_b200.build`` compiles ``csrc/*.cu`` and ``csrc/*.cpp`` into
+``sufkit_b200/libsufgpu.so`` with nvcc.  nvcc cross-compiles for sm_100a on a
+machine without a GPU, so this runs anywhere the CUDA toolkit is installed.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+CSRC = HERE / "csrc"
+LIB = HERE / "libsufgpu.so"
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def sources() -> list[Path]:
+    return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp"))
+
+
+def up_to_date() -> bool:
+    if not LIB.exists():
+        return False
+    stamp = LIB.stat().st_mtime
+    inputs = sources() + sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.hpp"))
+    inputs += sorted((HERE.parent / "include").rglob("*.h"))
+    return all(p.stat().st_mtime <= stamp for p in inputs)
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    if not force and up_to_date():
+        return LIB
+    nvcc = os.environ.get("NVCC", "nvcc")
+    cmd = [nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
+           "-Xcompiler", "-fvisibility=hidden", "-shared", "-o", str(LIB) + ".tmp",
+           *map(str, sources()), "-lz"]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    os.replace(str(LIB) + ".tmp", LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True)
+    print(LIB)

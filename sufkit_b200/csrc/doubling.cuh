@@ -1,0 +1,352 @@
+// Prefix-doubling suffix sort kernels.
+//
+// Seed: every position gets a 64-bit key packing its first s symbols (symbols
+// remapped to 1..sigma, 0 = past the end of the instance), and (key, position)
+// pairs are radix sorted.  Groups of equal keys then get their head row as
+// rank; rows in groups of two or more go to the active list.
+//
+// Round (prefix length h -> 2h): each active position p gets the composite key
+// (dense group id, rank[p+h] + 1 or 0 past the end); a radix sort of the
+// active list orders every group by its second key; new heads, SA rows and
+// ranks are written, and positions that became singletons retire.  Only the
+// still-unsorted positions are ever touched after the seed.
+#pragma once
+
+#include "common.cuh"
+#include "scan.cuh"
+
+namespace sufgpu {
+
+constexpr int kScanBlock = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanBlock * kScanItems;
+
+// Segment bounds for one instance-aware kernel.  count == 1 with begin = {0, n}
+// for a single reference.
+struct Segments {
+  const u64* begin;  // count+1 offsets into the concatenated text
+  u32 count;
+};
+
+__device__ __forceinline__ u64 segment_end(const Segments& s, u64 x) {
+  if (s.count == 1) return s.begin[1];
+  return s.begin[find_segment(s.begin, s.count, x) + 1];
+}
+
+__device__ __forceinline__ bool is_segment_start(const Segments& s, u64 x) {
+  if (x == 0) return true;
+  if (s.count == 1) return false;
+  return s.begin[find_segment(s.begin, s.count, x)] == x;
+}
+
+// Byte histogram of the text (for the symbol remap).  Runs of one byte value
+// are counted in registers first so long N runs do not serialise on one
+// shared-memory counter.
+__global__ void __launch_bounds__(256)
+alphabet_histogram_kernel(const u8* __restrict__ text, u64 n,
+                          u32* __restrict__ hist) {
+  __shared__ u32 local[256];
+  local[threadIdx.x] = 0;
+  __syncthreads();
+  const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x * 16;
+  for (u64 base = (static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x) * 16;
+       base < n; base += stride) {
+    u8 bytes[16];
+    if (base + 16 <= n) {
+      const uint4 v = *reinterpret_cast<const uint4*>(text + base);
+      const u32 w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+      for (int i = 0; i < 16; ++i) bytes[i] = static_cast<u8>(w[i >> 2] >> ((i & 3) * 8));
+    } else {
+      for (int i = 0; i < 16; ++i) bytes[i] = base + i < n ? text[base + i] : 0;
+    }
+    const int valid = base + 16 <= n ? 16 : static_cast<int>(n - base);
+    u32 run_value = bytes[0];
+    u32 run_len = 0;
+    for (int i = 0; i < valid; ++i) {
+      if (bytes[i] == run_value) {
+        ++run_len;
+      } else {
+        atomicAdd(&local[run_value], run_len);
+        run_value = bytes[i];
+        run_len = 1;
+      }
+    }
+    if (run_len) atomicAdd(&local[run_value], run_len);
+  }
+  __syncthreads();
+  if (local[threadIdx.x]) atomicAdd(&hist[threadIdx.x], local[threadIdx.x]);
+}
+
+// Seed keys.  Each thread computes kSeedRun consecutive keys by sliding a
+// window over text staged in shared memory (tile + halo).  code[] maps bytes
+// to 1..sigma (sigma <= 256, so 16-bit codes); symbols at or beyond the
+// instance end contribute 0.
+constexpr int kSeedBlock = 256;
+constexpr int kSeedRun = 16;
+constexpr int kSeedTile = kSeedBlock * kSeedRun;
+constexpr int kSeedHalo = 64;
+
+__global__ void __launch_bounds__(kSeedBlock)
+seed_keys_kernel(const u8* __restrict__ text, u64 n, Segments segs,
+                 const u16* __restrict__ code_table, u32 bits, u32 symbols,
+                 u64* __restrict__ keys, u32* __restrict__ vals) {
+  __shared__ u16 code[256];
+  __shared__ __align__(16) u8 window[kSeedTile + kSeedHalo];
+  code[threadIdx.x] = code_table[threadIdx.x];
+  const u64 tile_first = static_cast<u64>(blockIdx.x) * kSeedTile;
+  // Stage tile + halo as 16-byte vectors (the text buffer is padded).
+  for (int i = threadIdx.x; i < (kSeedTile + kSeedHalo) / 16; i += kSeedBlock) {
+    const u64 at = tile_first + static_cast<u64>(i) * 16;
+    uint4 v = make_uint4(0, 0, 0, 0);
+    if (at < n) v = *reinterpret_cast<const uint4*>(text + at);
+    *reinterpret_cast<uint4*>(window + i * 16) = v;
+  }
+  __syncthreads();
+  const u64 mask = symbols * bits >= 64 ? ~0ull : ((1ull << (symbols * bits)) - 1);
+  const u32 local0 = threadIdx.x * kSeedRun;
+  u64 pos = tile_first + local0;
+  if (pos >= n) return;
+  u64 end = segment_end(segs, pos);
+  u64 key = 0;
+  bool fresh = true;
+  u64 out_keys[kSeedRun];
+  int produced = 0;
+  for (int r = 0; r < kSeedRun && pos < n; ++r, ++pos) {
+    if (pos >= end) {  // crossed into the next instance
+      end = segment_end(segs, pos);
+      fresh = true;
+    }
+    const u32 local = local0 + r;
+    if (fresh) {
+      key = 0;
+      for (u32 t = 0; t < symbols; ++t) {
+        const u32 c = pos + t < end ? code[window[local + t]] : 0u;
+        key = (key << bits) | c;
+      }
+      fresh = false;
+    } else {
+      const u64 q = pos + symbols - 1;
+      const u32 c = q < end ? code[window[local + symbols - 1]] : 0u;
+      key = ((key << bits) | c) & mask;
+    }
+    out_keys[r] = key;
+    produced = r + 1;
+  }
+  const u64 first = tile_first + local0;
+  for (int r = 0; r < produced; ++r) {
+    keys[first + r] = out_keys[r];
+    vals[first + r] = static_cast<u32>(first + r);
+  }
+}
+
+// After the seed sort: head flags, head-row ranks and the initial active list.
+// Two scans share the tile: a max-scan of head rows and a sum-scan of active
+// flags (the compaction).  counters[0] receives the active count.
+__global__ void __launch_bounds__(kScanBlock)
+seed_rank_kernel(const u64* __restrict__ keys, const u32* __restrict__ sa,
+                 u64 n, Segments segs, u32* __restrict__ rank,
+                 u32* __restrict__ active, u64* status_max, u64* status_sum,
+                 u32* tile_counter, u64* active_count, DeviceFlags* flags) {
+  __shared__ u64 warp_smem[kScanBlock / 32];
+  __shared__ u64 tile_prefix[2];
+  __shared__ u32 tile_slot;
+  const u32 tile = claim_tile(tile_counter, &tile_slot);
+  const u64 row0 = static_cast<u64>(tile) * kScanTile + threadIdx.x * kScanItems;
+
+  u64 k[kScanItems + 2];  // rows row0-1 .. row0+kScanItems
+#pragma unroll
+  for (int i = 0; i < kScanItems + 2; ++i) {
+    const long long r = static_cast<long long>(row0) - 1 + i;
+    k[i] = (r >= 0 && static_cast<u64>(r) < n) ? keys[r] : 0;
+  }
+  bool head[kScanItems + 1];
+#pragma unroll
+  for (int i = 0; i < kScanItems + 1; ++i) {
+    const u64 r = row0 + i;
+    head[i] = r >= n || is_segment_start(segs, r) || k[i + 1] != k[i];
+  }
+  u64 head_max = 0;  // inclusive running max within the thread
+  u32 act = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const u64 r = row0 + i;
+    if (r < n) {
+      if (head[i]) head_max = r;
+      if (!(head[i] && head[i + 1])) ++act;
+    }
+  }
+  u64 agg_max, agg_sum;
+  const u64 excl_max = block_exclusive_scan<kScanBlock>(head_max, MaxOp{}, warp_smem, &agg_max);
+  const u64 excl_sum = block_exclusive_scan<kScanBlock>(act, SumOp{}, warp_smem, &agg_sum);
+  const u32 warp = threadIdx.x >> 5;
+  if (warp == 0) {
+    const u64 p = warp_lookback(status_max, tile, agg_max, MaxOp{}, flags, 2);
+    if ((threadIdx.x & 31) == 0) tile_prefix[0] = p;
+  } else if (warp == 1) {
+    const u64 p = warp_lookback(status_sum, tile, agg_sum, SumOp{}, flags, 3);
+    if ((threadIdx.x & 31) == 0) tile_prefix[1] = p;
+  }
+  __syncthreads();
+  u64 running_max = tile_prefix[0] > excl_max ? tile_prefix[0] : excl_max;
+  u64 out = tile_prefix[1] + excl_sum;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const u64 r = row0 + i;
+    if (r < n) {
+      if (head[i]) running_max = r;
+      const u32 p = sa[r];
+      rank[p] = static_cast<u32>(running_max);
+      if (!(head[i] && head[i + 1])) active[out++] = p;
+    }
+  }
+  const u64 tiles = (n + kScanTile - 1) / kScanTile;
+  if (tile == tiles - 1 && threadIdx.x == 0) *active_count = tile_prefix[1] + agg_sum;
+}
+
+// Round step 1: composite keys for the active list.  counters: *group_count
+// receives the number of groups G.  ghead/gstart are indexed by dense id.
+__global__ void __launch_bounds__(kScanBlock)
+round_keys_kernel(const u32* __restrict__ active, u64 count,
+                  const u32* __restrict__ rank, u64 h, Segments segs,
+                  u32 second_bits, u64* __restrict__ ckey,
+                  u32* __restrict__ cval, u32* __restrict__ ghead,
+                  u32* __restrict__ gstart, u64 group_cap, u64* status_sum,
+                  u32* tile_counter, u64* group_count, DeviceFlags* flags) {
+  __shared__ u64 warp_smem[kScanBlock / 32];
+  __shared__ u64 tile_prefix;
+  __shared__ u32 tile_slot;
+  const u32 tile = claim_tile(tile_counter, &tile_slot);
+  const u64 a0 = static_cast<u64>(tile) * kScanTile + threadIdx.x * kScanItems;
+
+  u32 pos[kScanItems];
+  u32 grp[kScanItems];
+  bool start[kScanItems];
+  u32 prev_group = 0xffffffffu;
+  if (a0 > 0 && a0 <= count) prev_group = rank[active[a0 - 1]];
+  u32 starts = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const u64 a = a0 + i;
+    if (a < count) {
+      pos[i] = active[a];
+      grp[i] = rank[pos[i]];
+      start[i] = a == 0 || grp[i] != prev_group;
+      prev_group = grp[i];
+      starts += start[i];
+    } else {
+      start[i] = false;
+    }
+  }
+  u64 agg;
+  const u64 excl = block_exclusive_scan<kScanBlock>(starts, SumOp{}, warp_smem, &agg);
+  if ((threadIdx.x >> 5) == 0) {
+    const u64 p = warp_lookback(status_sum, tile, agg, SumOp{}, flags, 4);
+    if ((threadIdx.x & 31) == 0) tile_prefix = p;
+  }
+  __syncthreads();
+  u64 dense = tile_prefix + excl;  // number of group starts before this item
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const u64 a = a0 + i;
+    if (a < count) {
+      if (start[i]) {
+        if (dense < group_cap) {
+          ghead[dense] = grp[i];
+          gstart[dense] = static_cast<u32>(a);
+        } else {
+          flag_error(flags, kErrBounds);
+        }
+        ++dense;
+      }
+      const u64 p = pos[i];
+      const u64 q = p + h;
+      const u64 second = q < segment_end(segs, p) ? static_cast<u64>(rank[q]) + 1 : 0;
+      ckey[a] = ((dense - 1) << second_bits) | second;
+      cval[a] = static_cast<u32>(p);
+    }
+  }
+  const u64 tiles = (count + kScanTile - 1) / kScanTile;
+  if (tile == tiles - 1 && threadIdx.x == 0) *group_count = tile_prefix + agg;
+}
+
+// Round step 2 (after sorting the composite keys): new heads, SA rows, ranks,
+// and the next active list.
+__global__ void __launch_bounds__(kScanBlock)
+round_rank_kernel(const u64* __restrict__ ckey, const u32* __restrict__ cval,
+                  u64 count, u32 second_bits, const u32* __restrict__ ghead,
+                  const u32* __restrict__ gstart, u64 group_cap, u64 rows,
+                  u32* __restrict__ sa,
+                  u32* __restrict__ rank, u32* __restrict__ next_active,
+                  u64* status_max, u64* status_sum, u32* tile_counter,
+                  u64* next_count, DeviceFlags* flags) {
+  __shared__ u64 warp_smem[kScanBlock / 32];
+  __shared__ u64 tile_prefix[2];
+  __shared__ u32 tile_slot;
+  const u32 tile = claim_tile(tile_counter, &tile_slot);
+  const u64 a0 = static_cast<u64>(tile) * kScanTile + threadIdx.x * kScanItems;
+
+  u64 k[kScanItems + 2];
+#pragma unroll
+  for (int i = 0; i < kScanItems + 2; ++i) {
+    const long long a = static_cast<long long>(a0) - 1 + i;
+    k[i] = (a >= 0 && static_cast<u64>(a) < count) ? ckey[a] : ~0ull;
+  }
+  bool head[kScanItems + 1];
+#pragma unroll
+  for (int i = 0; i < kScanItems + 1; ++i) {
+    const u64 a = a0 + i;
+    head[i] = a >= count || a == 0 || k[i + 1] != k[i];
+  }
+  u64 head_max = 0;
+  u32 keep = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const u64 a = a0 + i;
+    if (a < count) {
+      if (head[i]) head_max = a;
+      if (!(head[i] && head[i + 1])) ++keep;
+    }
+  }
+  u64 agg_max, agg_sum;
+  const u64 excl_max = block_exclusive_scan<kScanBlock>(head_max, MaxOp{}, warp_smem, &agg_max);
+  const u64 excl_sum = block_exclusive_scan<kScanBlock>(keep, SumOp{}, warp_smem, &agg_sum);
+  const u32 warp = threadIdx.x >> 5;
+  if (warp == 0) {
+    const u64 p = warp_lookback(status_max, tile, agg_max, MaxOp{}, flags, 5);
+    if ((threadIdx.x & 31) == 0) tile_prefix[0] = p;
+  } else if (warp == 1) {
+    const u64 p = warp_lookback(status_sum, tile, agg_sum, SumOp{}, flags, 6);
+    if ((threadIdx.x & 31) == 0) tile_prefix[1] = p;
+  }
+  __syncthreads();
+  u64 sub_start = tile_prefix[0] > excl_max ? tile_prefix[0] : excl_max;
+  u64 out = tile_prefix[1] + excl_sum;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const u64 a = a0 + i;
+    if (a < count) {
+      if (head[i]) sub_start = a;
+      const u64 dense = k[i + 1] >> second_bits;
+      if (dense >= group_cap) {
+        flag_error(flags, kErrBounds);
+        continue;
+      }
+      const u32 group_head = ghead[dense];
+      const u32 group_first = gstart[dense];
+      const u32 p = cval[a];
+      const u64 row = group_head + (a - group_first);
+      if (row >= rows || p >= rows || a < group_first) {
+        flag_error(flags, kErrBounds);
+        continue;
+      }
+      sa[row] = p;
+      rank[p] = static_cast<u32>(group_head + (sub_start - group_first));
+      if (!(head[i] && head[i + 1])) next_active[out++] = p;
+    }
+  }
+  const u64 tiles = (count + kScanTile - 1) / kScanTile;
+  if (tile == tiles - 1 && threadIdx.x == 0) *next_count = tile_prefix[1] + agg_sum;
+}
+
+}  // namespace sufgpu

@@ -1,0 +1,873 @@
+// sufgpu engine: context, device memory plan, build orchestration and the
+// C ABI declared in include/sufgpu/sufgpu.h.
+//
+// Device layout for a build of n symbols (all coordinates 32-bit):
+//   text  n+pad bytes      rank  4n (head row of each position's group; = ISA)
+//   sa    4n               k0,k1 8n each (sort keys; later PHI/PLCP/LCP)
+//   v0    4n               x,y   4n each (active lists, group tables, queues)
+// plus look-back status words and radix histograms.  About 37n bytes in all.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/sufgpu/sufgpu.h"
+#include "common.cuh"
+#include "doubling.cuh"
+#include "lcp.cuh"
+#include "pack.cuh"
+#include "radix.cuh"
+
+using namespace sufgpu;
+
+namespace {
+
+constexpr u64 kTextPad = 64;
+constexpr u32 kMaxSegmentsPerLaunch = 8192;
+
+struct CudaError {
+  cudaError_t code;
+  const char* what;
+};
+
+#define SG_CUDA(call)                                             \
+  do {                                                            \
+    cudaError_t sg_err_ = (call);                                 \
+    if (sg_err_ != cudaSuccess) throw CudaError{sg_err_, #call};  \
+  } while (0)
+
+struct BuildError {
+  sufgpu_status status;
+  std::string message;
+};
+
+u64 round_up(u64 v, u64 a) { return (v + a - 1) / a * a; }
+
+// One grown-on-demand device allocation carved into named regions.
+struct Arena {
+  void* base = nullptr;
+  u64 bytes = 0;
+  ~Arena() {
+    if (base) cudaFree(base);
+  }
+  void reserve(u64 need) {
+    if (need <= bytes) return;
+    if (base) {
+      cudaFree(base);
+      base = nullptr;
+      bytes = 0;
+    }
+    cudaError_t err = cudaMalloc(&base, need);
+    if (err != cudaSuccess) {
+      cudaGetLastError();
+      base = nullptr;
+      throw BuildError{SUFGPU_BUILD_FAILURE,
+                       "cannot allocate " + std::to_string(need) +
+                           " bytes of device memory: " + cudaGetErrorString(err)};
+    }
+    bytes = need;
+  }
+};
+
+struct Layout {
+  u8* text;
+  u32* rank;
+  u32* sa;
+  u64* k0;
+  u64* k1;
+  u32* v0;
+  u32* x;
+  u32* y;
+  u64* status;       // look-back words: radix (tiles*256) or 2 scan arrays
+  u64 status_words;
+  u32* hist;         // radix histograms [seg][pass][256]
+  u64* digit_start;  // [seg][pass][256]
+  u64* seg_begin;    // count+1
+  u32* seg_tiles;    // count+1
+  u64* sort_begin;   // 2 entries: the active list as one sort segment
+  u32* sort_tiles;   // 2 entries
+  u32* counters;     // tile counters
+  u64* scalars;      // device-written counts
+  u32* alpha;        // 256 byte counts
+  u16* code;         // 256 symbol codes (1..sigma)
+  DeviceFlags* flags;
+  u64 total;
+};
+
+Layout plan_layout(u8* base, u64 n, u32 segments) {
+  Layout l{};
+  u64 off = 0;
+  auto take = [&](u64 bytes) {
+    u8* p = base + off;
+    off += round_up(bytes, 256);
+    return p;
+  };
+  const u64 n4 = std::max<u64>(n, 1) * 4;
+  l.text = take(n + kTextPad);
+  l.rank = reinterpret_cast<u32*>(take(n4));
+  l.sa = reinterpret_cast<u32*>(take(n4));
+  l.k0 = reinterpret_cast<u64*>(take(2 * n4));
+  l.k1 = reinterpret_cast<u64*>(take(2 * n4));
+  l.v0 = reinterpret_cast<u32*>(take(n4));
+  l.x = reinterpret_cast<u32*>(take(n4));
+  l.y = reinterpret_cast<u32*>(take(n4));
+  const u64 radix_tiles = (n + kSortTile - 1) / kSortTile + segments;
+  const u64 scan_tiles = (n + kScanTile - 1) / kScanTile + 1;
+  l.status_words = std::max<u64>(radix_tiles * kRadixDigits, 2 * scan_tiles);
+  l.status = reinterpret_cast<u64*>(take(l.status_words * 8));
+  l.hist = reinterpret_cast<u32*>(take(u64(segments) * kMaxPasses * kRadixDigits * 4));
+  l.digit_start = reinterpret_cast<u64*>(take(u64(segments) * kMaxPasses * kRadixDigits * 8));
+  l.seg_begin = reinterpret_cast<u64*>(take(u64(segments + 1) * 8));
+  l.seg_tiles = reinterpret_cast<u32*>(take(u64(segments + 1) * 4));
+  l.sort_begin = reinterpret_cast<u64*>(take(16));
+  l.sort_tiles = reinterpret_cast<u32*>(take(8));
+  l.counters = reinterpret_cast<u32*>(take(64 * 4));
+  l.scalars = reinterpret_cast<u64*>(take(64 * 8));
+  l.alpha = reinterpret_cast<u32*>(take(256 * 4));
+  l.code = reinterpret_cast<u16*>(take(512));
+  l.flags = reinterpret_cast<DeviceFlags*>(take(sizeof(DeviceFlags)));
+  l.total = off;
+  return l;
+}
+
+u64 sort_smem_bytes() { return sizeof(OnesweepSmem); }
+
+}  // namespace
+
+struct PendingLaunch {
+  const char* name;
+  u64 bytes;
+  cudaEvent_t before, after;
+};
+
+struct KernelTotals {
+  std::string name;
+  u64 launches = 0;
+  double seconds = 0;
+  u64 bytes = 0;
+};
+
+// Reusable CUDA events for the per-kernel profile.
+struct EventPool {
+  std::vector<cudaEvent_t> all;
+  size_t next = 0;
+  cudaEvent_t take() {
+    if (next == all.size()) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) throw CudaError{cudaErrorMemoryAllocation, "cudaEventCreate"};
+      all.push_back(e);
+    }
+    return all[next++];
+  }
+  void reset() { next = 0; }
+  ~EventPool() {
+    for (auto e : all) cudaEventDestroy(e);
+  }
+};
+
+struct sufgpu_ctx {
+  int device = 0;
+  bool profiling = false;
+  EventPool event_pool;
+  std::vector<PendingLaunch> pending;
+  std::vector<KernelTotals> profile;
+  int sm_count = 148;
+  cudaStream_t stream = nullptr;
+  Arena arena;
+  std::string last_error;
+  u64* host_scalars = nullptr;  // pinned readback slots
+  u8* host_small = nullptr;     // pinned staging for small uploads (1 MiB)
+  std::vector<u8> anchor_pos;
+  std::vector<u8> anchor_val;
+  cudaEvent_t ev[8] = {};
+  u32 launches = 0;
+  // Tunables (the autotuner may change them): symbols per seed key (0 = as
+  // many as fit in 64 bits).
+  u32 seed_symbols = 0;
+};
+
+namespace {
+
+struct Engine {
+  sufgpu_ctx& c;
+  Layout L{};
+  std::vector<u64> begin;  // host segment offsets (count+1)
+  u32 segs = 1;
+  u64 n = 0;
+  sufgpu_build_stats st{};
+  // After the doubling: where the sorted SA lives, and the other n-row u32
+  // buffer (free for PHI flags and byte-coded primaries).
+  u32* sa = nullptr;
+  u32* spare = nullptr;
+
+  explicit Engine(sufgpu_ctx& ctx) : c(ctx) {}
+
+  Segments segments() const { return Segments{L.seg_begin, segs}; }
+
+  void sync() { SG_CUDA(cudaStreamSynchronize(c.stream)); }
+
+  u64 read_scalar(int slot) {
+    SG_CUDA(cudaMemcpyAsync(c.host_scalars + slot, L.scalars + slot, 8,
+                            cudaMemcpyDeviceToHost, c.stream));
+    sync();
+    return c.host_scalars[slot];
+  }
+
+  void upload(void* dst, const void* src, u64 bytes) {
+    if (bytes <= (1u << 20)) {
+      sync();  // the staging buffer may still feed an earlier copy
+      std::memcpy(c.host_small, src, bytes);
+      SG_CUDA(cudaMemcpyAsync(dst, c.host_small, bytes, cudaMemcpyHostToDevice, c.stream));
+    } else {
+      SG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c.stream));
+    }
+  }
+
+  void zero(void* p, u64 bytes) { SG_CUDA(cudaMemsetAsync(p, 0, bytes, c.stream)); }
+
+  // Launches one kernel on the context stream.  `name` and `bytes` (the
+  // kernel's algorithmic bytes: what it must read and write at minimum) feed
+  // the optional per-kernel profile.
+  template <class K, class... Args>
+  void launch(const char* name, u64 bytes, K kernel, u64 grid, u32 block, u64 smem,
+              Args... args) {
+    if (grid == 0) return;
+    cudaEvent_t before = nullptr, after = nullptr;
+    if (c.profiling) {
+      before = c.event_pool.take();
+      after = c.event_pool.take();
+      SG_CUDA(cudaEventRecord(before, c.stream));
+    }
+    kernel<<<static_cast<unsigned>(grid), block, smem, c.stream>>>(args...);
+    SG_CUDA(cudaGetLastError());
+    ++c.launches;
+    if (c.profiling) {
+      SG_CUDA(cudaEventRecord(after, c.stream));
+      c.pending.push_back(PendingLaunch{name, bytes, before, after});
+    }
+  }
+
+  u64 grid_stride_blocks(u64 work, u32 block) {
+    const u64 want = (work + block - 1) / block;
+    return std::max<u64>(1, std::min<u64>(want, u64(c.sm_count) * 16));
+  }
+
+  // Radix sort (keys, vals) in place over [begin_bit, end_bit) using the
+  // alternates as ping-pong buffers.  seg_begin/seg_tiles must be uploaded.
+  // Returns true when the result ended in the alternate buffers.
+  bool radix_sort(u64* keys, u32* vals, u64* keys_alt, u32* vals_alt,
+                  const u64* seg_begin, const u32* seg_tiles, u32 seg_count,
+                  u32 total_tiles, u64 sort_elems, u32 begin_bit, u32 end_bit,
+                  bool check_needed) {
+    if (end_bit <= begin_bit || total_tiles == 0) return false;
+    const u32 passes = (end_bit - begin_bit + kRadixBits - 1) / kRadixBits;
+    SortSegments ss{seg_begin, seg_tiles, seg_count, total_tiles};
+    const u64 elems = sort_elems;
+    u32 needed[kMaxPasses];
+    for (u32 p = 0; p < passes; ++p) needed[p] = 1;
+    if (check_needed) {
+      zero(L.hist, u64(seg_count) * passes * kRadixDigits * 4);
+      zero(L.counters + 32, 4 * kMaxPasses);
+      launch("radix_histogram", elems * 8, radix_histogram_kernel, total_tiles, kSortBlock, 0,
+             keys, ss, begin_bit, passes, L.hist);
+      launch("radix_offsets", u64(seg_count) * passes * kRadixDigits * 12, radix_offsets_kernel,
+             seg_count, kRadixDigits, 0, L.hist, seg_begin, passes, L.digit_start,
+             L.counters + 32);
+      SG_CUDA(cudaMemcpyAsync(c.host_small, L.counters + 32, 4 * passes,
+                              cudaMemcpyDeviceToHost, c.stream));
+      sync();
+      std::memcpy(needed, c.host_small, 4 * passes);
+    } else {
+      zero(L.hist, u64(seg_count) * passes * kRadixDigits * 4);
+      launch("radix_histogram", elems * 8, radix_histogram_kernel, total_tiles, kSortBlock, 0,
+             keys, ss, begin_bit, passes, L.hist);
+      launch("radix_offsets", u64(seg_count) * passes * kRadixDigits * 12, radix_offsets_kernel,
+             seg_count, kRadixDigits, 0, L.hist, seg_begin, passes, L.digit_start,
+             L.counters + 32);
+    }
+    bool swapped = false;
+    u64* kin = keys;
+    u32* vin = vals;
+    u64* kout = keys_alt;
+    u32* vout = vals_alt;
+    for (u32 p = 0; p < passes; ++p) {
+      if (!needed[p]) continue;
+      zero(L.status, u64(total_tiles) * kRadixDigits * 8);
+      zero(L.counters, 4);
+      launch("radix_onesweep", elems * 24, radix_onesweep_kernel, total_tiles, kSortBlock,
+             sort_smem_bytes(),
+             kin, vin, kout, vout, ss, begin_bit + p * kRadixBits, p, passes,
+             L.digit_start, L.status, L.counters, L.flags);
+      std::swap(kin, kout);
+      std::swap(vin, vout);
+      swapped = !swapped;
+    }
+    return swapped;
+  }
+
+  void upload_segments(const std::vector<u64>& b) {
+    std::vector<u32> tiles(b.size());
+    tiles[0] = 0;
+    for (size_t j = 0; j + 1 < b.size(); ++j) {
+      tiles[j + 1] = tiles[j] + static_cast<u32>((b[j + 1] - b[j] + kSortTile - 1) / kSortTile);
+    }
+    std::vector<u8> blob(b.size() * 12);
+    std::memcpy(blob.data(), b.data(), b.size() * 8);
+    std::memcpy(blob.data() + b.size() * 8, tiles.data(), b.size() * 4);
+    sync();
+    std::memcpy(c.host_small, blob.data(), blob.size());
+    SG_CUDA(cudaMemcpyAsync(L.seg_begin, c.host_small, b.size() * 8, cudaMemcpyHostToDevice, c.stream));
+    SG_CUDA(cudaMemcpyAsync(L.seg_tiles, c.host_small + b.size() * 8, b.size() * 4,
+                            cudaMemcpyHostToDevice, c.stream));
+    last_tiles = tiles.back();
+  }
+  u32 last_tiles = 0;
+
+  // ---- the doubling sort: leaves SA in `sa` and ISA (global rows) in rank.
+  void suffix_sort() {
+    // Alphabet remap.
+    zero(L.alpha, 256 * 4);
+    launch("alphabet_histogram", n, alphabet_histogram_kernel,
+           grid_stride_blocks(n / 16 + 1, 256), 256, 0,
+           L.text, n, L.alpha);
+    u32 counts[256];
+    SG_CUDA(cudaMemcpyAsync(c.host_small, L.alpha, sizeof(counts), cudaMemcpyDeviceToHost, c.stream));
+    sync();
+    std::memcpy(counts, c.host_small, sizeof(counts));
+    u16 code[256];
+    u32 sigma = 0;
+    for (int b = 0; b < 256; ++b) code[b] = counts[b] ? static_cast<u16>(++sigma) : 0;
+    const u32 bits = std::max<u32>(1, bits_for(sigma));
+    u32 symbols = 64 / bits;
+    if (c.seed_symbols) symbols = std::min(symbols, c.seed_symbols);
+    st.seed_symbols = symbols;
+    upload(L.code, code, sizeof(code));
+
+    // Seed keys and the segmented seed sort.
+    upload_segments(begin);
+    const u32 seed_tiles = last_tiles;
+    launch("seed_keys", n * 13, seed_keys_kernel, (n + kSeedTile - 1) / kSeedTile, kSeedBlock, 0,
+           L.text, n, segments(), L.code, bits, symbols, L.k0, L.v0);
+    u64* keys = L.k0;
+    const bool swapped = radix_sort(L.k0, L.v0, L.k1, L.sa, L.seg_begin, L.seg_tiles,
+                                    segs, seed_tiles, n, 0, bits * symbols, true);
+    if (swapped) {
+      keys = L.k1;
+      sa = L.sa;
+      spare = L.v0;
+    } else {
+      keys = L.k0;
+      sa = L.v0;
+      spare = L.sa;
+    }
+    // Seed ranks and the initial active list (in x).
+    const u64 scan_tiles = (n + kScanTile - 1) / kScanTile;
+    zero(L.status, 2 * (scan_tiles + 1) * 8);
+    zero(L.counters, 4);
+    u64* status_max = L.status;
+    u64* status_sum = L.status + scan_tiles + 1;
+    launch("seed_rank", n * 16, seed_rank_kernel, scan_tiles, kScanBlock, 0, keys, sa, n,
+           segments(),
+           L.rank, L.x, status_max, status_sum, L.counters, L.scalars + 0, L.flags);
+    u64 active = read_scalar(0);
+
+    // Rounds.  act and other alternate between x and the spare SA-sized
+    // buffer; y holds the per-group tables.
+    u32* act = L.x;
+    u32* other = spare;
+    const u32 second_bits = bits_for(n);
+    u64 h = symbols;
+    u32 rounds = 0;
+    while (active > 0) {
+      if (++rounds > 64) throw BuildError{SUFGPU_BUILD_FAILURE, "prefix doubling did not converge"};
+      st.active_rows += active;
+      const u64 tiles = (active + kScanTile - 1) / kScanTile;
+      u32* ghead = L.y;
+      u32* gstart = L.y + (n - n / 2);  // G <= active/2 <= n/2 entries each
+      zero(L.status, (tiles + 1) * 8);
+      zero(L.counters, 4);
+      launch("round_keys", active * 28, round_keys_kernel, tiles, kScanBlock, 0, act, active,
+             L.rank, h,
+             segments(), second_bits, L.k0, other, ghead, gstart, u64(n / 2),
+             L.status, L.counters, L.scalars + 1, L.flags);
+      // Dense ids are < active/2 (every group has two or more rows).
+      const u32 id_bits = bits_for(active / 2 > 0 ? active / 2 - 1 : 0);
+      const u32 t = static_cast<u32>((active + kSortTile - 1) / kSortTile);
+      const u64 b2[2] = {0, active};
+      const u32 t2[2] = {0, t};
+      std::memcpy(c.host_small + 4096, b2, 16);
+      std::memcpy(c.host_small + 4096 + 16, t2, 8);
+      SG_CUDA(cudaMemcpyAsync(L.sort_begin, c.host_small + 4096, 16, cudaMemcpyHostToDevice, c.stream));
+      SG_CUDA(cudaMemcpyAsync(L.sort_tiles, c.host_small + 4096 + 16, 8, cudaMemcpyHostToDevice, c.stream));
+      const bool sw = radix_sort(L.k0, other, L.k1, act, L.sort_begin, L.sort_tiles, 1, t,
+                                 active, 0, second_bits + id_bits, false);
+      u64* ck = sw ? L.k1 : L.k0;
+      u32* cv = sw ? act : other;
+      u32* next = sw ? other : act;
+      zero(L.status, 2 * (tiles + 1) * 8);
+      zero(L.counters, 4);
+      launch("round_rank", active * 32, round_rank_kernel, tiles, kScanBlock, 0, ck, cv, active,
+             second_bits,
+             ghead, gstart, u64(n / 2), n, sa, L.rank, next, L.status,
+             L.status + tiles + 1,
+             L.counters, L.scalars + 2, L.flags);
+      active = read_scalar(2);  // synchronizes: host_small may be reused
+      other = sw ? act : other;
+      act = next;
+      h *= 2;
+    }
+    st.rounds = rounds;
+  }
+
+  // ---- LCP phase: PLCP in k1 (as u32).  Returns pointer to PLCP.
+  u32* plcp_phase() {
+    u32* phi = reinterpret_cast<u32*>(L.k0);
+    u32* plcp = reinterpret_cast<u32*>(L.k1);
+    u8* irr = reinterpret_cast<u8*>(spare);
+    LongLcpItem* queue = reinterpret_cast<LongLcpItem*>(L.x);
+    const u64 queue_cap = (u64(std::max<u64>(n, 1)) * 8) / sizeof(LongLcpItem);
+    launch("phi", n * 8, phi_kernel, grid_stride_blocks(n, 256), 256, 0, sa, n, segments(), phi);
+    zero(L.scalars + 3, 8);
+    launch("plcp_irreducible", n * 10, plcp_irreducible_kernel, grid_stride_blocks(n, 256), 256,
+           0, L.text, phi,
+           n, segments(), plcp, irr, queue, queue_cap, L.scalars + 3, L.flags);
+    launch("long_lcp", 0, long_lcp_kernel, u64(c.sm_count) * 8, 256, 0, L.text, queue,
+           L.scalars + 3, queue_cap, segments(), plcp);
+    const u64 tiles = (n + kScanTile - 1) / kScanTile;
+    zero(L.status, (tiles + 1) * 8);
+    zero(L.counters, 4);
+    launch("plcp_propagate", n * 5, plcp_propagate_kernel, tiles, kScanBlock, 0, irr, n, plcp,
+           L.status,
+           L.counters, L.flags);
+    return plcp;
+  }
+};
+
+sufgpu_status fail(sufgpu_ctx* ctx, sufgpu_status s, const std::string& m) {
+  if (ctx) ctx->last_error = m;
+  return s;
+}
+
+bool valid_width(u32 bits) { return bits == 32 || bits == 40 || bits == 48 || bits == 64; }
+
+// Copies `bytes` from device src to dst (host or device) on the stream.
+void copy_out(sufgpu_ctx& c, void* dst, const void* src, u64 bytes) {
+  if (!dst || bytes == 0) return;
+  SG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, c.stream));
+}
+
+u64 plane_bytes(u32 bits, u64 rows) { return rows * (bits == 64 ? 8 : 4); }
+u64 high_bytes(u32 bits, u64 rows) { return bits == 40 ? rows : bits == 48 ? 2 * rows : 0; }
+
+// Shared build body for one or many instances (already concatenated in
+// L.text).  outs[j] receives instance j's planes.
+void run_build(Engine& e, const sufgpu_build_desc& d, sufgpu_outputs* outs,
+               sufgpu_anchors* anchors, u32 count) {
+  sufgpu_ctx& c = e.c;
+  Layout& L = e.L;
+  const u64 n = e.n;
+  SG_CUDA(cudaEventRecord(c.ev[1], c.stream));
+  e.suffix_sort();
+  SG_CUDA(cudaEventRecord(c.ev[2], c.stream));
+
+  // ISA: rank holds global rows.  Stage packed planes in k0/k1 when the
+  // layout differs from the device one, then copy each instance's rows.
+  const bool want_isa = d.isa_storage_bits != 0;
+  auto emit = [&](const u32* values, u32 bits, bool isa) {
+    const bool direct = bits == 32 && count == 1;
+    u8* low = reinterpret_cast<u8*>(L.k0);
+    u8* high = reinterpret_cast<u8*>(L.k1);
+    if (!direct) {
+      e.launch("pack", n * (4 + (bits == 64 ? 8 : 4) + high_bytes(bits, 1)), pack_kernel,
+               e.grid_stride_blocks(n, 256), 256, 0, values, n,
+               e.segments(), bits, static_cast<void*>(low), static_cast<void*>(high));
+    }
+    for (u32 j = 0; j < count; ++j) {
+      const u64 b = e.begin[j], rows = e.begin[j + 1] - e.begin[j];
+      void* dst_low = isa ? outs[j].isa_low : outs[j].sa_low;
+      void* dst_high = isa ? outs[j].isa_high : outs[j].sa_high;
+      const u64 w = bits == 64 ? 8 : 4;
+      if (direct) copy_out(c, dst_low, values + b, rows * 4);
+      else copy_out(c, dst_low, low + b * w, rows * w);
+      if (!direct && high_bytes(bits, 1)) {
+        copy_out(c, dst_high, high + b * high_bytes(bits, 1), high_bytes(bits, rows));
+      }
+    }
+  };
+  if (want_isa) emit(L.rank, d.isa_storage_bits, true);
+  SG_CUDA(cudaEventRecord(c.ev[3], c.stream));
+  if (d.flags & SUFGPU_FLAG_VALIDATE) {
+    e.launch("validate", n * 8, validate_kernel, e.grid_stride_blocks(n, 256), 256, 0, e.sa,
+             L.rank,
+             n, e.segments(), L.flags);
+  }
+  emit(e.sa, d.sa_storage_bits, false);
+  SG_CUDA(cudaEventRecord(c.ev[4], c.stream));
+
+  // LCP.
+  if (d.lcp_encoding != SUFGPU_LCP_NONE) {
+    u32* plcp = e.plcp_phase();
+    if (d.lcp_encoding == SUFGPU_LCP_RAW32 || d.lcp_encoding == SUFGPU_LCP_RAW64) {
+      const bool wide = d.lcp_encoding == SUFGPU_LCP_RAW64;
+      if (wide) {
+        e.launch("lcp_gather", n * 16, lcp_gather_kernel<u64>, e.grid_stride_blocks(n, 256), 256, 0,
+                 static_cast<const u32*>(e.sa), static_cast<const u32*>(plcp), n, L.k0);
+      } else {
+        e.launch("lcp_gather", n * 12, lcp_gather_kernel<u32>, e.grid_stride_blocks(n, 256), 256, 0,
+                 static_cast<const u32*>(e.sa), static_cast<const u32*>(plcp), n,
+                 reinterpret_cast<u32*>(L.k0));
+      }
+      const u64 w = wide ? 8 : 4;
+      for (u32 j = 0; j < count; ++j) {
+        const u64 b = e.begin[j], rows = e.begin[j + 1] - e.begin[j];
+        copy_out(c, outs[j].lcp, reinterpret_cast<u8*>(L.k0) + b * w, rows * w);
+      }
+    } else {
+      const bool wide = d.lcp_encoding == SUFGPU_LCP_BYTE64;
+      u8* primary = reinterpret_cast<u8*>(e.spare);
+      e.launch("lcp_primary", n * 9, lcp_primary_kernel, e.grid_stride_blocks(n, 256), 256, 0,
+               static_cast<const u32*>(e.sa), static_cast<const u32*>(plcp), n, primary);
+      for (u32 j = 0; j < count; ++j) {
+        const u64 b = e.begin[j], rows = e.begin[j + 1] - e.begin[j];
+        copy_out(c, outs[j].lcp, primary + b, rows);
+      }
+      // Anchors into x/y (8n bytes).
+      const u64 w = wide ? 8 : 4;
+      const u64 cap = (std::max<u64>(n, 1) * 8) / (2 * w);
+      u8* pos = reinterpret_cast<u8*>(L.x);
+      u8* val = pos + cap * w;
+      const u64 tiles = (n + kScanTile - 1) / kScanTile;
+      e.zero(L.status, (tiles + 1) * 8);
+      e.zero(L.counters, 4);
+      if (wide) {
+        e.launch("anchors", n * 4, anchor_kernel<u64>, tiles, kScanBlock, 0, static_cast<const u32*>(plcp), n,
+                 e.segments(), reinterpret_cast<u64*>(pos), reinterpret_cast<u64*>(val),
+                 cap, L.status, L.counters, L.scalars + 4, L.flags);
+      } else {
+        e.launch("anchors", n * 4, anchor_kernel<u32>, tiles, kScanBlock, 0, static_cast<const u32*>(plcp), n,
+                 e.segments(), reinterpret_cast<u32*>(pos), reinterpret_cast<u32*>(val),
+                 cap, L.status, L.counters, L.scalars + 4, L.flags);
+      }
+      const u64 total = e.read_scalar(4);
+      e.st.anchors = total;
+      if (total > cap) throw BuildError{SUFGPU_BUILD_FAILURE, "anchor buffer overflow"};
+      c.anchor_pos.resize(std::max<u64>(total * w, 8));
+      c.anchor_val.resize(std::max<u64>(total * w, 8));
+      SG_CUDA(cudaMemcpyAsync(c.anchor_pos.data(), pos, total * w, cudaMemcpyDeviceToHost, c.stream));
+      SG_CUDA(cudaMemcpyAsync(c.anchor_val.data(), val, total * w, cudaMemcpyDeviceToHost, c.stream));
+      e.sync();
+      // Anchors arrive in global text order, so each instance owns one
+      // contiguous run; convert its positions to instance coordinates.
+      if (anchors) {
+        u64 at = 0;
+        for (u32 j = 0; j < count; ++j) {
+          const u64 first = at;
+          while (at < total) {
+            const u64 p = wide ? reinterpret_cast<u64*>(c.anchor_pos.data())[at]
+                               : reinterpret_cast<u32*>(c.anchor_pos.data())[at];
+            if (p >= e.begin[j + 1]) break;
+            const u64 local = p - e.begin[j];
+            if (wide) reinterpret_cast<u64*>(c.anchor_pos.data())[at] = local;
+            else reinterpret_cast<u32*>(c.anchor_pos.data())[at] = static_cast<u32>(local);
+            ++at;
+          }
+          anchors[j] = sufgpu_anchors{c.anchor_pos.data() + first * w,
+                                      c.anchor_val.data() + first * w, at - first,
+                                      static_cast<u32>(w * 8)};
+        }
+      }
+    }
+  }
+  SG_CUDA(cudaEventRecord(c.ev[5], c.stream));
+  e.sync();
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+static thread_local std::string g_create_error;
+
+sufgpu_status sufgpu_create(sufgpu_ctx** out, int device) {
+  if (!out) return SUFGPU_INVALID_INPUT;
+  *out = nullptr;
+  auto* ctx = new sufgpu_ctx();
+  try {
+    ctx->device = device;
+    SG_CUDA(cudaSetDevice(device));
+    int sms = 0;
+    SG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    ctx->sm_count = sms;
+    SG_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    SG_CUDA(cudaMallocHost(reinterpret_cast<void**>(&ctx->host_scalars), 64 * 8));
+    SG_CUDA(cudaMallocHost(reinterpret_cast<void**>(&ctx->host_small), 1u << 20));
+    for (auto& ev : ctx->ev) SG_CUDA(cudaEventCreate(&ev));
+    SG_CUDA(cudaFuncSetAttribute(radix_onesweep_kernel,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(sort_smem_bytes())));
+  } catch (const CudaError& err) {
+    g_create_error = std::string("CUDA error in ") + err.what + ": " + cudaGetErrorString(err.code);
+    sufgpu_destroy(ctx);
+    return SUFGPU_BUILD_FAILURE;
+  }
+  *out = ctx;
+  return SUFGPU_OK;
+}
+
+void sufgpu_destroy(sufgpu_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto& ev : ctx->ev) {
+    if (ev) cudaEventDestroy(ev);
+  }
+  if (ctx->host_scalars) cudaFreeHost(ctx->host_scalars);
+  if (ctx->host_small) cudaFreeHost(ctx->host_small);
+  if (ctx->arena.base) {
+    cudaFree(ctx->arena.base);
+    ctx->arena.base = nullptr;
+  }
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+const char* sufgpu_last_error(const sufgpu_ctx* ctx) {
+  return ctx ? ctx->last_error.c_str() : g_create_error.c_str();
+}
+
+uint64_t sufgpu_max_symbols(void) { return 0xffffffffull; }
+
+uint64_t sufgpu_device_bytes(uint64_t n, const sufgpu_build_desc*) {
+  return plan_layout(nullptr, n, 1).total;
+}
+
+void* sufgpu_host_alloc(uint64_t bytes) {
+  void* p = nullptr;
+  if (cudaMallocHost(&p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return p;
+}
+
+void sufgpu_host_free(void* p) {
+  if (p) cudaFreeHost(p);
+}
+
+static sufgpu_status check_desc(sufgpu_ctx* ctx, const sufgpu_build_desc* d) {
+  if (!d) return fail(ctx, SUFGPU_INVALID_INPUT, "build descriptor is null");
+  if (!valid_width(d->sa_storage_bits)) return fail(ctx, SUFGPU_INVALID_INPUT, "invalid SA storage width");
+  if (d->isa_storage_bits && !valid_width(d->isa_storage_bits))
+    return fail(ctx, SUFGPU_INVALID_INPUT, "invalid ISA storage width");
+  if (d->lcp_encoding > SUFGPU_LCP_BYTE64) return fail(ctx, SUFGPU_INVALID_INPUT, "invalid LCP encoding");
+  return SUFGPU_OK;
+}
+
+static sufgpu_status finish(sufgpu_ctx* ctx, Engine& e, sufgpu_build_stats* stats,
+                            std::chrono::steady_clock::time_point t0) {
+  DeviceFlags flags{};
+  SG_CUDA(cudaMemcpy(&flags, e.L.flags, sizeof(flags), cudaMemcpyDeviceToHost));
+  if (flags.error) {
+    char buf[160];
+    std::snprintf(buf, sizeof(buf), "device check failed (flags 0x%x, site %u)", flags.error,
+                  flags.timeout_site);
+    return fail(ctx, SUFGPU_BUILD_FAILURE, buf);
+  }
+  if (ctx->profiling) {
+    for (const auto& p : ctx->pending) {
+      float kms = 0;
+      SG_CUDA(cudaEventElapsedTime(&kms, p.before, p.after));
+      auto it = std::find_if(ctx->profile.begin(), ctx->profile.end(),
+                             [&](const KernelTotals& k) { return k.name == p.name; });
+      if (it == ctx->profile.end()) {
+        ctx->profile.push_back(KernelTotals{p.name});
+        it = ctx->profile.end() - 1;
+      }
+      it->launches += 1;
+      it->seconds += kms / 1e3;
+      it->bytes += p.bytes;
+    }
+    ctx->pending.clear();
+    ctx->event_pool.reset();
+  }
+  if (stats) {
+    float ms = 0;
+    auto span = [&](int a, int b) {
+      cudaEventElapsedTime(&ms, ctx->ev[a], ctx->ev[b]);
+      return ms / 1e3;
+    };
+    e.st.h2d_seconds = span(0, 1);
+    e.st.sa_seconds = span(1, 2);
+    e.st.isa_seconds = span(2, 3);
+    e.st.storage_seconds = span(3, 4);
+    e.st.lcp_seconds = span(4, 5);
+    e.st.device_seconds = span(0, 5);
+    e.st.total_seconds =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    e.st.symbols = e.n;
+    *stats = e.st;
+  }
+  return SUFGPU_OK;
+}
+
+sufgpu_status sufgpu_build(sufgpu_ctx* ctx, const uint8_t* text, uint64_t n,
+                           const sufgpu_build_desc* desc, const sufgpu_outputs* out,
+                           sufgpu_anchors* anchors, sufgpu_build_stats* stats) {
+  if (!ctx) return SUFGPU_INVALID_INPUT;
+  if (auto s = check_desc(ctx, desc)) return s;
+  if (n > sufgpu_max_symbols()) return fail(ctx, SUFGPU_INVALID_INPUT, "text exceeds 2^32-1 symbols");
+  if (n > 0 && !text) return fail(ctx, SUFGPU_INVALID_INPUT, "text is null");
+  if (!out) return fail(ctx, SUFGPU_INVALID_INPUT, "outputs are null");
+  const auto t0 = std::chrono::steady_clock::now();
+  ctx->launches = 0;
+  ctx->pending.clear();
+  ctx->event_pool.reset();
+  if (anchors) *anchors = sufgpu_anchors{nullptr, nullptr, 0, 0};
+  if (n == 0) {
+    if (stats) *stats = sufgpu_build_stats{};
+    return SUFGPU_OK;
+  }
+  try {
+    SG_CUDA(cudaSetDevice(ctx->device));
+    Engine e(*ctx);
+    e.n = n;
+    e.segs = 1;
+    e.begin = {0, n};
+    const Layout probe = plan_layout(nullptr, n, 1);
+    ctx->arena.reserve(probe.total);
+    e.L = plan_layout(static_cast<u8*>(ctx->arena.base), n, 1);
+    SG_CUDA(cudaEventRecord(ctx->ev[0], ctx->stream));
+    e.zero(e.L.flags, sizeof(DeviceFlags));
+    SG_CUDA(cudaMemcpyAsync(e.L.text, text, n, cudaMemcpyDefault, ctx->stream));
+    e.zero(e.L.text + n, kTextPad);
+    sufgpu_outputs o = *out;
+    run_build(e, *desc, &o, anchors, 1);
+    e.st.kernel_launches = ctx->launches;
+    return finish(ctx, e, stats, t0);
+  } catch (const CudaError& err) {
+    cudaGetLastError();
+    return fail(ctx, SUFGPU_BUILD_FAILURE,
+                std::string("CUDA error in ") + err.what + ": " + cudaGetErrorString(err.code));
+  } catch (const BuildError& err) {
+    return fail(ctx, err.status, err.message);
+  } catch (const std::exception& err) {
+    return fail(ctx, SUFGPU_BUILD_FAILURE, err.what());
+  }
+}
+
+int sufgpu_divsufsort64(sufgpu_ctx* ctx, const uint8_t* T, int64_t* SA, int64_t n) {
+  if (!ctx || !T || !SA || n < 0) return -1;
+  if (n <= 1) {
+    if (n == 1) SA[0] = 0;
+    return 0;
+  }
+  sufgpu_build_desc d{64, 0, SUFGPU_LCP_NONE, 0};
+  sufgpu_outputs o{SA, nullptr, nullptr, nullptr, nullptr};
+  return sufgpu_build(ctx, T, static_cast<u64>(n), &d, &o, nullptr, nullptr) == SUFGPU_OK ? 0 : -2;
+}
+
+int sufgpu_divsufsort(sufgpu_ctx* ctx, const uint8_t* T, int32_t* SA, int32_t n) {
+  if (!ctx || !T || !SA || n < 0) return -1;
+  if (n <= 1) {
+    if (n == 1) SA[0] = 0;
+    return 0;
+  }
+  sufgpu_build_desc d{32, 0, SUFGPU_LCP_NONE, 0};
+  sufgpu_outputs o{SA, nullptr, nullptr, nullptr, nullptr};
+  return sufgpu_build(ctx, T, static_cast<u64>(n), &d, &o, nullptr, nullptr) == SUFGPU_OK ? 0 : -2;
+}
+
+}  // extern "C"
+
+extern "C" sufgpu_status sufgpu_build_batch(sufgpu_ctx* ctx, sufgpu_instance* instances,
+                                            uint32_t count, const sufgpu_build_desc* desc,
+                                            sufgpu_build_stats* stats) {
+  if (!ctx) return SUFGPU_INVALID_INPUT;
+  if (auto s = check_desc(ctx, desc)) return s;
+  if (count == 0) {
+    if (stats) *stats = sufgpu_build_stats{};
+    return SUFGPU_OK;
+  }
+  if (!instances) return fail(ctx, SUFGPU_INVALID_INPUT, "instances are null");
+  if (count > kMaxSegmentsPerLaunch) {
+    return fail(ctx, SUFGPU_INVALID_INPUT, "too many instances in one batch launch");
+  }
+  std::vector<u64> begin(count + 1, 0);
+  for (u32 j = 0; j < count; ++j) {
+    if (instances[j].n == 0) return fail(ctx, SUFGPU_INVALID_INPUT, "batch instance is empty");
+    if (!instances[j].text) return fail(ctx, SUFGPU_INVALID_INPUT, "batch instance text is null");
+    begin[j + 1] = begin[j] + instances[j].n;
+    if (begin[j + 1] > sufgpu_max_symbols()) {
+      return fail(ctx, SUFGPU_INVALID_INPUT, "batch exceeds 2^32-1 symbols");
+    }
+  }
+  const auto t0 = std::chrono::steady_clock::now();
+  ctx->launches = 0;
+  ctx->pending.clear();
+  ctx->event_pool.reset();
+  try {
+    SG_CUDA(cudaSetDevice(ctx->device));
+    Engine e(*ctx);
+    e.n = begin[count];
+    e.segs = count;
+    e.begin = begin;
+    const Layout probe = plan_layout(nullptr, e.n, count);
+    ctx->arena.reserve(probe.total);
+    e.L = plan_layout(static_cast<u8*>(ctx->arena.base), e.n, count);
+    SG_CUDA(cudaEventRecord(ctx->ev[0], ctx->stream));
+    e.zero(e.L.flags, sizeof(DeviceFlags));
+    for (u32 j = 0; j < count; ++j) {
+      SG_CUDA(cudaMemcpyAsync(e.L.text + begin[j], instances[j].text, instances[j].n,
+                              cudaMemcpyDefault, ctx->stream));
+    }
+    e.zero(e.L.text + e.n, kTextPad);
+    std::vector<sufgpu_outputs> outs(count);
+    std::vector<sufgpu_anchors> anchors(count);
+    for (u32 j = 0; j < count; ++j) outs[j] = instances[j].out;
+    run_build(e, *desc, outs.data(), anchors.data(), count);
+    for (u32 j = 0; j < count; ++j) instances[j].anchors = anchors[j];
+    e.st.kernel_launches = ctx->launches;
+    return finish(ctx, e, stats, t0);
+  } catch (const CudaError& err) {
+    cudaGetLastError();
+    return fail(ctx, SUFGPU_BUILD_FAILURE,
+                std::string("CUDA error in ") + err.what + ": " + cudaGetErrorString(err.code));
+  } catch (const BuildError& err) {
+    return fail(ctx, err.status, err.message);
+  } catch (const std::exception& err) {
+    return fail(ctx, SUFGPU_BUILD_FAILURE, err.what());
+  }
+}
+
+extern "C" void sufgpu_set_profiling(sufgpu_ctx* ctx, int enable) {
+  if (!ctx) return;
+  ctx->profiling = enable != 0;
+  ctx->profile.clear();
+  ctx->pending.clear();
+  ctx->event_pool.reset();
+}
+
+extern "C" uint32_t sufgpu_profile_count(const sufgpu_ctx* ctx) {
+  return ctx ? static_cast<uint32_t>(ctx->profile.size()) : 0;
+}
+
+extern "C" sufgpu_status sufgpu_profile_entry(const sufgpu_ctx* ctx, uint32_t index,
+                                              const char** name, uint64_t* launches,
+                                              double* seconds, uint64_t* bytes) {
+  if (!ctx || index >= ctx->profile.size()) return SUFGPU_INVALID_INPUT;
+  const auto& k = ctx->profile[index];
+  if (name) *name = k.name.c_str();
+  if (launches) *launches = k.launches;
+  if (seconds) *seconds = k.seconds;
+  if (bytes) *bytes = k.bytes;
+  return SUFGPU_OK;
+}

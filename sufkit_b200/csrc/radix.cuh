@@ -1,0 +1,245 @@
+// Segmented LSD radix sort of (u64 key, u32 value) pairs, onesweep style.
+//
+// Many independent segments (one per reference instance in a batch) are sorted
+// by the same launches: tiles never cross a segment, digit offsets are kept
+// per segment, and the decoupled look-back of a tile stops at its segment's
+// first tile.  One histogram launch counts every digit of every pass at once;
+// each pass is then one launch that ranks a 4096-key tile in shared memory
+// (warp match-any ranking, stable), looks back for its global digit offsets,
+// and scatters through shared memory so that runs of equal digits are written
+// contiguously.
+#pragma once
+
+#include "common.cuh"
+#include "scan.cuh"
+
+namespace sufgpu {
+
+constexpr int kRadixBits = 8;
+constexpr int kRadixDigits = 1 << kRadixBits;
+constexpr int kSortBlock = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortBlock * kSortItems;
+constexpr int kMaxPasses = 8;
+
+struct SortSegments {
+  const u64* begin;       // count+1 element offsets
+  const u32* tile_begin;  // count+1 tile offsets
+  u32 count;
+  u32 total_tiles;
+};
+
+__device__ __forceinline__ void segment_of_tile(const SortSegments& s, u32 tile,
+                                                u32* seg, u64* first,
+                                                u64* last) {
+  u32 lo = 0, hi = s.count;
+  while (hi - lo > 1) {
+    const u32 mid = (lo + hi) >> 1;
+    if (s.tile_begin[mid] <= tile) lo = mid;
+    else hi = mid;
+  }
+  // Skip empty segments that share the tile offset.
+  while (lo + 1 < s.count && s.tile_begin[lo + 1] <= tile) ++lo;
+  *seg = lo;
+  const u64 start = s.begin[lo] + static_cast<u64>(tile - s.tile_begin[lo]) * kSortTile;
+  const u64 end_seg = s.begin[lo + 1];
+  *first = start;
+  *last = start + kSortTile < end_seg ? start + kSortTile : end_seg;
+}
+
+// hist layout: [segment][pass][digit], u32 counts.
+__global__ void __launch_bounds__(kSortBlock)
+radix_histogram_kernel(const u64* __restrict__ keys, SortSegments segs,
+                       u32 begin_bit, u32 passes, u32* __restrict__ hist) {
+  __shared__ u32 local[kMaxPasses][kRadixDigits];
+  for (int i = threadIdx.x; i < kMaxPasses * kRadixDigits; i += kSortBlock) {
+    (&local[0][0])[i] = 0;
+  }
+  __syncthreads();
+  u32 seg;
+  u64 first, last;
+  segment_of_tile(segs, blockIdx.x, &seg, &first, &last);
+  const u32 lane = threadIdx.x & 31;
+  for (int item = 0; item < kSortItems; ++item) {
+    const u64 idx = first + static_cast<u64>(item) * kSortBlock + threadIdx.x;
+    const bool valid = idx < last;
+    const u64 key = valid ? keys[idx] : 0;
+    for (u32 p = 0; p < passes; ++p) {
+      const u32 digit = valid ? static_cast<u32>((key >> (begin_bit + p * kRadixBits)) & 0xff)
+                              : 0x100u;
+      const u32 peers = __match_any_sync(0xffffffffu, digit);
+      if (valid && lane == static_cast<u32>(__ffs(peers) - 1)) {
+        atomicAdd(&local[p][digit], static_cast<u32>(__popc(peers)));
+      }
+    }
+  }
+  __syncthreads();
+  u32* out = hist + static_cast<u64>(seg) * passes * kRadixDigits;
+  for (u32 i = threadIdx.x; i < passes * kRadixDigits; i += kSortBlock) {
+    const u32 c = (&local[0][0])[i];
+    if (c) atomicAdd(&out[i], c);
+  }
+}
+
+// digit_start layout: [segment][pass][digit], absolute u64 element offsets.
+// needed[p] is set when some segment has more than one non-empty digit in
+// pass p (otherwise the pass is the identity and is skipped).
+__global__ void __launch_bounds__(kRadixDigits)
+radix_offsets_kernel(const u32* __restrict__ hist, const u64* __restrict__ begin,
+                     u32 passes, u64* __restrict__ digit_start,
+                     u32* __restrict__ needed) {
+  __shared__ u64 warp_smem[kRadixDigits / 32];
+  __shared__ u32 nonzero;
+  const u32 seg = blockIdx.x;
+  const u32 d = threadIdx.x;
+  for (u32 p = 0; p < passes; ++p) {
+    if (d == 0) nonzero = 0;
+    __syncthreads();
+    const u64 base = (static_cast<u64>(seg) * passes + p) * kRadixDigits;
+    const u32 c = hist[base + d];
+    if (c) atomicAdd(&nonzero, 1u);
+    u64 total;
+    const u64 excl = block_exclusive_scan<kRadixDigits>(c, SumOp{}, warp_smem, &total);
+    digit_start[base + d] = begin[seg] + excl;
+    if (d == 0 && nonzero > 1) atomicOr(&needed[p], 1u);
+    __syncthreads();
+  }
+}
+
+// One LSD pass over bits [shift, shift+8).
+// Shared memory: keys (32 KB) + values (16 KB) + per-warp digit counters.
+struct OnesweepSmem {
+  u64 keys[kSortTile];
+  u32 vals[kSortTile];
+  u32 warp_hist[kSortBlock / 32][kRadixDigits];
+  u32 digit_excl[kRadixDigits];
+  long long digit_gbase[kRadixDigits];
+  u64 warp_scan[kSortBlock / 32];
+  u32 tile;
+};
+
+__global__ void __launch_bounds__(kSortBlock)
+radix_onesweep_kernel(const u64* __restrict__ keys_in,
+                      const u32* __restrict__ vals_in,
+                      u64* __restrict__ keys_out, u32* __restrict__ vals_out,
+                      SortSegments segs, u32 shift, u32 pass, u32 passes,
+                      const u64* __restrict__ digit_start, u64* status,
+                      u32* tile_counter, DeviceFlags* flags) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  OnesweepSmem& sm = *reinterpret_cast<OnesweepSmem*>(smem_raw);
+  constexpr int kWarps = kSortBlock / 32;
+  const u32 lane = threadIdx.x & 31;
+  const u32 warp = threadIdx.x >> 5;
+
+  for (int i = threadIdx.x; i < kWarps * kRadixDigits; i += kSortBlock) {
+    (&sm.warp_hist[0][0])[i] = 0;
+  }
+  const u32 tile = claim_tile(tile_counter, &sm.tile);
+  u32 seg;
+  u64 first, last;
+  segment_of_tile(segs, tile, &seg, &first, &last);
+  const u32 count = static_cast<u32>(last - first);
+  const bool first_tile_of_segment = tile == segs.tile_begin[seg];
+
+  // Warp-striped load: warp w owns tile slots [w*32*ITEMS, (w+1)*32*ITEMS).
+  u64 key[kSortItems];
+  u32 rank[kSortItems];
+  const u32 warp_base = warp * 32 * kSortItems;
+#pragma unroll
+  for (int i = 0; i < kSortItems; ++i) {
+    const u32 slot = warp_base + i * 32 + lane;
+    key[i] = slot < count ? keys_in[first + slot] : ~0ull;
+  }
+  // Stable warp-level ranking by digit; invalid slots never update counters.
+  const u32 lanemask_lt = (1u << lane) - 1;
+#pragma unroll
+  for (int i = 0; i < kSortItems; ++i) {
+    const u32 slot = warp_base + i * 32 + lane;
+    const bool valid = slot < count;
+    const u32 digit = valid ? static_cast<u32>((key[i] >> shift) & 0xff) : 0x100u;
+    const u32 peers = __match_any_sync(0xffffffffu, digit);
+    const u32 leader = __ffs(peers) - 1;
+    u32 base = 0;
+    if (valid && lane == leader) {
+      base = sm.warp_hist[warp][digit];
+      sm.warp_hist[warp][digit] = base + __popc(peers);
+    }
+    base = __shfl_sync(0xffffffffu, base, leader);
+    rank[i] = base + __popc(peers & lanemask_lt);
+    __syncwarp();
+  }
+  __syncthreads();
+
+  // Per digit: exclusive offsets across warps, tile count, tile-local start.
+  const u32 d = threadIdx.x;  // kSortBlock == kRadixDigits
+  u32 digit_count = 0;
+#pragma unroll
+  for (int w = 0; w < kWarps; ++w) {
+    const u32 c = sm.warp_hist[w][d];
+    sm.warp_hist[w][d] = digit_count;
+    digit_count += c;
+  }
+  u64 tile_total;
+  const u64 local_start =
+      block_exclusive_scan<kSortBlock>(digit_count, SumOp{}, sm.warp_scan, &tile_total);
+  sm.digit_excl[d] = static_cast<u32>(local_start);
+
+  // Decoupled look-back, one digit per thread.  Prefix values are absolute
+  // output positions; a segment's first tile seeds them from digit_start.
+  u64* my_status = status + static_cast<u64>(tile) * kRadixDigits + d;
+  u64 global_start;
+  if (first_tile_of_segment) {
+    global_start =
+        digit_start[(static_cast<u64>(seg) * passes + pass) * kRadixDigits + d];
+    store_status(my_status, kFlagPrefix | ((global_start + digit_count) & kValueMask));
+  } else {
+    store_status(my_status, kFlagAggregate | digit_count);
+    u64 exclusive = 0;
+    long long t = static_cast<long long>(tile) - 1;
+    while (true) {
+      const u64 v = wait_status(status + static_cast<u64>(t) * kRadixDigits + d,
+                                flags, 1);
+      exclusive += v & kValueMask;
+      if ((v >> 62) == 2) break;
+      --t;
+    }
+    global_start = exclusive;
+    store_status(my_status, kFlagPrefix | ((global_start + digit_count) & kValueMask));
+  }
+  sm.digit_gbase[d] = static_cast<long long>(global_start) - static_cast<long long>(local_start);
+  __syncthreads();
+
+  // Scatter keys to their tile-local sorted slot, then write runs out.
+  u32 local_slot[kSortItems];
+#pragma unroll
+  for (int i = 0; i < kSortItems; ++i) {
+    const u32 slot = warp_base + i * 32 + lane;
+    if (slot < count) {
+      const u32 digit = static_cast<u32>((key[i] >> shift) & 0xff);
+      local_slot[i] = sm.digit_excl[digit] + sm.warp_hist[warp][digit] + rank[i];
+      sm.keys[local_slot[i]] = key[i];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < kSortItems; ++i) {
+    const u32 slot = warp_base + i * 32 + lane;
+    if (slot < count) sm.vals[local_slot[i]] = vals_in[first + slot];
+  }
+  __syncthreads();
+  const u64 seg_first = segs.begin[seg];
+  const u64 seg_end = segs.begin[seg + 1];
+  for (u32 s = threadIdx.x; s < count; s += kSortBlock) {
+    const u64 k = sm.keys[s];
+    const u32 digit = static_cast<u32>((k >> shift) & 0xff);
+    const u64 out = static_cast<u64>(sm.digit_gbase[digit] + static_cast<long long>(s));
+    if (out < seg_first || out >= seg_end) {  // only after a failed look-back
+      flag_error(flags, kErrBounds);
+      continue;
+    }
+    keys_out[out] = k;
+    vals_out[out] = sm.vals[s];
+  }
+}
+
+}  // namespace sufgpu

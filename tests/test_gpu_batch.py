@@ -1,0 +1,36 @@
+"""GPU: a batch of uneven references equals each reference built alone."""
+import numpy as np
+import pytest
+
+import oracle
+import sufkit_b200 as sg
+from sufkit_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def test_batch_equals_single(ctx):
+    refs = synth.uneven_collection(count=12, scale=0.01)
+    texts = [r.logical_text() for r in refs]
+    texts.append(np.array([0], np.uint8))              # one-symbol instance
+    texts.append(np.full(5000, 6, np.uint8))           # no sentinel, one run
+    texts.append(np.tile(np.array([2, 3], np.uint8), 3000))
+    for lcp in (sg.LcpEncoding.RAW32, sg.LcpEncoding.BYTE32):
+        batch = ctx.build_batch(texts, sa_bits=32, isa_bits=32, lcp=lcp, validate=True)
+        for t, b in zip(texts, batch):
+            s = ctx.build(t, sa_bits=32, isa_bits=32, lcp=lcp)
+            assert (b.sa_low == s.sa_low).all()
+            assert (b.isa_low == s.isa_low).all()
+            assert (b.lcp == s.lcp).all()
+            if lcp == sg.LcpEncoding.BYTE32:
+                assert (b.anchor_positions == s.anchor_positions).all()
+                assert (b.anchor_values == s.anchor_values).all()
+
+
+def test_batch_against_oracle(ctx):
+    rng = np.random.default_rng(11)
+    texts = [synth.random_text(rng, int(n), 4) for n in rng.integers(1, 20000, size=40)]
+    batch = ctx.build_batch(texts, sa_bits=64, isa_bits=0, lcp=sg.LcpEncoding.RAW64)
+    for t, b in zip(texts, batch):
+        sa, isa, lcp = oracle.full_build(t)
+        assert (b.sa_low == sa).all() and (b.lcp == lcp).all()

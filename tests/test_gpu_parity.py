@@ -1,0 +1,154 @@
+"""GPU parity: every build through the C ABI equals the reference's
+divsufsort64 build (SA, ISA, Kasai LCP, byte-coded LCP, packed planes) word
+for word."""
+import numpy as np
+import pytest
+
+import oracle
+import sufkit_b200 as sg
+from sufkit_b200 import synth, verify
+
+pytestmark = pytest.mark.gpu
+
+
+def expected(text):
+    """(sa, isa, lcp) from the reference when built here, else the port."""
+    if oracle.ref() is not None:
+        sa, isa, lcp, _ = oracle.ref_adapter(text, 64)
+        return sa, isa, lcp
+    return oracle.full_build(text)
+
+
+def check_full(ctx, text, sa_bits=32, isa_bits=32, lcp=sg.LcpEncoding.RAW32):
+    text = np.ascontiguousarray(text, np.uint8)
+    sa, isa, lcp_ref = expected(text)
+    r = ctx.build(text, sa_bits=sa_bits, isa_bits=isa_bits, lcp=lcp, validate=True)
+    assert (r.sa == sa).all(), "SA differs"
+    if isa_bits:
+        assert (r.isa == isa).all(), "ISA differs"
+    if lcp in (sg.LcpEncoding.RAW32, sg.LcpEncoding.RAW64):
+        assert (r.lcp.astype(np.uint64) == lcp_ref).all(), "LCP differs"
+    elif lcp in (sg.LcpEncoding.BYTE32, sg.LcpEncoding.BYTE64):
+        width = 32 if lcp == sg.LcpEncoding.BYTE32 else 64
+        primary, pos, val = oracle.bytecode(text, sa, isa, width)
+        assert (r.lcp == primary).all(), "primary bytes differ"
+        assert (r.anchor_positions.astype(np.uint64) == pos).all(), "anchor positions differ"
+        assert (r.anchor_values.astype(np.uint64) == val).all(), "anchor values differ"
+    return r
+
+
+def test_golden_cases(ctx, golden):
+    for name, case in golden.items():
+        t = case["text"]
+        r = ctx.build(t, sa_bits=32, isa_bits=32, lcp=sg.LcpEncoding.RAW32, validate=True)
+        assert (r.sa_low == case["sa"]).all(), name
+        assert (r.isa_low == case["isa"]).all(), name
+        assert (r.lcp == case["lcp"]).all(), name
+        b = ctx.build(t, sa_bits=32, isa_bits=0, lcp=sg.LcpEncoding.BYTE32)
+        assert (b.lcp == case["primary"]).all(), name
+        assert (b.anchor_positions == case["anchor_pos"]).all(), name
+        assert (b.anchor_values == case["anchor_val"]).all(), name
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 15, 16, 17, 255, 4095, 4096, 4097, 65537])
+def test_small_sizes(ctx, n):
+    rng = np.random.default_rng(n)
+    for alphabet in (1, 2, 4):
+        check_full(ctx, synth.random_text(rng, n, alphabet))
+
+
+def test_no_sentinel_arbitrary_bytes(ctx):
+    rng = np.random.default_rng(7)
+    for n in (1, 2, 10, 1000, 50000):
+        check_full(ctx, rng.integers(0, 256, size=n).astype(np.uint8))
+        check_full(ctx, np.full(n, 65, np.uint8))
+        check_full(ctx, np.tile(np.array([1, 2, 1], np.uint8), n)[:n])
+
+
+def test_periodic_and_runs(ctx):
+    # Long runs and short periods force the most doubling rounds.
+    for period in (1, 2, 3, 7, 50):
+        unit = (np.arange(period) % 4 + 2).astype(np.uint8)
+        body = np.tile(unit, 200_000 // period + 1)[:200_000]
+        check_full(ctx, np.concatenate([body, np.array([1, 0], np.uint8)]))
+
+
+@pytest.mark.parametrize("sa_bits", [32, 40, 48, 64])
+def test_storage_widths(ctx, sa_bits):
+    t = synth.plain_4mbp(scale=0.01).logical_text()
+    check_full(ctx, t, sa_bits=sa_bits, isa_bits=sa_bits, lcp=sg.LcpEncoding.RAW64)
+    r = ctx.build(t, sa_bits=sa_bits, isa_bits=sa_bits)
+    if sa_bits in (40, 48):
+        assert r.sa_high is not None and not r.sa_high.any()
+        _, low, high = oracle.pack(r.sa, t.size, sa_bits)
+        assert (low == r.sa_low).all() and (high == r.sa_high).all()
+
+
+@pytest.mark.parametrize("width", [32, 64])
+def test_byte_coded(ctx, width):
+    enc = sg.LcpEncoding.BYTE32 if width == 32 else sg.LcpEncoding.BYTE64
+    t = synth.repeat_rich_100mbp(scale=0.005).logical_text()
+    check_full(ctx, t, isa_bits=0, lcp=enc)
+    # Overflow anchors from long runs and tandem repeats.
+    runs = np.concatenate([np.full(3000, 6, np.uint8), np.array([2, 3], np.uint8),
+                           np.full(1000, 6, np.uint8), np.array([1, 0], np.uint8)])
+    check_full(ctx, runs, isa_bits=0, lcp=enc)
+
+
+def test_workload1_full_size(ctx):
+    """Workload 1 (4,000,005 symbols): word for word against the reference."""
+    t = synth.plain_4mbp().logical_text()
+    r = check_full(ctx, t)
+    assert r.stats["symbols"] == 4_000_005
+
+
+def test_workload2_scaled_word_for_word(ctx):
+    t = synth.repeat_rich_100mbp(scale=0.05).logical_text()
+    check_full(ctx, t)
+
+
+def test_workload2_full_size_properties(ctx):
+    """Workload 2 at 100,000,025 symbols: size-independent exactness checks
+    (permutation, equal prefixes by hash, ordered first mismatch, ISA inverse)."""
+    t = synth.repeat_rich_100mbp().logical_text()
+    r = ctx.build(t, sa_bits=32, isa_bits=32, lcp=sg.LcpEncoding.RAW32, validate=True)
+    verify.check_suffix_array(t, r.sa_low, r.lcp)
+    isa = r.isa_low.astype(np.int64)
+    assert (r.sa_low[isa] == np.arange(t.size)).all()
+
+
+def test_strain_collection_long_lcp(ctx):
+    ref = synth.strain_collection(copies=8, genome_bp=200_000)
+    check_full(ctx, ref.logical_text(), isa_bits=0, lcp=sg.LcpEncoding.BYTE32)
+
+
+def test_divsufsort_dropins(ctx):
+    t = synth.plain_4mbp(scale=0.01).logical_text()
+    sa, _, _ = expected(t)
+    assert (ctx.divsufsort64(t) == sa.astype(np.int64)).all()
+    assert (ctx.divsufsort(t) == sa.astype(np.int32)).all()
+    if oracle.ref() is not None:
+        assert (ctx.divsufsort64(t) == oracle.ref_divsufsort64(t)).all()
+
+
+def test_build_cuda_mirror(ctx):
+    t = synth.plain_4mbp(scale=0.01).logical_text()
+    sa, isa, lcp = expected(t)
+    r64 = sg.build_cuda64(t, 1, True, True, 1)
+    assert r64.suffix_array.dtype == np.int64 and (r64.suffix_array == sa.astype(np.int64)).all()
+    assert (r64.isa == isa).all() and (r64.lcp == lcp).all()
+    r32 = sg.build_cuda32(t, 1, True, False, 1)
+    assert r32.suffix_array.dtype == np.int32 and (r32.lcp == lcp).all()
+    assert r32.isa.size == 0
+    with pytest.raises(sg.SufkitError) as e:
+        sg.build_cuda32(t, 2, True, False, 1)
+    assert e.value.code == sg.ErrorCode.UNSUPPORTED_BACKEND
+
+
+def test_invalid_inputs(ctx):
+    t = np.zeros(4, np.uint8)
+    with pytest.raises(sg.SufkitError) as e:
+        ctx.build(t, sa_bits=33)
+    assert e.value.code == sg.ErrorCode.INVALID_INPUT
+    r = ctx.build(np.zeros(0, np.uint8))
+    assert r.sa_low.size == 0

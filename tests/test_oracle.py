@@ -1,0 +1,96 @@
+"""CPU: the oracle restatement against the reference's golden vectors and,
+where the reference library was built here, against the reference itself."""
+import numpy as np
+import pytest
+
+import oracle
+from sufkit_b200 import synth
+
+
+def test_port_matches_golden(golden):
+    for name, case in golden.items():
+        t = case["text"]
+        sa, isa, lcp = oracle.full_build(t)
+        assert (sa == case["sa"]).all(), name
+        assert (isa == case["isa"]).all(), name
+        assert (lcp == case["lcp"]).all(), name
+        primary, pos, val = oracle.bytecode(t, sa, isa, 32)
+        assert (primary == case["primary"]).all(), name
+        assert (pos == case["anchor_pos"]).all(), name
+        assert (val == case["anchor_val"]).all(), name
+
+
+def test_golden_logical_text_pins_encoding(golden):
+    # tests/test_sufkit.cpp:219-221 (2-contig... 3-record reference.fa)
+    expected = [2, 3, 4, 5, 6, 2, 3, 4, 5, 1, 5, 5, 5, 2, 3, 4, 5, 2, 2, 2, 1, 2, 2, 2, 1, 0]
+    assert golden["reference_fa"]["text"].tolist() == expected
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 7, 64, 1000, 20000])
+def test_port_matches_reference_random(n):
+    if oracle.ref() is None:
+        pytest.skip("reference library not built")
+    rng = np.random.default_rng(n)
+    for alphabet in (1, 2, 4):
+        t = synth.random_text(rng, n, alphabet)
+        sa, isa, lcp, _ = oracle.ref_adapter(t)
+        psa, pisa, plcp = oracle.full_build(t)
+        assert (psa == sa).all() and (pisa == isa).all() and (plcp == lcp).all()
+        for width in (32, 64):
+            a = oracle.bytecode(t, sa, isa, width)
+            b = oracle.ref_bytecode(t, sa, isa, width)
+            for x, y in zip(a, b):
+                assert (x == y).all()
+
+
+def test_port_matches_reference_synthetic():
+    if oracle.ref() is None:
+        pytest.skip("reference library not built")
+    t = synth.plain_4mbp(scale=0.05).logical_text()
+    sa, isa, lcp, _ = oracle.ref_adapter(t)
+    psa, pisa, plcp = oracle.full_build(t)
+    assert (psa == sa).all() and (plcp == lcp).all()
+
+
+def test_bytecode_separate_overflow_runs():
+    # tests/test_lcp_storage.cpp:225-245: LCP {0,300,299,10,400,399} with the
+    # identity ISA opens anchors at 1 and 4 only.  Text order = row order here.
+    lcp = np.array([0, 300, 299, 10, 400, 399], np.uint64)
+    opens = [p for p in range(lcp.size)
+             if lcp[p] >= 255 and not (p > 0 and lcp[p - 1] == lcp[p] + 1)]
+    assert opens == [1, 4]
+    if oracle.ref() is not None:
+        isa = np.arange(6, dtype=np.uint64)
+        _, pos, val = oracle.ref_bytecode_from_raw(lcp, isa, 32)
+        assert pos.tolist() == [1, 4] and val.tolist() == [300, 400]
+
+
+def test_guide_block_boundaries():
+    # tests/test_lcp_storage.cpp:247-272: anchors at 4095, 4096, 8193.
+    pos = np.array([4095, 4096, 8193], np.uint64)
+    g = oracle.guide(pos, 9000)
+    # guide[b] = first anchor at or after b * 4096, b = 0..ceil(9000/4096).
+    assert g.tolist() == [0, 1, 2, 3]
+
+
+@pytest.mark.parametrize("bits", [0, 32, 40, 48, 64])
+def test_pack_matches_reference(bits):
+    if oracle.ref() is None:
+        pytest.skip("reference library not built")
+    rng = np.random.default_rng(bits)
+    symbol_count = {0: 1 << 33, 32: 1 << 32, 40: 1 << 40, 48: 1 << 48, 64: 1 << 50}[bits]
+    v = rng.integers(0, symbol_count, size=5000, dtype=np.uint64)
+    v[:3] = [0, symbol_count - 1, min(symbol_count - 1, 0xFFFFFFFF)]
+    a = oracle.pack(v, symbol_count, bits)
+    b = oracle.ref_pack(v, symbol_count, bits)
+    assert a[0] == b[0]
+    assert (a[1] == b[1]).all()
+    if a[2] is not None:
+        assert (a[2] == b[2]).all()
+
+
+def test_pack_rejects_out_of_range():
+    with pytest.raises(ValueError):
+        oracle.pack(np.array([5], np.uint64), 5, 32)  # value >= symbol count
+    with pytest.raises(ValueError):
+        oracle.pack(np.array([1], np.uint64), (1 << 32) + 2, 32)  # text too big for 32
