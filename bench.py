@@ -42,8 +42,12 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="plain100m",
                     choices=["plain100m", "plain4m", "batched"])
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="shrink the workload (profiling captures only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--tune", action="append", default=[],
+                    help="library tuning knob key=value (sufgpu_set_tuning)")
     return ap.parse_args()
 
 
@@ -58,7 +62,7 @@ def peaks():
 # ---------------------------------------------------------------------------
 # Workloads
 # ---------------------------------------------------------------------------
-def workload(name: str):
+def workload(name: str, scale: float = 1.0):
     from sufkit_b200 import synth
     if name == "plain4m":
         ref = synth.plain_4mbp()
@@ -70,7 +74,7 @@ def workload(name: str):
         desc = ("batched uneven collection sample: 64 bacterial-like references "
                 "(log-normal, median 4 Mbp), SA+raw LCP32 per reference, one batch")
         return [r.logical_text() for r in refs], desc
-    ref = synth.repeat_rich_100mbp()
+    ref = synth.repeat_rich_100mbp(scale)
     desc = ("repeat-rich 100 Mbp plain build: 24 contigs, GC 41%, 25% interspersed "
             "repeats (500 families, 5-15% divergence), 3% tandem repeats, 0.5% N runs; "
             "Fast profile SA+ISA+raw LCP32, 32-bit construction and storage")
@@ -228,7 +232,9 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    texts, desc = workload(args.workload)
+    texts, desc = workload(args.workload, args.scale)
+    if args.scale != 1.0:
+        desc += f" (scaled x{args.scale})"
 
     if args.impl == "reference":
         if rank == 0:
@@ -247,6 +253,9 @@ def main():
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     ctx = sg.Context(local)
+    for item in args.tune:
+        key, value = item.split("=", 1)
+        ctx.set_tuning(key, int(value))
     lcp_enc = sg.LcpEncoding.RAW32
     isa_bits = 0 if args.workload == "batched" else 32
 

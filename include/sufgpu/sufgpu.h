@@ -176,6 +176,12 @@ SUFGPU_API sufgpu_status sufgpu_profile_entry(const sufgpu_ctx *ctx, uint32_t in
                                               const char **name, uint64_t *launches,
                                               double *seconds, uint64_t *bytes);
 
+/* Tuning knobs (picked by the autotuner, sufkit_b200/autotune.py):
+ *   "seed_symbols"  symbols packed per seed key, 0 = as many as fit 64 bits;
+ *   "ballot_rank"   1 = onesweep ranks digits with ballots, 0 = match-any.
+ * Results are identical for every setting; only speed changes. */
+SUFGPU_API sufgpu_status sufgpu_set_tuning(sufgpu_ctx *ctx, const char *key, int64_t value);
+
 /* Pinned host memory helpers (fast transfers for callers that can use them). */
 SUFGPU_API void *sufgpu_host_alloc(uint64_t bytes);
 SUFGPU_API void sufgpu_host_free(void *ptr);

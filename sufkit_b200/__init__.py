@@ -121,6 +121,7 @@ _SIGNATURES = {
                                             ctypes.POINTER(ctypes.c_uint64),
                                             ctypes.POINTER(ctypes.c_double),
                                             ctypes.POINTER(ctypes.c_uint64)]),
+    "sufgpu_set_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int64]),
     "sufgpu_host_alloc": (ctypes.c_void_p, [ctypes.c_uint64]),
     "sufgpu_host_free": (None, [ctypes.c_void_p]),
     "sufgpu_encode_fasta": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_uint64,
@@ -318,6 +319,11 @@ class Context:
             results.append(BuildResult(anchor_positions=pos, anchor_values=val,
                                        stats=self.last_stats, **planes))
         return results
+
+    def set_tuning(self, key: str, value: int) -> None:
+        status = self._lib.sufgpu_set_tuning(self._h, key.encode(), int(value))
+        if status != 0:
+            _raise(status, self._error())
 
     def set_profiling(self, enable: bool = True) -> None:
         self._lib.sufgpu_set_profiling(self._h, int(enable))

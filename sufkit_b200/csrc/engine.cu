@@ -190,6 +190,8 @@ struct sufgpu_ctx {
   // Tunables (the autotuner may change them): symbols per seed key (0 = as
   // many as fit in 64 bits).
   u32 seed_symbols = 0;
+  // Onesweep ranking: ballots over digit bits (true) or match-any (false).
+  bool ballot_rank = true;
 };
 
 namespace {
@@ -261,7 +263,7 @@ struct Engine {
   // Radix sort (keys, vals) in place over [begin_bit, end_bit) using the
   // alternates as ping-pong buffers.  seg_begin/seg_tiles must be uploaded.
   // Returns true when the result ended in the alternate buffers.
-  bool radix_sort(u64* keys, u32* vals, u64* keys_alt, u32* vals_alt,
+  bool radix_sort(const char* name, u64* keys, u32* vals, u64* keys_alt, u32* vals_alt,
                   const u64* seg_begin, const u32* seg_tiles, u32 seg_count,
                   u32 total_tiles, u64 sort_elems, u32 begin_bit, u32 end_bit,
                   bool check_needed) {
@@ -300,7 +302,9 @@ struct Engine {
       if (!needed[p]) continue;
       zero(L.status, u64(total_tiles) * kRadixDigits * 8);
       zero(L.counters, 4);
-      launch("radix_onesweep", elems * 24, radix_onesweep_kernel, total_tiles, kSortBlock,
+      launch(name, elems * 24,
+             c.ballot_rank ? radix_onesweep_kernel<true> : radix_onesweep_kernel<false>,
+             total_tiles, kSortBlock,
              sort_smem_bytes(),
              kin, vin, kout, vout, ss, begin_bit + p * kRadixBits, p, passes,
              L.digit_start, L.status, L.counters, L.flags);
@@ -355,7 +359,7 @@ struct Engine {
     launch("seed_keys", n * 13, seed_keys_kernel, (n + kSeedTile - 1) / kSeedTile, kSeedBlock, 0,
            L.text, n, segments(), L.code, bits, symbols, L.k0, L.v0);
     u64* keys = L.k0;
-    const bool swapped = radix_sort(L.k0, L.v0, L.k1, L.sa, L.seg_begin, L.seg_tiles,
+    const bool swapped = radix_sort("seed_onesweep", L.k0, L.v0, L.k1, L.sa, L.seg_begin, L.seg_tiles,
                                     segs, seed_tiles, n, 0, bits * symbols, true);
     if (swapped) {
       keys = L.k1;
@@ -405,7 +409,7 @@ struct Engine {
       std::memcpy(c.host_small + 4096 + 16, t2, 8);
       SG_CUDA(cudaMemcpyAsync(L.sort_begin, c.host_small + 4096, 16, cudaMemcpyHostToDevice, c.stream));
       SG_CUDA(cudaMemcpyAsync(L.sort_tiles, c.host_small + 4096 + 16, 8, cudaMemcpyHostToDevice, c.stream));
-      const bool sw = radix_sort(L.k0, other, L.k1, act, L.sort_begin, L.sort_tiles, 1, t,
+      const bool sw = radix_sort("round_onesweep", L.k0, other, L.k1, act, L.sort_begin, L.sort_tiles, 1, t,
                                  active, 0, second_bits + id_bits, false);
       u64* ck = sw ? L.k1 : L.k0;
       u32* cv = sw ? act : other;
@@ -425,27 +429,65 @@ struct Engine {
     st.rounds = rounds;
   }
 
-  // ---- LCP phase: PLCP in k1 (as u32).  Returns pointer to PLCP.
-  u32* plcp_phase() {
-    u32* phi = reinterpret_cast<u32*>(L.k0);
-    u32* plcp = reinterpret_cast<u32*>(L.k1);
-    u8* irr = reinterpret_cast<u8*>(spare);
-    LongLcpItem* queue = reinterpret_cast<LongLcpItem*>(L.x);
-    const u64 queue_cap = (u64(std::max<u64>(n, 1)) * 8) / sizeof(LongLcpItem);
-    launch("phi", n * 8, phi_kernel, grid_stride_blocks(n, 256), 256, 0, sa, n, segments(), phi);
-    zero(L.scalars + 3, 8);
-    launch("plcp_irreducible", n * 10, plcp_irreducible_kernel, grid_stride_blocks(n, 256), 256,
-           0, L.text, phi,
-           n, segments(), plcp, irr, queue, queue_cap, L.scalars + 3, L.flags);
-    launch("long_lcp", 0, long_lcp_kernel, u64(c.sm_count) * 8, 256, 0, L.text, queue,
-           L.scalars + 3, queue_cap, segments(), plcp);
-    const u64 tiles = (n + kScanTile - 1) / kScanTile;
-    zero(L.status, (tiles + 1) * 8);
-    zero(L.counters, 4);
-    launch("plcp_propagate", n * 5, plcp_propagate_kernel, tiles, kScanBlock, 0, irr, n, plcp,
-           L.status,
-           L.counters, L.flags);
-    return plcp;
+  // ---- LCP phase: final row-order LCP (u32) in the first half of k1.  The
+  // position-sorted long irreducible rows stay in k0 (positions) and the
+  // second half of k1 (values) for the anchor pass; their count is returned.
+  struct LcpPhase {
+    u32* lcp;
+    const u64* sorted_pos;
+    const u32* sorted_val;
+    u64 longs;
+  };
+  LcpPhase lcp_phase() {
+    u32* lcp = reinterpret_cast<u32*>(L.k1);
+    LongRow* longs = reinterpret_cast<LongRow*>(L.x);  // x and y: 8n bytes
+    const u64 long_cap = std::max<u64>(n, 1) * 8 / sizeof(LongRow);
+    u32* pending = spare;
+    const u64 pending_cap = n;
+    zero(L.scalars + 5, 16);
+    launch("lcp_rows", n * 13, lcp_rows_kernel, grid_stride_blocks(n, 256), 256, 0, L.text,
+           static_cast<const u32*>(sa), n, segments(), lcp, longs, long_cap, L.scalars + 5,
+           pending, pending_cap, L.scalars + 6, L.flags);
+    SG_CUDA(cudaMemcpyAsync(c.host_scalars + 5, L.scalars + 5, 16, cudaMemcpyDeviceToHost, c.stream));
+    sync();
+    const u64 q_all = c.host_scalars[5], pend_all = c.host_scalars[6];
+    if (q_all > long_cap || pend_all > pending_cap) {
+      throw BuildError{SUFGPU_BUILD_FAILURE, "long-LCP queue overflow"};
+    }
+    const u64 q = q_all;
+    st.irreducible_long = q;
+    u64* spos = L.k0;
+    u64* spos_alt = L.k0 + n / 2 + 1;
+    u32* sval = reinterpret_cast<u32*>(L.k1) + n;
+    u32* sval_alt = sval + n / 2 + 1;
+    const u64* sorted_pos = spos;
+    const u32* sorted_val = sval;
+    if (q > 0) {
+      launch("long_rows", 0, long_rows_kernel, u64(c.sm_count) * 8, 256, 0, L.text,
+             static_cast<const LongRow*>(longs), static_cast<const u64*>(L.scalars + 5),
+             long_cap, segments(), lcp, spos, sval);
+      const u32 t = static_cast<u32>((q + kSortTile - 1) / kSortTile);
+      const u64 b2[2] = {0, q};
+      const u32 t2[2] = {0, t};
+      std::memcpy(c.host_small + 4096, b2, 16);
+      std::memcpy(c.host_small + 4096 + 16, t2, 8);
+      SG_CUDA(cudaMemcpyAsync(L.sort_begin, c.host_small + 4096, 16, cudaMemcpyHostToDevice, c.stream));
+      SG_CUDA(cudaMemcpyAsync(L.sort_tiles, c.host_small + 4096 + 16, 8, cudaMemcpyHostToDevice, c.stream));
+      const bool sw = radix_sort("long_sort", spos, sval, spos_alt, sval_alt, L.sort_begin,
+                                 L.sort_tiles, 1, t, q, 0, std::max<u32>(1, bits_for(n)), false);
+      if (sw) {
+        sorted_pos = spos_alt;
+        sorted_val = sval_alt;
+      }
+    }
+    if (pend_all > 0) {
+      if (q == 0) throw BuildError{SUFGPU_BUILD_FAILURE, "reducible long row without an anchor row"};
+      launch("pending_rows", pend_all * 16, pending_rows_kernel, grid_stride_blocks(pend_all, 256),
+             256, 0, static_cast<const u32*>(sa), static_cast<const u32*>(pending),
+             static_cast<const u64*>(L.scalars + 6), pending_cap, sorted_pos, sorted_val,
+             static_cast<const u64*>(L.scalars + 5), long_cap, lcp, L.flags);
+    }
+    return LcpPhase{lcp, sorted_pos, sorted_val, q};
   }
 };
 
@@ -512,47 +554,50 @@ void run_build(Engine& e, const sufgpu_build_desc& d, sufgpu_outputs* outs,
 
   // LCP.
   if (d.lcp_encoding != SUFGPU_LCP_NONE) {
-    u32* plcp = e.plcp_phase();
+    const Engine::LcpPhase ph = e.lcp_phase();
     if (d.lcp_encoding == SUFGPU_LCP_RAW32 || d.lcp_encoding == SUFGPU_LCP_RAW64) {
       const bool wide = d.lcp_encoding == SUFGPU_LCP_RAW64;
+      const u8* src = reinterpret_cast<const u8*>(ph.lcp);
       if (wide) {
-        e.launch("lcp_gather", n * 16, lcp_gather_kernel<u64>, e.grid_stride_blocks(n, 256), 256, 0,
-                 static_cast<const u32*>(e.sa), static_cast<const u32*>(plcp), n, L.k0);
-      } else {
-        e.launch("lcp_gather", n * 12, lcp_gather_kernel<u32>, e.grid_stride_blocks(n, 256), 256, 0,
-                 static_cast<const u32*>(e.sa), static_cast<const u32*>(plcp), n,
-                 reinterpret_cast<u32*>(L.k0));
+        e.launch("lcp_widen", n * 12, widen_kernel<u64>, e.grid_stride_blocks(n, 256), 256, 0,
+                 static_cast<const u32*>(ph.lcp), n, L.k0);
+        src = reinterpret_cast<const u8*>(L.k0);
       }
       const u64 w = wide ? 8 : 4;
       for (u32 j = 0; j < count; ++j) {
         const u64 b = e.begin[j], rows = e.begin[j + 1] - e.begin[j];
-        copy_out(c, outs[j].lcp, reinterpret_cast<u8*>(L.k0) + b * w, rows * w);
+        copy_out(c, outs[j].lcp, src + b * w, rows * w);
       }
     } else {
       const bool wide = d.lcp_encoding == SUFGPU_LCP_BYTE64;
       u8* primary = reinterpret_cast<u8*>(e.spare);
-      e.launch("lcp_primary", n * 9, lcp_primary_kernel, e.grid_stride_blocks(n, 256), 256, 0,
-               static_cast<const u32*>(e.sa), static_cast<const u32*>(plcp), n, primary);
+      e.launch("lcp_primary", n * 5, lcp_primary_kernel, e.grid_stride_blocks(n, 256), 256, 0,
+               static_cast<const u32*>(ph.lcp), n, primary);
       for (u32 j = 0; j < count; ++j) {
         const u64 b = e.begin[j], rows = e.begin[j + 1] - e.begin[j];
         copy_out(c, outs[j].lcp, primary + b, rows);
       }
-      // Anchors into x/y (8n bytes).
+      // Anchors into x/y (8n bytes): a filter of the sorted long rows.
       const u64 w = wide ? 8 : 4;
       const u64 cap = (std::max<u64>(n, 1) * 8) / (2 * w);
       u8* pos = reinterpret_cast<u8*>(L.x);
       u8* val = pos + cap * w;
-      const u64 tiles = (n + kScanTile - 1) / kScanTile;
+      const u64 tiles = (ph.longs + kScanTile - 1) / kScanTile;
+      e.zero(L.scalars + 4, 8);
       e.zero(L.status, (tiles + 1) * 8);
       e.zero(L.counters, 4);
       if (wide) {
-        e.launch("anchors", n * 4, anchor_kernel<u64>, tiles, kScanBlock, 0, static_cast<const u32*>(plcp), n,
-                 e.segments(), reinterpret_cast<u64*>(pos), reinterpret_cast<u64*>(val),
-                 cap, L.status, L.counters, L.scalars + 4, L.flags);
+        e.launch("anchors", ph.longs * 24, anchor_kernel<u64>, tiles, kScanBlock, 0,
+                 ph.sorted_pos, ph.sorted_val, static_cast<const u64*>(L.scalars + 5),
+                 n, e.segments(), static_cast<const u32*>(L.rank),
+                 static_cast<const u32*>(ph.lcp), reinterpret_cast<u64*>(pos),
+                 reinterpret_cast<u64*>(val), cap, L.status, L.counters, L.scalars + 4, L.flags);
       } else {
-        e.launch("anchors", n * 4, anchor_kernel<u32>, tiles, kScanBlock, 0, static_cast<const u32*>(plcp), n,
-                 e.segments(), reinterpret_cast<u32*>(pos), reinterpret_cast<u32*>(val),
-                 cap, L.status, L.counters, L.scalars + 4, L.flags);
+        e.launch("anchors", ph.longs * 24, anchor_kernel<u32>, tiles, kScanBlock, 0,
+                 ph.sorted_pos, ph.sorted_val, static_cast<const u64*>(L.scalars + 5),
+                 n, e.segments(), static_cast<const u32*>(L.rank),
+                 static_cast<const u32*>(ph.lcp), reinterpret_cast<u32*>(pos),
+                 reinterpret_cast<u32*>(val), cap, L.status, L.counters, L.scalars + 4, L.flags);
       }
       const u64 total = e.read_scalar(4);
       e.st.anchors = total;
@@ -611,7 +656,10 @@ sufgpu_status sufgpu_create(sufgpu_ctx** out, int device) {
     SG_CUDA(cudaMallocHost(reinterpret_cast<void**>(&ctx->host_scalars), 64 * 8));
     SG_CUDA(cudaMallocHost(reinterpret_cast<void**>(&ctx->host_small), 1u << 20));
     for (auto& ev : ctx->ev) SG_CUDA(cudaEventCreate(&ev));
-    SG_CUDA(cudaFuncSetAttribute(radix_onesweep_kernel,
+    SG_CUDA(cudaFuncSetAttribute(radix_onesweep_kernel<true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(sort_smem_bytes())));
+    SG_CUDA(cudaFuncSetAttribute(radix_onesweep_kernel<false>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(sort_smem_bytes())));
   } catch (const CudaError& err) {
@@ -869,5 +917,19 @@ extern "C" sufgpu_status sufgpu_profile_entry(const sufgpu_ctx* ctx, uint32_t in
   if (launches) *launches = k.launches;
   if (seconds) *seconds = k.seconds;
   if (bytes) *bytes = k.bytes;
+  return SUFGPU_OK;
+}
+
+extern "C" sufgpu_status sufgpu_set_tuning(sufgpu_ctx* ctx, const char* key, int64_t value) {
+  if (!ctx || !key) return SUFGPU_INVALID_INPUT;
+  const std::string k(key);
+  if (k == "seed_symbols") {
+    if (value < 0 || value > 64) return fail(ctx, SUFGPU_INVALID_INPUT, "seed_symbols out of range");
+    ctx->seed_symbols = static_cast<u32>(value);
+  } else if (k == "ballot_rank") {
+    ctx->ballot_rank = value != 0;
+  } else {
+    return fail(ctx, SUFGPU_INVALID_INPUT, "unknown tuning key " + k);
+  }
   return SUFGPU_OK;
 }

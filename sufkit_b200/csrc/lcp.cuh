@@ -1,13 +1,23 @@
-// LCP kernels: PHI, irreducible PLCP, propagation, row-order gather, byte
-// coding (primary bytes + text-ordered overflow anchors).
+// LCP kernels (row order), byte coding and overflow anchors.
 //
-// PLCP[i] = lcp(i, phi[i]) where phi[i] is the suffix just before i in SA
-// order.  A position is reducible when text[i-1] == text[phi[i]-1]; then
-// phi[i-1] = phi[i] - 1 and PLCP[i] = PLCP[i-1] - 1 exactly.  Only irreducible
-// positions compare text (their total is O(n log n) and close to n on genomic
-// text); every reducible PLCP follows from the nearest irreducible position r
-// before it as PLCP[r] - (i - r).  This gives the same values as the
-// reference's sequential Kasai loop without its carry chain.
+// LCP[r] = lcp(SA[r-1], SA[r]).  Every row first compares up to 64 bytes
+// directly (on genomic text almost every row ends there; the text is read
+// through L2).  A row whose first 64 bytes match is "long":
+//   * if its suffix b = SA[r] is irreducible (text[b-1] != text[a-1] for
+//     a = SA[r-1], or b or a starts its instance), a warp finishes the compare;
+//   * otherwise b is reducible: PLCP[b] = PLCP[b-1] - 1, and by induction
+//     PLCP[b] = PLCP[p] - (b - p) for the nearest irreducible text position
+//     p < b.  That p has PLCP[p] >= PLCP[b] + (b - p) > 64, so it is one of the
+//     long irreducible rows; after those are sorted by position a binary search
+//     finds it.
+// This reaches the values of the reference's Kasai loop (src/divsufsort_
+// backend.cpp:121-150) without a text-order carry chain, without the PHI
+// scatter and without a row-order gather; only long rows touch a queue.
+//
+// Byte-coded overflow anchors (src/lcp_storage.cpp:394-412) open at text
+// positions p with PLCP[p] >= 255 that do not continue the run of p-1.  A
+// reducible p always continues, so anchors are a filter of the sorted long
+// irreducible rows: p opens unless PLCP[p-1] == PLCP[p] + 1.
 #pragma once
 
 #include "common.cuh"
@@ -27,205 +37,205 @@ __device__ __forceinline__ u64 load8(const u8* __restrict__ text, u64 pos) {
   return (lo >> s) | (hi << (64 - s));
 }
 
-__global__ void __launch_bounds__(256)
-phi_kernel(const u32* __restrict__ sa, u64 n, Segments segs,
-           u32* __restrict__ phi) {
-  const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
-  for (u64 r = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; r < n; r += stride) {
-    const u32 p = sa[r];
-    phi[p] = is_segment_start(segs, r) ? kNone : sa[r - 1];
-  }
-}
+constexpr u32 kDirectLcpBytes = 64;
 
-// Thread-level compare budget before a position is handed to a warp.
-constexpr u32 kThreadLcpBytes = 64;
-
-struct LongLcpItem {
-  u32 i, j;
-  u64 done;  // bytes already known equal
+struct LongRow {
+  u32 row;   // SA row
+  u32 pos;   // suffix position b = SA[row]
+  u32 prev;  // a = SA[row - 1]
+  u32 done;  // bytes known equal
 };
 
+// Warp-aggregated append of one item per participating lane.
+__device__ __forceinline__ u64 warp_append(u64* counter, bool take) {
+  const u32 mask = __ballot_sync(0xffffffffu, take);
+  if (!mask) return 0;
+  const u32 lane = threadIdx.x & 31;
+  const u32 leader = __ffs(mask) - 1;
+  u64 base = 0;
+  if (lane == leader) base = atomicAdd(reinterpret_cast<unsigned long long*>(counter), __popc(mask));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  return base + __popc(mask & ((1u << lane) - 1));
+}
+
+// Row pass.  lcp receives final values for short rows; long rows go to the
+// irreducible queue or the pending (reducible) list.
 __global__ void __launch_bounds__(256)
-plcp_irreducible_kernel(const u8* __restrict__ text, const u32* __restrict__ phi,
-                        u64 n, Segments segs, u32* __restrict__ plcp,
-                        u8* __restrict__ irreducible, LongLcpItem* queue,
-                        u64 queue_cap, u64* queue_count, DeviceFlags* flags) {
+lcp_rows_kernel(const u8* __restrict__ text, const u32* __restrict__ sa, u64 n,
+                Segments segs, u32* __restrict__ lcp, LongRow* __restrict__ longs,
+                u64 long_cap, u64* long_count, u32* __restrict__ pending,
+                u64 pending_cap, u64* pending_count, DeviceFlags* flags) {
   const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
-  for (u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
-    const u32 j = phi[i];
-    if (j == kNone) {
-      plcp[i] = 0;
-      irreducible[i] = 1;
-      continue;
-    }
-    const u64 seg_first = segs.count == 1 ? 0 : segs.begin[find_segment(segs.begin, segs.count, i)];
-    const bool irr = i == seg_first || j == seg_first || text[i - 1] != text[j - 1];
-    irreducible[i] = irr;
-    if (!irr) continue;
-    const u64 end = segment_end(segs, i);
-    const u64 far = i > j ? i : j;
-    const u64 limit = end - far;
-    const u64 budget = limit < kThreadLcpBytes ? limit : kThreadLcpBytes;
-    u64 l = 0;
-    bool mismatch = false;
-    while (l < budget) {
-      const u64 x = load8(text, i + l) ^ load8(text, j + l);
-      if (x) {
-        l += static_cast<u64>(__ffsll(static_cast<long long>(x)) - 1) >> 3;
-        mismatch = true;
-        break;
-      }
-      l += 8;
-    }
-    if (l > limit) l = limit;
-    if (!mismatch && l < limit) {
-      const u64 slot = atomicAdd(reinterpret_cast<unsigned long long*>(queue_count), 1ull);
-      if (slot < queue_cap) {
-        queue[slot] = LongLcpItem{static_cast<u32>(i), j, l};
+  const u64 rows = (n + 31) / 32 * 32;  // whole warps stay converged
+  for (u64 r = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; r < rows; r += stride) {
+    bool is_long = false, irreducible = false;
+    u32 b = 0, a = 0, l = 0;
+    if (r < n) {
+      b = sa[r];
+      const u64 seg_first = segs.count == 1 ? 0 : segs.begin[find_segment(segs.begin, segs.count, r)];
+      if (r == seg_first) {
+        lcp[r] = 0;
       } else {
-        flag_error(flags, kErrQueueOverflow);
+        a = sa[r - 1];
+        const u64 end = segment_end(segs, r);
+        const u64 far = a > b ? a : b;
+        const u64 limit = end - far;
+        const u64 budget = limit < kDirectLcpBytes ? limit : kDirectLcpBytes;
+        u64 m = 0;
+        bool mismatch = false;
+        while (m < budget) {
+          const u64 x = load8(text, b + m) ^ load8(text, a + m);
+          if (x) {
+            m += static_cast<u64>(__ffsll(static_cast<long long>(x)) - 1) >> 3;
+            mismatch = true;
+            break;
+          }
+          m += 8;
+        }
+        if (m > limit) m = limit;
+        if (mismatch || m >= limit) {
+          lcp[r] = static_cast<u32>(m);
+        } else {
+          is_long = true;
+          l = static_cast<u32>(m);
+          irreducible = b == seg_first || a == seg_first || text[b - 1] != text[a - 1];
+        }
       }
     }
-    plcp[i] = static_cast<u32>(l);
+    const u64 q = warp_append(long_count, is_long && irreducible);
+    if (is_long && irreducible) {
+      if (q < long_cap) longs[q] = LongRow{static_cast<u32>(r), b, a, l};
+      else flag_error(flags, kErrQueueOverflow);
+    }
+    const u64 s = warp_append(pending_count, is_long && !irreducible);
+    if (is_long && !irreducible) {
+      if (s < pending_cap) pending[s] = static_cast<u32>(r);
+      else flag_error(flags, kErrQueueOverflow);
+    }
   }
 }
 
-// One warp per long item: 32 lanes x 16 bytes per step.
+// One warp per long irreducible row: 32 lanes x 16 bytes per step.  Writes
+// the final LCP and the (position, value) pair for the position sort.
 __global__ void __launch_bounds__(256)
-long_lcp_kernel(const u8* __restrict__ text, const LongLcpItem* __restrict__ queue,
-                const u64* queue_count, u64 queue_cap, Segments segs,
-                u32* __restrict__ plcp) {
+long_rows_kernel(const u8* __restrict__ text, const LongRow* __restrict__ longs,
+                 const u64* long_count, u64 long_cap, Segments segs,
+                 u32* __restrict__ lcp, u64* __restrict__ sort_pos,
+                 u32* __restrict__ sort_val) {
   const u32 lane = threadIdx.x & 31;
   const u64 warps = static_cast<u64>(gridDim.x) * (blockDim.x / 32);
-  u64 count = *queue_count;
-  if (count > queue_cap) count = queue_cap;
+  u64 count = *long_count;
+  if (count > long_cap) count = long_cap;
   for (u64 w = (static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x) / 32; w < count; w += warps) {
-    const LongLcpItem item = queue[w];
-    const u64 end = segment_end(segs, item.i);
-    const u64 far = item.i > item.j ? item.i : item.j;
+    const LongRow item = longs[w];
+    const u64 end = segment_end(segs, item.row);
+    const u64 far = item.pos > item.prev ? item.pos : item.prev;
     const u64 limit = end - far;
     u64 l = item.done;
     while (l < limit) {
       const u64 off = l + lane * 16;
-      // Lanes at or past the limit load nothing and report a stop at off;
-      // loads therefore never reach beyond limit + 16 <= the padded end.
+      // Lanes at or past the limit load nothing and report a stop at off, so
+      // loads never reach beyond limit + 16 <= the padded end of the text.
       u64 local = 0;
       if (off < limit) {
-        const u64 x0 = load8(text, item.i + off) ^ load8(text, item.j + off);
-        const u64 x1 = load8(text, item.i + off + 8) ^ load8(text, item.j + off + 8);
+        const u64 x0 = load8(text, item.pos + off) ^ load8(text, item.prev + off);
+        const u64 x1 = load8(text, item.pos + off + 8) ^ load8(text, item.prev + off + 8);
         local = 16;
         if (x0) local = static_cast<u64>(__ffsll(static_cast<long long>(x0)) - 1) >> 3;
         else if (x1) local = 8 + (static_cast<u64>(__ffsll(static_cast<long long>(x1)) - 1) >> 3);
       }
       const u32 hit = __ballot_sync(0xffffffffu, local < 16);
       if (hit) {
-        const u32 first = __ffs(hit) - 1;
-        const u64 found = __shfl_sync(0xffffffffu, off + local, first);
-        l = found;
+        l = __shfl_sync(0xffffffffu, off + local, __ffs(hit) - 1);
         break;
       }
       l += 512;
     }
     if (l > limit) l = limit;
-    if (lane == 0) plcp[item.i] = static_cast<u32>(l);
+    if (lane == 0) {
+      lcp[item.row] = static_cast<u32>(l);
+      sort_pos[w] = item.pos;
+      sort_val[w] = static_cast<u32>(l);
+    }
   }
 }
 
-// Reducible positions: PLCP[i] = PLCP[r] - (i - r), r = last irreducible <= i.
-__global__ void __launch_bounds__(kScanBlock)
-plcp_propagate_kernel(const u8* __restrict__ irreducible, u64 n,
-                      u32* __restrict__ plcp, u64* status_max,
-                      u32* tile_counter, DeviceFlags* flags) {
-  __shared__ u64 warp_smem[kScanBlock / 32];
-  __shared__ u64 tile_prefix;
-  __shared__ u32 tile_slot;
-  const u32 tile = claim_tile(tile_counter, &tile_slot);
-  const u64 i0 = static_cast<u64>(tile) * kScanTile + threadIdx.x * kScanItems;
-  bool irr[kScanItems];
-  u64 last = 0;
-#pragma unroll
-  for (int k = 0; k < kScanItems; ++k) {
-    const u64 i = i0 + k;
-    irr[k] = i < n && irreducible[i];
-    if (irr[k]) last = i;
-  }
-  u64 agg;
-  const u64 excl = block_exclusive_scan<kScanBlock>(last, MaxOp{}, warp_smem, &agg);
-  if ((threadIdx.x >> 5) == 0) {
-    const u64 p = warp_lookback(status_max, tile, agg, MaxOp{}, flags, 7);
-    if ((threadIdx.x & 31) == 0) tile_prefix = p;
-  }
-  __syncthreads();
-  u64 r = tile_prefix > excl ? tile_prefix : excl;
-  u32 base = 0;
-  bool have = false;
-#pragma unroll
-  for (int k = 0; k < kScanItems; ++k) {
-    const u64 i = i0 + k;
-    if (i >= n) break;
-    if (irr[k]) {
-      r = i;
-      have = false;
+// Pending (reducible long) rows: PLCP[b] = PLCP[p] - (b - p) with p the last
+// long irreducible position <= b (sorted_pos is ascending).
+__global__ void __launch_bounds__(256)
+pending_rows_kernel(const u32* __restrict__ sa, const u32* __restrict__ pending,
+                    const u64* pending_count, u64 pending_cap,
+                    const u64* __restrict__ sorted_pos, const u32* __restrict__ sorted_val,
+                    const u64* long_count, u64 long_cap, u32* __restrict__ lcp,
+                    DeviceFlags* flags) {
+  u64 count = *pending_count;
+  if (count > pending_cap) count = pending_cap;
+  u64 q = *long_count;
+  if (q > long_cap) q = long_cap;
+  const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+  for (u64 k = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; k < count; k += stride) {
+    const u32 r = pending[k];
+    const u64 b = sa[r];
+    u64 lo = 0, hi = q;  // first index with sorted_pos > b
+    while (lo < hi) {
+      const u64 mid = (lo + hi) >> 1;
+      if (sorted_pos[mid] <= b) lo = mid + 1;
+      else hi = mid;
+    }
+    if (lo == 0) {
+      flag_error(flags, kErrBounds);
       continue;
     }
-    if (!have) {
-      base = plcp[r];
-      have = true;
-    }
-    plcp[i] = base - static_cast<u32>(i - r);
+    const u64 p = sorted_pos[lo - 1];
+    lcp[r] = sorted_val[lo - 1] - static_cast<u32>(b - p);
   }
 }
 
-// Row order: LCP[r] = PLCP[SA[r]].
 template <class Out>
 __global__ void __launch_bounds__(256)
-lcp_gather_kernel(const u32* __restrict__ sa, const u32* __restrict__ plcp,
-                  u64 n, Out* __restrict__ lcp) {
+widen_kernel(const u32* __restrict__ in, u64 n, Out* __restrict__ out) {
   const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
   for (u64 r = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; r < n; r += stride) {
-    lcp[r] = static_cast<Out>(plcp[sa[r]]);
+    out[r] = static_cast<Out>(in[r]);
   }
 }
 
 __global__ void __launch_bounds__(256)
-lcp_primary_kernel(const u32* __restrict__ sa, const u32* __restrict__ plcp,
-                   u64 n, u8* __restrict__ primary) {
+lcp_primary_kernel(const u32* __restrict__ lcp, u64 n, u8* __restrict__ primary) {
   const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
   for (u64 r = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; r < n; r += stride) {
-    const u32 v = plcp[sa[r]];
+    const u32 v = lcp[r];
     primary[r] = static_cast<u8>(v < 255 ? v : 255);
   }
 }
 
-// Overflow anchors in text order: p opens an anchor when PLCP[p] >= 255 and p
-// does not continue the run of p-1 (PLCP[p-1] == PLCP[p] + 1, same instance).
-// Positions are written as global (concatenated-text) positions; the host
-// splits them per instance and subtracts the instance start.
+// Overflow anchors from the position-sorted long irreducible rows (global
+// positions; the host splits them per instance).  Compaction keeps order.
 template <class Coord>
 __global__ void __launch_bounds__(kScanBlock)
-anchor_kernel(const u32* __restrict__ plcp, u64 n, Segments segs,
+anchor_kernel(const u64* __restrict__ sorted_pos, const u32* __restrict__ sorted_val,
+              const u64* long_count, u64 long_cap, Segments segs,
+              const u32* __restrict__ rank, const u32* __restrict__ lcp,
               Coord* __restrict__ anchor_pos, Coord* __restrict__ anchor_val,
               u64 anchor_cap, u64* status_sum, u32* tile_counter,
               u64* anchor_count, DeviceFlags* flags) {
   __shared__ u64 warp_smem[kScanBlock / 32];
   __shared__ u64 tile_prefix;
   __shared__ u32 tile_slot;
+  u64 q = *long_count;
+  if (q > long_cap) q = long_cap;
   const u32 tile = claim_tile(tile_counter, &tile_slot);
   const u64 i0 = static_cast<u64>(tile) * kScanTile + threadIdx.x * kScanItems;
-  u32 v[kScanItems + 1];
-#pragma unroll
-  for (int k = 0; k < kScanItems + 1; ++k) {
-    const long long i = static_cast<long long>(i0) - 1 + k;
-    v[k] = (i >= 0 && static_cast<u64>(i) < n) ? plcp[i] : 0;
-  }
   bool open[kScanItems];
   u32 opens = 0;
 #pragma unroll
   for (int k = 0; k < kScanItems; ++k) {
     const u64 i = i0 + k;
     open[k] = false;
-    if (i < n && v[k + 1] >= 255) {
-      const bool continues = !is_segment_start(segs, i) && v[k] == v[k + 1] + 1;
+    if (i < q && sorted_val[i] >= 255) {
+      const u64 p = sorted_pos[i];
+      bool continues = false;
+      if (!is_segment_start(segs, p)) continues = lcp[rank[p - 1]] == sorted_val[i] + 1;
       open[k] = !continues;
       opens += open[k];
     }
@@ -243,15 +253,18 @@ anchor_kernel(const u32* __restrict__ plcp, u64 n, Segments segs,
     if (!open[k]) continue;
     const u64 i = i0 + k;
     if (out < anchor_cap) {
-      anchor_pos[out] = static_cast<Coord>(i);
-      anchor_val[out] = static_cast<Coord>(v[k + 1]);
+      anchor_pos[out] = static_cast<Coord>(sorted_pos[i]);
+      anchor_val[out] = static_cast<Coord>(sorted_val[i]);
     } else {
       flag_error(flags, kErrQueueOverflow);
     }
     ++out;
   }
-  const u64 tiles = (n + kScanTile - 1) / kScanTile;
-  if (tile == tiles - 1 && threadIdx.x == 0) *anchor_count = tile_prefix + agg;
+  if (threadIdx.x == 0 && (tile + 1) * static_cast<u64>(kScanTile) >= q) {
+    // The tile holding the last item writes the total (tile_prefix covers
+    // every earlier tile).
+    *anchor_count = tile_prefix + agg;
+  }
 }
 
 }  // namespace sufgpu

@@ -47,7 +47,9 @@ __device__ __forceinline__ void segment_of_tile(const SortSegments& s, u32 tile,
   *last = start + kSortTile < end_seg ? start + kSortTile : end_seg;
 }
 
-// hist layout: [segment][pass][digit], u32 counts.
+// hist layout: [segment][pass][digit], u32 counts.  Per item and pass a warp
+// whose lanes share one digit adds once (long runs of equal keys); otherwise
+// each lane adds to the block's shared histogram.
 __global__ void __launch_bounds__(kSortBlock)
 radix_histogram_kernel(const u64* __restrict__ keys, SortSegments segs,
                        u32 begin_bit, u32 passes, u32* __restrict__ hist) {
@@ -60,16 +62,19 @@ radix_histogram_kernel(const u64* __restrict__ keys, SortSegments segs,
   u64 first, last;
   segment_of_tile(segs, blockIdx.x, &seg, &first, &last);
   const u32 lane = threadIdx.x & 31;
+#pragma unroll 4
   for (int item = 0; item < kSortItems; ++item) {
     const u64 idx = first + static_cast<u64>(item) * kSortBlock + threadIdx.x;
     const bool valid = idx < last;
     const u64 key = valid ? keys[idx] : 0;
+    const bool full = __all_sync(0xffffffffu, valid);
     for (u32 p = 0; p < passes; ++p) {
-      const u32 digit = valid ? static_cast<u32>((key >> (begin_bit + p * kRadixBits)) & 0xff)
-                              : 0x100u;
-      const u32 peers = __match_any_sync(0xffffffffu, digit);
-      if (valid && lane == static_cast<u32>(__ffs(peers) - 1)) {
-        atomicAdd(&local[p][digit], static_cast<u32>(__popc(peers)));
+      const u32 digit = static_cast<u32>((key >> (begin_bit + p * kRadixBits)) & 0xff);
+      const u32 d0 = __shfl_sync(0xffffffffu, digit, 0);
+      if (full && __all_sync(0xffffffffu, digit == d0)) {
+        if (lane == 0) atomicAdd(&local[p][d0], 32u);
+      } else if (valid) {
+        atomicAdd(&local[p][digit], 1u);
       }
     }
   }
@@ -118,6 +123,7 @@ struct OnesweepSmem {
   u32 tile;
 };
 
+template <bool kBallot>
 __global__ void __launch_bounds__(kSortBlock)
 radix_onesweep_kernel(const u64* __restrict__ keys_in,
                       const u32* __restrict__ vals_in,
@@ -151,13 +157,27 @@ radix_onesweep_kernel(const u64* __restrict__ keys_in,
     key[i] = slot < count ? keys_in[first + slot] : ~0ull;
   }
   // Stable warp-level ranking by digit; invalid slots never update counters.
+  // kBallot selects peers with eight ballots over the digit bits instead of
+  // one match-any.
   const u32 lanemask_lt = (1u << lane) - 1;
 #pragma unroll
   for (int i = 0; i < kSortItems; ++i) {
     const u32 slot = warp_base + i * 32 + lane;
     const bool valid = slot < count;
     const u32 digit = valid ? static_cast<u32>((key[i] >> shift) & 0xff) : 0x100u;
-    const u32 peers = __match_any_sync(0xffffffffu, digit);
+    u32 peers;
+    if (kBallot) {
+      peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+      for (int b = 0; b < kRadixBits; ++b) {
+        const bool bit = (digit >> b) & 1;
+        const u32 vote = __ballot_sync(0xffffffffu, bit);
+        peers &= bit ? vote : ~vote;
+      }
+      if (!valid) peers = 1u << lane;
+    } else {
+      peers = __match_any_sync(0xffffffffu, digit);
+    }
     const u32 leader = __ffs(peers) - 1;
     u32 base = 0;
     if (valid && lane == leader) {
