@@ -186,6 +186,28 @@ SUFGPU_API sufgpu_status sufgpu_set_tuning(sufgpu_ctx *ctx, const char *key, int
 SUFGPU_API void *sufgpu_host_alloc(uint64_t bytes);
 SUFGPU_API void sufgpu_host_free(void *ptr);
 
+/* Largest n accepted by sufgpu_lcp_noalloc. */
+#define SUFGPU_NOALLOC_MAX_SYMBOLS (1u << 18)
+
+/* LCP[r] = lcp(SA[r-1], SA[r]) of a device-resident text and suffix array,
+ * written to a device array, for callers that can't allocate device memory:
+ * code running under another framework's allocator (its pool owns the
+ * device, so a foreign cudaMalloc fails or fragments it), callbacks that run
+ * while an allocation lock is held, and loops that cannot block on an
+ * allocation.  Its scratch is one fixed array compiled into the library
+ * (about 11.6 MB, held on every GPU that loads the library until exit); it
+ * calls no cudaMalloc, cudaFree or allocating library routine.  n above
+ * SUFGPU_NOALLOC_MAX_SYMBOLS returns SUFGPU_INVALID_INPUT.  All calls share
+ * the array (each clears what must start at zero), so calls that overlap on
+ * the GPU race and must be serialized by the caller.  The first call on a
+ * device resolves the array's address and a kernel attribute with that
+ * device current; make it before any stream capture.  stream is a
+ * cudaStream_t (NULL = default stream); the call returns after the result is
+ * complete.  No counterpart in the reference: sufkit computes LCP on the host
+ * with its own allocations (src/divsufsort_backend.cpp:121-150). */
+SUFGPU_API sufgpu_status sufgpu_lcp_noalloc(const uint8_t *text, const uint32_t *sa,
+                                            uint64_t n, uint32_t *lcp, void *stream);
+
 /* Normalizes FASTA (plain or gzip) exactly like GenomeReference::FromFasta
  * (src/genome_reference.cpp:30-57, 131-156, 222-268): A/C/G/T (any case) ->
  * 2..5, every other byte -> 6, a 1 after every record.  Writes at most cap

@@ -122,6 +122,8 @@ _SIGNATURES = {
                                             ctypes.POINTER(ctypes.c_double),
                                             ctypes.POINTER(ctypes.c_uint64)]),
     "sufgpu_set_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int64]),
+    "sufgpu_lcp_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                          ctypes.c_void_p, ctypes.c_void_p]),
     "sufgpu_host_alloc": (ctypes.c_void_p, [ctypes.c_uint64]),
     "sufgpu_host_free": (None, [ctypes.c_void_p]),
     "sufgpu_encode_fasta": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_uint64,

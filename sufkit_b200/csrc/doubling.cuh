@@ -42,7 +42,7 @@ __device__ __forceinline__ bool is_segment_start(const Segments& s, u64 x) {
 // Byte histogram of the text (for the symbol remap).  Runs of one byte value
 // are counted in registers first so long N runs do not serialise on one
 // shared-memory counter.
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
 alphabet_histogram_kernel(const u8* __restrict__ text, u64 n,
                           u32* __restrict__ hist) {
   __shared__ u32 local[256];
@@ -87,7 +87,7 @@ constexpr int kSeedRun = 16;
 constexpr int kSeedTile = kSeedBlock * kSeedRun;
 constexpr int kSeedHalo = 64;
 
-__global__ void __launch_bounds__(kSeedBlock)
+static __global__ void __launch_bounds__(kSeedBlock)
 seed_keys_kernel(const u8* __restrict__ text, u64 n, Segments segs,
                  const u16* __restrict__ code_table, u32 bits, u32 symbols,
                  u64* __restrict__ keys, u32* __restrict__ vals) {
@@ -143,7 +143,7 @@ seed_keys_kernel(const u8* __restrict__ text, u64 n, Segments segs,
 // After the seed sort: head flags, head-row ranks and the initial active list.
 // Two scans share the tile: a max-scan of head rows and a sum-scan of active
 // flags (the compaction).  counters[0] receives the active count.
-__global__ void __launch_bounds__(kScanBlock)
+static __global__ void __launch_bounds__(kScanBlock)
 seed_rank_kernel(const u64* __restrict__ keys, const u32* __restrict__ sa,
                  u64 n, Segments segs, u32* __restrict__ rank,
                  u32* __restrict__ active, u64* status_max, u64* status_sum,
@@ -206,7 +206,7 @@ seed_rank_kernel(const u64* __restrict__ keys, const u32* __restrict__ sa,
 
 // Round step 1: composite keys for the active list.  counters: *group_count
 // receives the number of groups G.  ghead/gstart are indexed by dense id.
-__global__ void __launch_bounds__(kScanBlock)
+static __global__ void __launch_bounds__(kScanBlock)
 round_keys_kernel(const u32* __restrict__ active, u64 count,
                   const u32* __restrict__ rank, u64 h, Segments segs,
                   u32 second_bits, u64* __restrict__ ckey,
@@ -272,7 +272,7 @@ round_keys_kernel(const u32* __restrict__ active, u64 count,
 
 // Round step 2 (after sorting the composite keys): new heads, SA rows, ranks,
 // and the next active list.
-__global__ void __launch_bounds__(kScanBlock)
+static __global__ void __launch_bounds__(kScanBlock)
 round_rank_kernel(const u64* __restrict__ ckey, const u32* __restrict__ cval,
                   u64 count, u32 second_bits, const u32* __restrict__ ghead,
                   const u32* __restrict__ gstart, u64 group_cap, u64 rows,

@@ -60,7 +60,7 @@ __device__ __forceinline__ u64 warp_append(u64* counter, bool take) {
 
 // Row pass.  lcp receives final values for short rows; long rows go to the
 // irreducible queue or the pending (reducible) list.
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
 lcp_rows_kernel(const u8* __restrict__ text, const u32* __restrict__ sa, u64 n,
                 Segments segs, u32* __restrict__ lcp, LongRow* __restrict__ longs,
                 u64 long_cap, u64* long_count, u32* __restrict__ pending,
@@ -117,7 +117,7 @@ lcp_rows_kernel(const u8* __restrict__ text, const u32* __restrict__ sa, u64 n,
 
 // One warp per long irreducible row: 32 lanes x 16 bytes per step.  Writes
 // the final LCP and the (position, value) pair for the position sort.
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
 long_rows_kernel(const u8* __restrict__ text, const LongRow* __restrict__ longs,
                  const u64* long_count, u64 long_cap, Segments segs,
                  u32* __restrict__ lcp, u64* __restrict__ sort_pos,
@@ -162,7 +162,7 @@ long_rows_kernel(const u8* __restrict__ text, const LongRow* __restrict__ longs,
 
 // Pending (reducible long) rows: PLCP[b] = PLCP[p] - (b - p) with p the last
 // long irreducible position <= b (sorted_pos is ascending).
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
 pending_rows_kernel(const u32* __restrict__ sa, const u32* __restrict__ pending,
                     const u64* pending_count, u64 pending_cap,
                     const u64* __restrict__ sorted_pos, const u32* __restrict__ sorted_val,
@@ -192,7 +192,7 @@ pending_rows_kernel(const u32* __restrict__ sa, const u32* __restrict__ pending,
 }
 
 template <class Out>
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
 widen_kernel(const u32* __restrict__ in, u64 n, Out* __restrict__ out) {
   const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
   for (u64 r = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; r < n; r += stride) {
@@ -200,7 +200,7 @@ widen_kernel(const u32* __restrict__ in, u64 n, Out* __restrict__ out) {
   }
 }
 
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
 lcp_primary_kernel(const u32* __restrict__ lcp, u64 n, u8* __restrict__ primary) {
   const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
   for (u64 r = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; r < n; r += stride) {
@@ -212,7 +212,7 @@ lcp_primary_kernel(const u32* __restrict__ lcp, u64 n, u8* __restrict__ primary)
 // Overflow anchors from the position-sorted long irreducible rows (global
 // positions; the host splits them per instance).  Compaction keeps order.
 template <class Coord>
-__global__ void __launch_bounds__(kScanBlock)
+static __global__ void __launch_bounds__(kScanBlock)
 anchor_kernel(const u64* __restrict__ sorted_pos, const u32* __restrict__ sorted_val,
               const u64* long_count, u64 long_cap, Segments segs,
               const u32* __restrict__ rank, const u32* __restrict__ lcp,

@@ -11,7 +11,7 @@ namespace sufgpu {
 // into the low plane, and the high plane when the width has one.  Device
 // coordinates are 32-bit, so high planes of split40/48 receive zeros and the
 // native64 plane the zero-extended value.
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
 pack_kernel(const u32* __restrict__ values, u64 n, Segments segs, u32 bits,
             void* __restrict__ low, void* __restrict__ high) {
   const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
@@ -31,7 +31,7 @@ pack_kernel(const u32* __restrict__ values, u64 n, Segments segs, u32 bits,
 // SA validation (the check RepackSuffixArray performs on the host): every row
 // holds a position of its own instance, and ISA[SA[r]] == r, which together
 // make SA a permutation.
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
 validate_kernel(const u32* __restrict__ sa, const u32* __restrict__ isa, u64 n,
                 Segments segs, DeviceFlags* flags) {
   const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;

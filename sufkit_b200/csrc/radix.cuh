@@ -50,7 +50,7 @@ __device__ __forceinline__ void segment_of_tile(const SortSegments& s, u32 tile,
 // hist layout: [segment][pass][digit], u32 counts.  Per item and pass a warp
 // whose lanes share one digit adds once (long runs of equal keys); otherwise
 // each lane adds to the block's shared histogram.
-__global__ void __launch_bounds__(kSortBlock)
+static __global__ void __launch_bounds__(kSortBlock)
 radix_histogram_kernel(const u64* __restrict__ keys, SortSegments segs,
                        u32 begin_bit, u32 passes, u32* __restrict__ hist) {
   __shared__ u32 local[kMaxPasses][kRadixDigits];
@@ -89,7 +89,7 @@ radix_histogram_kernel(const u64* __restrict__ keys, SortSegments segs,
 // digit_start layout: [segment][pass][digit], absolute u64 element offsets.
 // needed[p] is set when some segment has more than one non-empty digit in
 // pass p (otherwise the pass is the identity and is skipped).
-__global__ void __launch_bounds__(kRadixDigits)
+static __global__ void __launch_bounds__(kRadixDigits)
 radix_offsets_kernel(const u32* __restrict__ hist, const u64* __restrict__ begin,
                      u32 passes, u64* __restrict__ digit_start,
                      u32* __restrict__ needed) {
@@ -124,7 +124,7 @@ struct OnesweepSmem {
 };
 
 template <bool kBallot>
-__global__ void __launch_bounds__(kSortBlock)
+static __global__ void __launch_bounds__(kSortBlock)
 radix_onesweep_kernel(const u64* __restrict__ keys_in,
                       const u32* __restrict__ vals_in,
                       u64* __restrict__ keys_out, u32* __restrict__ vals_out,
