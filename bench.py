@@ -42,6 +42,10 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="plain100m",
                     choices=["plain100m", "plain4m", "batched"])
+    ap.add_argument("--count", type=int, default=256,
+                    help="references in the batched workload (1,024 in the full collection)")
+    ap.add_argument("--batch-symbols", type=float, default=1.2e9,
+                    help="HBM admission budget per batch launch (symbols)")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="shrink the workload (profiling captures only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -62,7 +66,7 @@ def peaks():
 # ---------------------------------------------------------------------------
 # Workloads
 # ---------------------------------------------------------------------------
-def workload(name: str, scale: float = 1.0):
+def workload(name: str, scale: float = 1.0, count: int = 256):
     from sufkit_b200 import synth
     if name == "plain4m":
         ref = synth.plain_4mbp()
@@ -70,9 +74,11 @@ def workload(name: str, scale: float = 1.0):
                 "0.1% N runs; Fast profile SA+ISA+raw LCP32, 32-bit storage")
         return [ref.logical_text()], desc
     if name == "batched":
-        refs = synth.uneven_collection(count=64)
-        desc = ("batched uneven collection sample: 64 bacterial-like references "
-                "(log-normal, median 4 Mbp), SA+raw LCP32 per reference, one batch")
+        refs = synth.uneven_collection(count=count, scale=scale)
+        desc = (f"batched uneven collection: first {count} of 1,024 bacterial-like references "
+                "(log-normal sizes, median 4 Mbp, clipped 0.5-12 Mbp, GC 30-70%, 1-8 contigs); "
+                "SA + raw LCP32 per reference, 32-bit, HBM-admitted batch launches, "
+                "compared with the plain build one reference at a time")
         return [r.logical_text() for r in refs], desc
     ref = synth.repeat_rich_100mbp(scale)
     desc = ("repeat-rich 100 Mbp plain build: 24 contigs, GC 41%, 25% interspersed "
@@ -232,7 +238,7 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    texts, desc = workload(args.workload, args.scale)
+    texts, desc = workload(args.workload, args.scale, args.count)
     if args.scale != 1.0:
         desc += f" (scaled x{args.scale})"
 
@@ -267,18 +273,41 @@ def main():
               "lcp": torch.empty(t.size, dtype=torch.int32, device=dev)} for t in texts]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
+    def ptrs(o):
+        return {k: (v.data_ptr() if v is not None else None) for k, v in o.items()}
+
+    # Batches admitted by their symbol footprint (each launch holds at most
+    # --batch-symbols symbols on the device).
+    batches, cur, cur_n = [], [], 0
+    for j, t in enumerate(texts):
+        if cur and cur_n + t.size > args.batch_symbols:
+            batches.append(cur)
+            cur, cur_n = [], 0
+        cur.append(j)
+        cur_n += int(t.size)
+    if cur:
+        batches.append(cur)
+
     def device_step():
         if len(texts) == 1:
-            st = ctx.build_device(d_texts[0].data_ptr(), int(texts[0].size),
-                                  {k: (v.data_ptr() if v is not None else None)
-                                   for k, v in d_out[0].items()},
-                                  sa_bits=32, isa_bits=isa_bits, lcp=lcp_enc)
-        else:
-            st = ctx.build_batch_device([(d.data_ptr(), int(t.size)) for d, t in zip(d_texts, texts)],
-                                        [{k: (v.data_ptr() if v is not None else None)
-                                          for k, v in o.items()} for o in d_out],
+            return ctx.build_device(d_texts[0].data_ptr(), int(texts[0].size), ptrs(d_out[0]),
+                                    sa_bits=32, isa_bits=isa_bits, lcp=lcp_enc)
+        total = {"device_seconds": 0.0, "kernel_launches": 0}
+        for b in batches:
+            st = ctx.build_batch_device([(d_texts[j].data_ptr(), int(texts[j].size)) for j in b],
+                                        [ptrs(d_out[j]) for j in b],
                                         sa_bits=32, isa_bits=isa_bits, lcp=lcp_enc)
-        return st
+            total["device_seconds"] += st["device_seconds"]
+            total["kernel_launches"] += st["kernel_launches"]
+        return total
+
+    def one_at_a_time():
+        seconds = 0.0
+        for j, t in enumerate(texts):
+            st = ctx.build_device(d_texts[j].data_ptr(), int(t.size), ptrs(d_out[j]),
+                                  sa_bits=32, isa_bits=isa_bits, lcp=lcp_enc)
+            seconds += st["device_seconds"]
+        return seconds
 
     for _ in range(args.warmup):
         flush.fill_(1)
@@ -308,6 +337,15 @@ def main():
         dist.barrier()
     profile = ctx.profile()
     ctx.set_profiling(False)
+    single = None
+    if len(texts) > 1:
+        one_at_a_time()  # warm
+        flush.fill_(3)
+        torch.cuda.synchronize()
+        sec = one_at_a_time()
+        single = {"one_at_a_time_Gsym_s": n_total / sec / 1e9,
+                  "batched_over_one_at_a_time": (sec / (device_seconds / args.steps)),
+                  "batches": len(batches), "references": len(texts)}
 
     step_seconds = device_seconds / args.steps
     if dist is not None:
@@ -401,7 +439,7 @@ def main():
                        "parallelism": f"{world} independent replica(s)",
                        "timing": "device time per build (library CUDA events), "
                                  "max over ranks", "wall_s": wall,
-                       "build_roofline": whole, "kernels": kernels},
+                       "build_roofline": whole, "batched": single, "kernels": kernels},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "clocks": clock_info, "gpu_launches": launches,
         }
@@ -416,8 +454,9 @@ def e2e_step(ctx, pinned_text, host_out, isa_bits, lcp_enc):
         t = pinned_text[0]
         return ctx.build_device(t.ctypes.data, int(t.size), host_out[0], sa_bits=32,
                                 isa_bits=isa_bits, lcp=lcp_enc)
-    return ctx.build_batch_device([(t.ctypes.data, int(t.size)) for t in pinned_text], host_out,
-                                  sa_bits=32, isa_bits=isa_bits, lcp=lcp_enc)
+    for lo in range(0, len(pinned_text), 64):
+        ctx.build_batch_device([(t.ctypes.data, int(t.size)) for t in pinned_text[lo:lo + 64]],
+                               host_out[lo:lo + 64], sa_bits=32, isa_bits=isa_bits, lcp=lcp_enc)
 
 
 if __name__ == "__main__":

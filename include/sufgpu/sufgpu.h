@@ -178,7 +178,9 @@ SUFGPU_API sufgpu_status sufgpu_profile_entry(const sufgpu_ctx *ctx, uint32_t in
 
 /* Tuning knobs (picked by the autotuner, sufkit_b200/autotune.py):
  *   "seed_symbols"  symbols packed per seed key, 0 = as many as fit 64 bits;
- *   "ballot_rank"   1 = onesweep ranks digits with ballots, 0 = match-any.
+ *   "ballot_rank"   1 = onesweep ranks digits with ballots, 0 = match-any;
+ *   "ballot_min_elems" smallest sort that uses ballot ranking;
+ *   "sort_block"    onesweep threads per 4096-key tile: 256 or 512.
  * Results are identical for every setting; only speed changes. */
 SUFGPU_API sufgpu_status sufgpu_set_tuning(sufgpu_ctx *ctx, const char *key, int64_t value);
 

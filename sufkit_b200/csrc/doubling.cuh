@@ -81,68 +81,105 @@ alphabet_histogram_kernel(const u8* __restrict__ text, u64 n,
 // Seed keys.  Each thread computes kSeedRun consecutive keys by sliding a
 // window over text staged in shared memory (tile + halo).  code[] maps bytes
 // to 1..sigma (sigma <= 256, so 16-bit codes); symbols at or beyond the
-// instance end contribute 0.
+// instance end contribute 0.  The tile's keys are staged in shared memory and
+// written out coalesced, and the digit histograms of every radix pass over
+// bits [0, passes*8) are accumulated on the way (per instance segment), so
+// the seed sort needs no separate histogram read of the keys.
 constexpr int kSeedBlock = 256;
 constexpr int kSeedRun = 16;
 constexpr int kSeedTile = kSeedBlock * kSeedRun;
 constexpr int kSeedHalo = 64;
 
+struct SeedSmem {
+  u64 keys[kSeedTile];
+  u32 hist[8][256];
+  u16 code[256];
+  __align__(16) u8 window[kSeedTile + kSeedHalo];
+};
+
 static __global__ void __launch_bounds__(kSeedBlock)
 seed_keys_kernel(const u8* __restrict__ text, u64 n, Segments segs,
                  const u16* __restrict__ code_table, u32 bits, u32 symbols,
+                 u32 passes, u32* __restrict__ hist_out,
                  u64* __restrict__ keys, u32* __restrict__ vals) {
-  __shared__ u16 code[256];
-  __shared__ __align__(16) u8 window[kSeedTile + kSeedHalo];
-  code[threadIdx.x] = code_table[threadIdx.x];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  SeedSmem& sm = *reinterpret_cast<SeedSmem*>(smem_raw);
+  sm.code[threadIdx.x] = code_table[threadIdx.x];
+  for (int i = threadIdx.x; i < 8 * 256; i += kSeedBlock) (&sm.hist[0][0])[i] = 0;
   const u64 tile_first = static_cast<u64>(blockIdx.x) * kSeedTile;
   // Stage tile + halo as 16-byte vectors (the text buffer is padded).
   for (int i = threadIdx.x; i < (kSeedTile + kSeedHalo) / 16; i += kSeedBlock) {
     const u64 at = tile_first + static_cast<u64>(i) * 16;
     uint4 v = make_uint4(0, 0, 0, 0);
     if (at < n) v = *reinterpret_cast<const uint4*>(text + at);
-    *reinterpret_cast<uint4*>(window + i * 16) = v;
+    *reinterpret_cast<uint4*>(sm.window + i * 16) = v;
   }
   __syncthreads();
+  const u32 block_seg = segs.count == 1 ? 0 : find_segment(segs.begin, segs.count, tile_first);
   const u64 mask = symbols * bits >= 64 ? ~0ull : ((1ull << (symbols * bits)) - 1);
   const u32 local0 = threadIdx.x * kSeedRun;
+  const u32 lane = threadIdx.x & 31;
   u64 pos = tile_first + local0;
-  if (pos >= n) return;
-  u64 end = segment_end(segs, pos);
+  u32 seg = segs.count == 1 ? 0 : (pos < n ? find_segment(segs.begin, segs.count, pos) : block_seg);
+  u64 end = pos < n ? segs.begin[seg + 1] : n;
   u64 key = 0;
   bool fresh = true;
-  u64 out_keys[kSeedRun];
-  int produced = 0;
-  for (int r = 0; r < kSeedRun && pos < n; ++r, ++pos) {
-    if (pos >= end) {  // crossed into the next instance
-      end = segment_end(segs, pos);
+  for (int r = 0; r < kSeedRun; ++r, ++pos) {
+    const bool valid = pos < n;
+    if (valid && pos >= end) {  // crossed into the next instance
+      seg = find_segment(segs.begin, segs.count, pos);
+      end = segs.begin[seg + 1];
       fresh = true;
     }
     const u32 local = local0 + r;
-    if (fresh) {
-      key = 0;
-      for (u32 t = 0; t < symbols; ++t) {
-        const u32 c = pos + t < end ? code[window[local + t]] : 0u;
-        key = (key << bits) | c;
+    if (valid) {
+      if (fresh) {
+        key = 0;
+        for (u32 t = 0; t < symbols; ++t) {
+          const u32 c = pos + t < end ? sm.code[sm.window[local + t]] : 0u;
+          key = (key << bits) | c;
+        }
+        fresh = false;
+      } else {
+        const u64 q = pos + symbols - 1;
+        const u32 c = q < end ? sm.code[sm.window[local + symbols - 1]] : 0u;
+        key = ((key << bits) | c) & mask;
       }
-      fresh = false;
-    } else {
-      const u64 q = pos + symbols - 1;
-      const u32 c = q < end ? code[window[local + symbols - 1]] : 0u;
-      key = ((key << bits) | c) & mask;
+      sm.keys[local] = key;
     }
-    out_keys[r] = key;
-    produced = r + 1;
+    // Histogram of every pass; a warp whose lanes agree adds once.
+    const bool mine = valid && seg == block_seg;
+    const bool all_mine = __all_sync(0xffffffffu, mine);
+    for (u32 p = 0; p < passes; ++p) {
+      const u32 digit = static_cast<u32>((key >> (p * 8)) & 0xff);
+      const u32 d0 = __shfl_sync(0xffffffffu, digit, 0);
+      if (all_mine && __all_sync(0xffffffffu, digit == d0)) {
+        if (lane == 0) atomicAdd(&sm.hist[p][d0], 32u);
+      } else if (mine) {
+        atomicAdd(&sm.hist[p][digit], 1u);
+      } else if (valid) {
+        atomicAdd(&hist_out[(static_cast<u64>(seg) * passes + p) * 256 + digit], 1u);
+      }
+    }
   }
-  const u64 first = tile_first + local0;
-  for (int r = 0; r < produced; ++r) {
-    keys[first + r] = out_keys[r];
-    vals[first + r] = static_cast<u32>(first + r);
+  __syncthreads();
+  for (u32 i = threadIdx.x; i < kSeedTile; i += kSeedBlock) {
+    const u64 at = tile_first + i;
+    if (at < n) {
+      keys[at] = sm.keys[i];
+      vals[at] = static_cast<u32>(at);
+    }
+  }
+  for (u32 i = threadIdx.x; i < passes * 256; i += kSeedBlock) {
+    const u32 c = (&sm.hist[0][0])[i];
+    if (c) atomicAdd(&hist_out[static_cast<u64>(block_seg) * passes * 256 + i], c);
   }
 }
 
-// After the seed sort: head flags, head-row ranks and the initial active list.
-// Two scans share the tile: a max-scan of head rows and a sum-scan of active
-// flags (the compaction).  counters[0] receives the active count.
+// After the seed sort: head flags, head-row ranks (rank[SA[r]] = head row of
+// r; the one full random scatter of the build, at the device's scattered-store
+// rate) and the initial active list.  Two scans share the tile: a max-scan of
+// head rows and a sum-scan of active flags (the compaction).
 static __global__ void __launch_bounds__(kScanBlock)
 seed_rank_kernel(const u64* __restrict__ keys, const u32* __restrict__ sa,
                  u64 n, Segments segs, u32* __restrict__ rank,

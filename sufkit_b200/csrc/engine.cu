@@ -136,7 +136,24 @@ Layout plan_layout(u8* base, u64 n, u32 segments) {
   return l;
 }
 
-u64 sort_smem_bytes() { return sizeof(OnesweepSmem); }
+using OnesweepFn = void (*)(const u64*, const u32*, u64*, u32*, SortSegments, u32, u32, u32,
+                            const u64*, u64*, u32*, DeviceFlags*);
+
+// Onesweep variants: ranking by ballots or match-any, 256x16 or 512x8 tiles.
+struct OnesweepVariant {
+  OnesweepFn fn;
+  u32 block;
+  u64 smem;
+};
+
+OnesweepVariant onesweep_variant(bool ballot, u32 block) {
+  if (block == 512) {
+    return {ballot ? radix_onesweep_kernel<true, 512, 8> : radix_onesweep_kernel<false, 512, 8>,
+            512, sizeof(OnesweepSmem<512>)};
+  }
+  return {ballot ? radix_onesweep_kernel<true, 256, 16> : radix_onesweep_kernel<false, 256, 16>,
+          256, sizeof(OnesweepSmem<256>)};
+}
 
 }  // namespace
 
@@ -192,6 +209,10 @@ struct sufgpu_ctx {
   u32 seed_symbols = 0;
   // Onesweep ranking: ballots over digit bits (true) or match-any (false).
   bool ballot_rank = true;
+  // Ballot ranking only pays off on large sorts; smaller ones use match-any.
+  u64 ballot_min_elems = u64(1) << 23;
+  // Onesweep block size (256 threads x 16 keys or 512 x 8).
+  u32 sort_block = 256;
 };
 
 namespace {
@@ -266,7 +287,7 @@ struct Engine {
   bool radix_sort(const char* name, u64* keys, u32* vals, u64* keys_alt, u32* vals_alt,
                   const u64* seg_begin, const u32* seg_tiles, u32 seg_count,
                   u32 total_tiles, u64 sort_elems, u32 begin_bit, u32 end_bit,
-                  bool check_needed) {
+                  bool check_needed, bool hist_ready = false) {
     if (end_bit <= begin_bit || total_tiles == 0) return false;
     const u32 passes = (end_bit - begin_bit + kRadixBits - 1) / kRadixBits;
     SortSegments ss{seg_begin, seg_tiles, seg_count, total_tiles};
@@ -274,10 +295,12 @@ struct Engine {
     u32 needed[kMaxPasses];
     for (u32 p = 0; p < passes; ++p) needed[p] = 1;
     if (check_needed) {
-      zero(L.hist, u64(seg_count) * passes * kRadixDigits * 4);
       zero(L.counters + 32, 4 * kMaxPasses);
-      launch("radix_histogram", elems * 8, radix_histogram_kernel, total_tiles, kSortBlock, 0,
-             keys, ss, begin_bit, passes, L.hist);
+      if (!hist_ready) {
+        zero(L.hist, u64(seg_count) * passes * kRadixDigits * 4);
+        launch("radix_histogram", elems * 8, radix_histogram_kernel, total_tiles, kSortBlock, 0,
+               keys, ss, begin_bit, passes, L.hist);
+      }
       launch("radix_offsets", u64(seg_count) * passes * kRadixDigits * 12, radix_offsets_kernel,
              seg_count, kRadixDigits, 0, L.hist, seg_begin, passes, L.digit_start,
              L.counters + 32);
@@ -302,10 +325,9 @@ struct Engine {
       if (!needed[p]) continue;
       zero(L.status, u64(total_tiles) * kRadixDigits * 8);
       zero(L.counters, 4);
-      launch(name, elems * 24,
-             c.ballot_rank ? radix_onesweep_kernel<true> : radix_onesweep_kernel<false>,
-             total_tiles, kSortBlock,
-             sort_smem_bytes(),
+      const OnesweepVariant v =
+          onesweep_variant(c.ballot_rank && elems >= c.ballot_min_elems, c.sort_block);
+      launch(name, elems * 24, v.fn, total_tiles, v.block, v.smem,
              kin, vin, kout, vout, ss, begin_bit + p * kRadixBits, p, passes,
              L.digit_start, L.status, L.counters, L.flags);
       std::swap(kin, kout);
@@ -356,11 +378,15 @@ struct Engine {
     // Seed keys and the segmented seed sort.
     upload_segments(begin);
     const u32 seed_tiles = last_tiles;
-    launch("seed_keys", n * 13, seed_keys_kernel, (n + kSeedTile - 1) / kSeedTile, kSeedBlock, 0,
-           L.text, n, segments(), L.code, bits, symbols, L.k0, L.v0);
+    const u32 seed_bits = bits * symbols;
+    const u32 seed_passes = (seed_bits + kRadixBits - 1) / kRadixBits;
+    zero(L.hist, u64(segs) * seed_passes * kRadixDigits * 4);
+    launch("seed_keys", n * 13, seed_keys_kernel, (n + kSeedTile - 1) / kSeedTile, kSeedBlock,
+           sizeof(SeedSmem), L.text, n, segments(), static_cast<const u16*>(L.code), bits,
+           symbols, seed_passes, L.hist, L.k0, L.v0);
     u64* keys = L.k0;
     const bool swapped = radix_sort("seed_onesweep", L.k0, L.v0, L.k1, L.sa, L.seg_begin, L.seg_tiles,
-                                    segs, seed_tiles, n, 0, bits * symbols, true);
+                                    segs, seed_tiles, n, 0, seed_bits, true, true);
     if (swapped) {
       keys = L.k1;
       sa = L.sa;
@@ -377,8 +403,7 @@ struct Engine {
     u64* status_max = L.status;
     u64* status_sum = L.status + scan_tiles + 1;
     launch("seed_rank", n * 16, seed_rank_kernel, scan_tiles, kScanBlock, 0, keys, sa, n,
-           segments(),
-           L.rank, L.x, status_max, status_sum, L.counters, L.scalars + 0, L.flags);
+           segments(), L.rank, L.x, status_max, status_sum, L.counters, L.scalars + 0, L.flags);
     u64 active = read_scalar(0);
 
     // Rounds.  act and other alternate between x and the spare SA-sized
@@ -656,12 +681,13 @@ sufgpu_status sufgpu_create(sufgpu_ctx** out, int device) {
     SG_CUDA(cudaMallocHost(reinterpret_cast<void**>(&ctx->host_scalars), 64 * 8));
     SG_CUDA(cudaMallocHost(reinterpret_cast<void**>(&ctx->host_small), 1u << 20));
     for (auto& ev : ctx->ev) SG_CUDA(cudaEventCreate(&ev));
-    SG_CUDA(cudaFuncSetAttribute(radix_onesweep_kernel<true>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(sort_smem_bytes())));
-    SG_CUDA(cudaFuncSetAttribute(radix_onesweep_kernel<false>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(sort_smem_bytes())));
+    for (bool ballot : {true, false}) {
+      for (u32 block : {256u, 512u}) {
+        const OnesweepVariant v = onesweep_variant(ballot, block);
+        SG_CUDA(cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(v.smem)));
+      }
+    }
   } catch (const CudaError& err) {
     g_create_error = std::string("CUDA error in ") + err.what + ": " + cudaGetErrorString(err.code);
     sufgpu_destroy(ctx);
@@ -928,6 +954,12 @@ extern "C" sufgpu_status sufgpu_set_tuning(sufgpu_ctx* ctx, const char* key, int
     ctx->seed_symbols = static_cast<u32>(value);
   } else if (k == "ballot_rank") {
     ctx->ballot_rank = value != 0;
+  } else if (k == "ballot_min_elems") {
+    if (value < 0) return fail(ctx, SUFGPU_INVALID_INPUT, "ballot_min_elems must be >= 0");
+    ctx->ballot_min_elems = static_cast<u64>(value);
+  } else if (k == "sort_block") {
+    if (value != 256 && value != 512) return fail(ctx, SUFGPU_INVALID_INPUT, "sort_block must be 256 or 512");
+    ctx->sort_block = static_cast<u32>(value);
   } else {
     return fail(ctx, SUFGPU_INVALID_INPUT, "unknown tuning key " + k);
   }

@@ -79,9 +79,9 @@ cudaError_t scratch_for_current_device(unsigned char** out) {
     void* ptr = nullptr;
     err = cudaGetSymbolAddress(&ptr, g_lcp_scratch);
     if (err != cudaSuccess) return err;
-    err = cudaFuncSetAttribute(radix_onesweep_kernel<true>,
+    err = cudaFuncSetAttribute(radix_onesweep_kernel<true, kSortBlock, kSortItems>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(sizeof(OnesweepSmem)));
+                               static_cast<int>(sizeof(OnesweepSmem<kSortBlock>)));
     if (err != cudaSuccess) return err;
     g_scratch_ptr[device] = static_cast<unsigned char*>(ptr);
   }
@@ -181,7 +181,8 @@ extern "C" sufgpu_status sufgpu_lcp_noalloc(const uint8_t* text, const uint32_t*
     for (u32 p = 0; p < passes; ++p) {
       NA_CUDA(cudaMemsetAsync(status, 0, u64(tiles) * kRadixDigits * 8, stream));
       NA_CUDA(cudaMemsetAsync(counters, 0, 4, stream));
-      radix_onesweep_kernel<true><<<tiles, kSortBlock, sizeof(OnesweepSmem), stream>>>(
+      radix_onesweep_kernel<true, kSortBlock, kSortItems>
+          <<<tiles, kSortBlock, sizeof(OnesweepSmem<kSortBlock>), stream>>>(
           kin, vin, kout, vout, ss, p * kRadixBits, p, passes, digits, status, counters, flags);
       NA_CUDA(cudaGetLastError());
       u64* tk = kin; kin = kout; kout = tk;

@@ -111,33 +111,37 @@ radix_offsets_kernel(const u32* __restrict__ hist, const u64* __restrict__ begin
   }
 }
 
-// One LSD pass over bits [shift, shift+8).
-// Shared memory: keys (32 KB) + values (16 KB) + per-warp digit counters.
+// One LSD pass over bits [shift, shift+8), for a tile of kSortTile pairs
+// handled by kBlock threads x kItems items.  Shared memory holds the tile's
+// keys and values in sorted-slot order and per-warp digit counters.
+template <int kBlock>
 struct OnesweepSmem {
   u64 keys[kSortTile];
   u32 vals[kSortTile];
-  u32 warp_hist[kSortBlock / 32][kRadixDigits];
+  u32 warp_hist[kBlock / 32][kRadixDigits];
   u32 digit_excl[kRadixDigits];
   long long digit_gbase[kRadixDigits];
-  u64 warp_scan[kSortBlock / 32];
+  u64 warp_scan[kBlock / 32];
   u32 tile;
 };
 
-template <bool kBallot>
-static __global__ void __launch_bounds__(kSortBlock)
+template <bool kBallot, int kBlock, int kItems>
+static __global__ void __launch_bounds__(kBlock)
 radix_onesweep_kernel(const u64* __restrict__ keys_in,
                       const u32* __restrict__ vals_in,
                       u64* __restrict__ keys_out, u32* __restrict__ vals_out,
                       SortSegments segs, u32 shift, u32 pass, u32 passes,
                       const u64* __restrict__ digit_start, u64* status,
                       u32* tile_counter, DeviceFlags* flags) {
+  static_assert(kBlock * kItems == kSortTile, "tile size is fixed");
+  static_assert(kBlock >= kRadixDigits, "one thread per digit");
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  OnesweepSmem& sm = *reinterpret_cast<OnesweepSmem*>(smem_raw);
-  constexpr int kWarps = kSortBlock / 32;
+  OnesweepSmem<kBlock>& sm = *reinterpret_cast<OnesweepSmem<kBlock>*>(smem_raw);
+  constexpr int kWarps = kBlock / 32;
   const u32 lane = threadIdx.x & 31;
   const u32 warp = threadIdx.x >> 5;
 
-  for (int i = threadIdx.x; i < kWarps * kRadixDigits; i += kSortBlock) {
+  for (int i = threadIdx.x; i < kWarps * kRadixDigits; i += kBlock) {
     (&sm.warp_hist[0][0])[i] = 0;
   }
   const u32 tile = claim_tile(tile_counter, &sm.tile);
@@ -147,12 +151,12 @@ radix_onesweep_kernel(const u64* __restrict__ keys_in,
   const u32 count = static_cast<u32>(last - first);
   const bool first_tile_of_segment = tile == segs.tile_begin[seg];
 
-  // Warp-striped load: warp w owns tile slots [w*32*ITEMS, (w+1)*32*ITEMS).
-  u64 key[kSortItems];
-  u32 rank[kSortItems];
-  const u32 warp_base = warp * 32 * kSortItems;
+  // Warp-striped load: warp w owns tile slots [w*32*kItems, (w+1)*32*kItems).
+  u64 key[kItems];
+  u32 rank[kItems];
+  const u32 warp_base = warp * 32 * kItems;
 #pragma unroll
-  for (int i = 0; i < kSortItems; ++i) {
+  for (int i = 0; i < kItems; ++i) {
     const u32 slot = warp_base + i * 32 + lane;
     key[i] = slot < count ? keys_in[first + slot] : ~0ull;
   }
@@ -161,7 +165,7 @@ radix_onesweep_kernel(const u64* __restrict__ keys_in,
   // one match-any.
   const u32 lanemask_lt = (1u << lane) - 1;
 #pragma unroll
-  for (int i = 0; i < kSortItems; ++i) {
+  for (int i = 0; i < kItems; ++i) {
     const u32 slot = warp_base + i * 32 + lane;
     const bool valid = slot < count;
     const u32 digit = valid ? static_cast<u32>((key[i] >> shift) & 0xff) : 0x100u;
@@ -191,48 +195,52 @@ radix_onesweep_kernel(const u64* __restrict__ keys_in,
   __syncthreads();
 
   // Per digit: exclusive offsets across warps, tile count, tile-local start.
-  const u32 d = threadIdx.x;  // kSortBlock == kRadixDigits
+  const u32 d = threadIdx.x;
   u32 digit_count = 0;
+  if (d < kRadixDigits) {
 #pragma unroll
-  for (int w = 0; w < kWarps; ++w) {
-    const u32 c = sm.warp_hist[w][d];
-    sm.warp_hist[w][d] = digit_count;
-    digit_count += c;
+    for (int w = 0; w < kWarps; ++w) {
+      const u32 c = sm.warp_hist[w][d];
+      sm.warp_hist[w][d] = digit_count;
+      digit_count += c;
+    }
   }
   u64 tile_total;
   const u64 local_start =
-      block_exclusive_scan<kSortBlock>(digit_count, SumOp{}, sm.warp_scan, &tile_total);
-  sm.digit_excl[d] = static_cast<u32>(local_start);
+      block_exclusive_scan<kBlock>(digit_count, SumOp{}, sm.warp_scan, &tile_total);
 
   // Decoupled look-back, one digit per thread.  Prefix values are absolute
   // output positions; a segment's first tile seeds them from digit_start.
-  u64* my_status = status + static_cast<u64>(tile) * kRadixDigits + d;
-  u64 global_start;
-  if (first_tile_of_segment) {
-    global_start =
-        digit_start[(static_cast<u64>(seg) * passes + pass) * kRadixDigits + d];
-    store_status(my_status, kFlagPrefix | ((global_start + digit_count) & kValueMask));
-  } else {
-    store_status(my_status, kFlagAggregate | digit_count);
-    u64 exclusive = 0;
-    long long t = static_cast<long long>(tile) - 1;
-    while (true) {
-      const u64 v = wait_status(status + static_cast<u64>(t) * kRadixDigits + d,
-                                flags, 1);
-      exclusive += v & kValueMask;
-      if ((v >> 62) == 2) break;
-      --t;
+  if (d < kRadixDigits) {
+    sm.digit_excl[d] = static_cast<u32>(local_start);
+    u64* my_status = status + static_cast<u64>(tile) * kRadixDigits + d;
+    u64 global_start;
+    if (first_tile_of_segment) {
+      global_start =
+          digit_start[(static_cast<u64>(seg) * passes + pass) * kRadixDigits + d];
+      store_status(my_status, kFlagPrefix | ((global_start + digit_count) & kValueMask));
+    } else {
+      store_status(my_status, kFlagAggregate | digit_count);
+      u64 exclusive = 0;
+      long long t = static_cast<long long>(tile) - 1;
+      while (true) {
+        const u64 v = wait_status(status + static_cast<u64>(t) * kRadixDigits + d,
+                                  flags, 1);
+        exclusive += v & kValueMask;
+        if ((v >> 62) == 2) break;
+        --t;
+      }
+      global_start = exclusive;
+      store_status(my_status, kFlagPrefix | ((global_start + digit_count) & kValueMask));
     }
-    global_start = exclusive;
-    store_status(my_status, kFlagPrefix | ((global_start + digit_count) & kValueMask));
+    sm.digit_gbase[d] = static_cast<long long>(global_start) - static_cast<long long>(local_start);
   }
-  sm.digit_gbase[d] = static_cast<long long>(global_start) - static_cast<long long>(local_start);
   __syncthreads();
 
-  // Scatter keys to their tile-local sorted slot, then write runs out.
-  u32 local_slot[kSortItems];
+  // Keys and values to their tile-local sorted slot, then runs out.
+  u32 local_slot[kItems];
 #pragma unroll
-  for (int i = 0; i < kSortItems; ++i) {
+  for (int i = 0; i < kItems; ++i) {
     const u32 slot = warp_base + i * 32 + lane;
     if (slot < count) {
       const u32 digit = static_cast<u32>((key[i] >> shift) & 0xff);
@@ -242,14 +250,14 @@ radix_onesweep_kernel(const u64* __restrict__ keys_in,
   }
   __syncthreads();
 #pragma unroll
-  for (int i = 0; i < kSortItems; ++i) {
+  for (int i = 0; i < kItems; ++i) {
     const u32 slot = warp_base + i * 32 + lane;
     if (slot < count) sm.vals[local_slot[i]] = vals_in[first + slot];
   }
   __syncthreads();
   const u64 seg_first = segs.begin[seg];
   const u64 seg_end = segs.begin[seg + 1];
-  for (u32 s = threadIdx.x; s < count; s += kSortBlock) {
+  for (u32 s = threadIdx.x; s < count; s += kBlock) {
     const u64 k = sm.keys[s];
     const u32 digit = static_cast<u32>((k >> shift) & 0xff);
     const u64 out = static_cast<u64>(sm.digit_gbase[digit] + static_cast<long long>(s));
