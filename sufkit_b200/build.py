@@ -30,8 +30,25 @@ def up_to_date() -> bool:
     return all(p.stat().st_mtime <= stamp for p in inputs)
 
 
+DRIVER = HERE.parent / "tests" / "cpp" / "cuda_backend_driver"
+
+
+def build_driver(verbose: bool = False) -> Path:
+    """The C++ adapter's test driver (tests/cpp), linked against libsufgpu.so."""
+    src = DRIVER.with_suffix(".cpp")
+    if DRIVER.exists() and DRIVER.stat().st_mtime >= max(src.stat().st_mtime, LIB.stat().st_mtime):
+        return DRIVER
+    cmd = [os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-o", str(DRIVER), str(src),
+           f"-L{HERE}", "-lsufgpu", f"-Wl,-rpath,{HERE}"]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    return DRIVER
+
+
 def build(force: bool = False, verbose: bool = False) -> Path:
     if not force and up_to_date():
+        build_driver(verbose)
         return LIB
     nvcc = os.environ.get("NVCC", "nvcc")
     cmd = [nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
@@ -41,6 +58,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)
     os.replace(str(LIB) + ".tmp", LIB)
+    build_driver(verbose)
     return LIB
 
 
