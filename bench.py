@@ -41,7 +41,7 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="plain100m",
-                    choices=["plain100m", "plain4m", "batched"])
+                    choices=["plain100m", "plain4m", "plain3g", "batched"])
     ap.add_argument("--count", type=int, default=256,
                     help="references in the batched workload (1,024 in the full collection)")
     ap.add_argument("--batch-symbols", type=float, default=1.2e9,
@@ -72,6 +72,13 @@ def workload(name: str, scale: float = 1.0, count: int = 256):
         ref = synth.plain_4mbp()
         desc = ("plain 4 Mbp build: 4 contigs (1.5/1.2/0.8/0.5 Mbp), uniform ACGT, "
                 "0.1% N runs; Fast profile SA+ISA+raw LCP32, 32-bit storage")
+        return [ref.logical_text()], desc
+    if name == "plain3g":
+        ref = synth.human_scale_3gbp(scale)
+        desc = ("human-scale 3.1 Gbp plain build: 25 contigs (50-250 Mbp), GC 41%, 50% "
+                "interspersed repeats, 1% segmental duplications, 150 Mbp of N in runs of "
+                "10 kbp-3 Mbp; Low-memory profile: 64-bit construction, split40 SA storage, "
+                "byte-coded LCP (32-bit anchors), no resident ISA")
         return [ref.logical_text()], desc
     if name == "batched":
         refs = synth.uneven_collection(count=count, scale=scale)
@@ -262,15 +269,18 @@ def main():
     for item in args.tune:
         key, value = item.split("=", 1)
         ctx.set_tuning(key, int(value))
-    lcp_enc = sg.LcpEncoding.RAW32
-    isa_bits = 0 if args.workload == "batched" else 32
+    lcp_enc = sg.LcpEncoding.BYTE32 if args.workload == "plain3g" else sg.LcpEncoding.RAW32
+    isa_bits = 0 if args.workload in ("batched", "plain3g") else 32
+    sa_bits = 40 if args.workload == "plain3g" else 32
 
     # Device-resident inputs and outputs.
     n_total = sum(int(t.size) for t in texts)
     d_texts = [torch.from_numpy(t).to(dev) for t in texts]
+    lcp_dtype = torch.uint8 if lcp_enc == sg.LcpEncoding.BYTE32 else torch.int32
     d_out = [{"sa_low": torch.empty(t.size, dtype=torch.int32, device=dev),
+              "sa_high": torch.empty(t.size, dtype=torch.uint8, device=dev) if sa_bits == 40 else None,
               "isa_low": torch.empty(t.size, dtype=torch.int32, device=dev) if isa_bits else None,
-              "lcp": torch.empty(t.size, dtype=torch.int32, device=dev)} for t in texts]
+              "lcp": torch.empty(t.size, dtype=lcp_dtype, device=dev)} for t in texts]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
     def ptrs(o):
@@ -291,7 +301,7 @@ def main():
     def device_step():
         if len(texts) == 1:
             return ctx.build_device(d_texts[0].data_ptr(), int(texts[0].size), ptrs(d_out[0]),
-                                    sa_bits=32, isa_bits=isa_bits, lcp=lcp_enc)
+                                    sa_bits=sa_bits, isa_bits=isa_bits, lcp=lcp_enc)
         total = {"device_seconds": 0.0, "kernel_launches": 0}
         for b in batches:
             st = ctx.build_batch_device([(d_texts[j].data_ptr(), int(texts[j].size)) for j in b],
@@ -365,21 +375,24 @@ def main():
         d2h = 0
         for t in texts:
             planes = {}
-            for key, on in (("sa_low", True), ("isa_low", bool(isa_bits)), ("lcp", True)):
+            layout = (("sa_low", np.uint32, True), ("sa_high", np.uint8, sa_bits == 40),
+                      ("isa_low", np.uint32, bool(isa_bits)),
+                      ("lcp", np.uint8 if lcp_enc == sg.LcpEncoding.BYTE32 else np.uint32, True))
+            for key, dtype, on in layout:
                 if not on:
                     continue
-                arr = sg.pinned_array(int(t.size), np.uint32)
+                arr = sg.pinned_array(int(t.size), dtype)
                 keep.append(arr)
                 planes[key] = arr.ctypes.data
                 d2h += arr.nbytes
             host_out.append(planes)
         for _ in range(2):
-            e2e_step(ctx, pinned_text, host_out, isa_bits, lcp_enc)
+            e2e_step(ctx, pinned_text, host_out, isa_bits, lcp_enc, sa_bits)
         if dist is not None:
             dist.barrier()
         t0 = time.perf_counter()
         for _ in range(args.steps):
-            e2e_step(ctx, pinned_text, host_out, isa_bits, lcp_enc)
+            e2e_step(ctx, pinned_text, host_out, isa_bits, lcp_enc, sa_bits)
         e2e_sec = (time.perf_counter() - t0) / args.steps
         if dist is not None:
             t = torch.tensor([e2e_sec], dtype=torch.float64, device=dev)
@@ -406,7 +419,7 @@ def main():
                       for k in profile), key=lambda k: -k["ms_per_step"])
 
     whole = None
-    if rank == 0 and len(texts) == 1:
+    if rank == 0 and len(texts) == 1 and isa_bits and lcp_enc == sg.LcpEncoding.RAW32:
         # Algorithmic bytes of the whole build from this build's own exact
         # outputs (A_k, C depend only on the text).
         sa = d_out[0]["sa_low"].cpu().numpy().view(np.uint32)
@@ -448,11 +461,10 @@ def main():
         dist.destroy_process_group()
 
 
-def e2e_step(ctx, pinned_text, host_out, isa_bits, lcp_enc):
-    import sufkit_b200 as sg
+def e2e_step(ctx, pinned_text, host_out, isa_bits, lcp_enc, sa_bits=32):
     if len(pinned_text) == 1:
         t = pinned_text[0]
-        return ctx.build_device(t.ctypes.data, int(t.size), host_out[0], sa_bits=32,
+        return ctx.build_device(t.ctypes.data, int(t.size), host_out[0], sa_bits=sa_bits,
                                 isa_bits=isa_bits, lcp=lcp_enc)
     for lo in range(0, len(pinned_text), 64):
         ctx.build_batch_device([(t.ctypes.data, int(t.size)) for t in pinned_text[lo:lo + 64]],

@@ -103,6 +103,7 @@ typedef struct sufgpu_build_stats {
   uint32_t rounds;            /* doubling rounds after the seed */
   uint32_t seed_symbols;      /* symbols packed per seed key */
   uint64_t active_rows;       /* sum over rounds of still-unsorted rows */
+  uint64_t active_first;      /* rows still unsorted after the seed */
   uint64_t irreducible_long;  /* PLCP positions finished by a warp */
   uint64_t anchors;
   uint32_t kernel_launches;   /* kernels launched by this call */
@@ -180,7 +181,9 @@ SUFGPU_API sufgpu_status sufgpu_profile_entry(const sufgpu_ctx *ctx, uint32_t in
  *   "seed_symbols"  symbols packed per seed key, 0 = as many as fit 64 bits;
  *   "ballot_rank"   1 = onesweep ranks digits with ballots, 0 = match-any;
  *   "ballot_min_elems" smallest sort that uses ballot ranking;
- *   "sort_block"    onesweep threads per 4096-key tile: 256 or 512.
+ *   "sort_block"    onesweep threads per 4096-key tile: 256 or 512;
+ *   "packed_max_bits" instances of at most 2^v symbols use the packed
+ *                   keys-only seed (index in the low key bits); 0 = never.
  * Results are identical for every setting; only speed changes. */
 SUFGPU_API sufgpu_status sufgpu_set_tuning(sufgpu_ctx *ctx, const char *key, int64_t value);
 

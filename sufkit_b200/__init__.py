@@ -82,7 +82,8 @@ class _Stats(ctypes.Structure):
                 ("total_seconds", ctypes.c_double), ("device_seconds", ctypes.c_double),
                 ("symbols", ctypes.c_uint64),
                 ("rounds", ctypes.c_uint32), ("seed_symbols", ctypes.c_uint32),
-                ("active_rows", ctypes.c_uint64), ("irreducible_long", ctypes.c_uint64),
+                ("active_rows", ctypes.c_uint64), ("active_first", ctypes.c_uint64),
+                ("irreducible_long", ctypes.c_uint64),
                 ("anchors", ctypes.c_uint64), ("kernel_launches", ctypes.c_uint32),
                 ("reserved", ctypes.c_uint32)]
 

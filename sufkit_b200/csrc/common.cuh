@@ -159,4 +159,17 @@ __device__ __forceinline__ u32 find_segment(const u64* begin, u32 count,
   return lo;
 }
 
+// Per-thread cache of the segment holding the last looked-up element; kernels
+// whose threads walk increasing indices search only when they leave it.
+struct SegCursor {
+  u64 lo = 1, hi = 0;  // empty until the first lookup
+  u32 j = 0;
+  __device__ __forceinline__ void locate(const u64* begin, u32 count, u64 x) {
+    if (x >= lo && x < hi) return;
+    j = count == 1 ? 0 : find_segment(begin, count, x);
+    lo = begin[j];
+    hi = begin[j + 1];
+  }
+};
+
 }  // namespace sufgpu

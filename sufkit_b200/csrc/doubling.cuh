@@ -97,10 +97,13 @@ struct SeedSmem {
   __align__(16) u8 window[kSeedTile + kSeedHalo];
 };
 
+// packed_shift > 0 selects the packed seed: key = (prefix << packed_shift) |
+// instance-local index (no value array); histograms then cover the passes
+// over bits [packed_shift, packed_shift + 8*passes).
 static __global__ void __launch_bounds__(kSeedBlock)
 seed_keys_kernel(const u8* __restrict__ text, u64 n, Segments segs,
                  const u16* __restrict__ code_table, u32 bits, u32 symbols,
-                 u32 passes, u32* __restrict__ hist_out,
+                 u32 passes, u32* __restrict__ hist_out, u32 packed_shift,
                  u64* __restrict__ keys, u32* __restrict__ vals) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SeedSmem& sm = *reinterpret_cast<SeedSmem*>(smem_raw);
@@ -122,6 +125,7 @@ seed_keys_kernel(const u8* __restrict__ text, u64 n, Segments segs,
   u64 pos = tile_first + local0;
   u32 seg = segs.count == 1 ? 0 : (pos < n ? find_segment(segs.begin, segs.count, pos) : block_seg);
   u64 end = pos < n ? segs.begin[seg + 1] : n;
+  u64 seg_lo = pos < n ? segs.begin[seg] : 0;
   u64 key = 0;
   bool fresh = true;
   for (int r = 0; r < kSeedRun; ++r, ++pos) {
@@ -129,6 +133,7 @@ seed_keys_kernel(const u8* __restrict__ text, u64 n, Segments segs,
     if (valid && pos >= end) {  // crossed into the next instance
       seg = find_segment(segs.begin, segs.count, pos);
       end = segs.begin[seg + 1];
+      seg_lo = segs.begin[seg];
       fresh = true;
     }
     const u32 local = local0 + r;
@@ -145,7 +150,7 @@ seed_keys_kernel(const u8* __restrict__ text, u64 n, Segments segs,
         const u32 c = q < end ? sm.code[sm.window[local + symbols - 1]] : 0u;
         key = ((key << bits) | c) & mask;
       }
-      sm.keys[local] = key;
+      sm.keys[local] = packed_shift ? (key << packed_shift) | (pos - seg_lo) : key;
     }
     // Histogram of every pass; a warp whose lanes agree adds once.
     const bool mine = valid && seg == block_seg;
@@ -167,7 +172,7 @@ seed_keys_kernel(const u8* __restrict__ text, u64 n, Segments segs,
     const u64 at = tile_first + i;
     if (at < n) {
       keys[at] = sm.keys[i];
-      vals[at] = static_cast<u32>(at);
+      if (!packed_shift) vals[at] = static_cast<u32>(at);
     }
   }
   for (u32 i = threadIdx.x; i < passes * 256; i += kSeedBlock) {
@@ -180,9 +185,16 @@ seed_keys_kernel(const u8* __restrict__ text, u64 n, Segments segs,
 // r; the one full random scatter of the build, at the device's scattered-store
 // rate) and the initial active list.  Two scans share the tile: a max-scan of
 // head rows and a sum-scan of active flags (the compaction).
+// Also writes the LCP of every seed-group head row straight from the keys: two
+// different seed keys share exactly (leading zeros of their XOR - unused top
+// bits) / bits symbols.  Rows inside a seed group get kLcpUnknown and are
+// resolved from the text later (their LCP is at least the seed length).
+constexpr u32 kLcpUnknown = 0xffffffffu;
+
 static __global__ void __launch_bounds__(kScanBlock)
-seed_rank_kernel(const u64* __restrict__ keys, const u32* __restrict__ sa,
-                 u64 n, Segments segs, u32* __restrict__ rank,
+seed_rank_kernel(const u64* __restrict__ keys, u32* __restrict__ sa,
+                 u64 n, Segments segs, u32 packed_shift, u32 bits, u32 symbols,
+                 u32* __restrict__ rank, u32* __restrict__ lcp,
                  u32* __restrict__ active, u64* status_max, u64* status_sum,
                  u32* tile_counter, u64* active_count, DeviceFlags* flags) {
   __shared__ u64 warp_smem[kScanBlock / 32];
@@ -191,17 +203,31 @@ seed_rank_kernel(const u64* __restrict__ keys, const u32* __restrict__ sa,
   const u32 tile = claim_tile(tile_counter, &tile_slot);
   const u64 row0 = static_cast<u64>(tile) * kScanTile + threadIdx.x * kScanItems;
 
+  // Compare only the prefix part of packed keys.
   u64 k[kScanItems + 2];  // rows row0-1 .. row0+kScanItems
 #pragma unroll
   for (int i = 0; i < kScanItems + 2; ++i) {
     const long long r = static_cast<long long>(row0) - 1 + i;
-    k[i] = (r >= 0 && static_cast<u64>(r) < n) ? keys[r] : 0;
+    k[i] = (r >= 0 && static_cast<u64>(r) < n) ? keys[r] >> packed_shift : 0;
   }
+  SegCursor cur;
   bool head[kScanItems + 1];
+  const u32 unused_top = 64 - bits * symbols;
 #pragma unroll
   for (int i = 0; i < kScanItems + 1; ++i) {
     const u64 r = row0 + i;
-    head[i] = r >= n || is_segment_start(segs, r) || k[i + 1] != k[i];
+    bool start = r >= n;
+    if (!start) {
+      cur.locate(segs.begin, segs.count, r);
+      start = r == cur.lo;
+    }
+    head[i] = start || k[i + 1] != k[i];
+    if (i < kScanItems && r < n) {
+      u32 v = kLcpUnknown;
+      if (start) v = 0;
+      else if (head[i]) v = (static_cast<u32>(__clzll(static_cast<long long>(k[i + 1] ^ k[i]))) - unused_top) / bits;
+      lcp[r] = v;
+    }
   }
   u64 head_max = 0;  // inclusive running max within the thread
   u32 act = 0;
@@ -227,12 +253,24 @@ seed_rank_kernel(const u64* __restrict__ keys, const u32* __restrict__ sa,
   __syncthreads();
   u64 running_max = tile_prefix[0] > excl_max ? tile_prefix[0] : excl_max;
   u64 out = tile_prefix[1] + excl_sum;
+  const u64 local_mask = packed_shift ? (1ull << packed_shift) - 1 : 0;
 #pragma unroll
   for (int i = 0; i < kScanItems; ++i) {
     const u64 r = row0 + i;
     if (r < n) {
       if (head[i]) running_max = r;
-      const u32 p = sa[r];
+      u32 p;
+      if (packed_shift) {
+        cur.locate(segs.begin, segs.count, r);
+        p = static_cast<u32>(cur.lo + (keys[r] & local_mask));
+        sa[r] = p;
+      } else {
+        p = sa[r];
+      }
+      if (p >= n) {
+        flag_error(flags, kErrBounds);
+        continue;
+      }
       rank[p] = static_cast<u32>(running_max);
       if (!(head[i] && head[i + 1])) active[out++] = p;
     }

@@ -84,6 +84,7 @@ struct Layout {
   u32* v0;
   u32* x;
   u32* y;
+  u32* lcp;          // row-order LCP (seed-group heads from the seed keys)
   u64* status;       // look-back words: radix (tiles*256) or 2 scan arrays
   u64 status_words;
   u32* hist;         // radix histograms [seg][pass][256]
@@ -117,6 +118,7 @@ Layout plan_layout(u8* base, u64 n, u32 segments) {
   l.v0 = reinterpret_cast<u32*>(take(n4));
   l.x = reinterpret_cast<u32*>(take(n4));
   l.y = reinterpret_cast<u32*>(take(n4));
+  l.lcp = reinterpret_cast<u32*>(take(n4));
   const u64 radix_tiles = (n + kSortTile - 1) / kSortTile + segments;
   const u64 scan_tiles = (n + kScanTile - 1) / kScanTile + 1;
   l.status_words = std::max<u64>(radix_tiles * kRadixDigits, 2 * scan_tiles);
@@ -139,20 +141,28 @@ Layout plan_layout(u8* base, u64 n, u32 segments) {
 using OnesweepFn = void (*)(const u64*, const u32*, u64*, u32*, SortSegments, u32, u32, u32,
                             const u64*, u64*, u32*, DeviceFlags*);
 
-// Onesweep variants: ranking by ballots or match-any, 256x16 or 512x8 tiles.
+// Onesweep variants: ranking by ballots or match-any, 256x16 or 512x8 tiles,
+// key-value pairs or keys only.
 struct OnesweepVariant {
   OnesweepFn fn;
   u32 block;
   u64 smem;
 };
 
-OnesweepVariant onesweep_variant(bool ballot, u32 block) {
+template <bool kVals>
+OnesweepVariant onesweep_variant_t(bool ballot, u32 block) {
   if (block == 512) {
-    return {ballot ? radix_onesweep_kernel<true, 512, 8> : radix_onesweep_kernel<false, 512, 8>,
+    return {ballot ? radix_onesweep_kernel<true, 512, 8, kVals>
+                   : radix_onesweep_kernel<false, 512, 8, kVals>,
             512, sizeof(OnesweepSmem<512>)};
   }
-  return {ballot ? radix_onesweep_kernel<true, 256, 16> : radix_onesweep_kernel<false, 256, 16>,
+  return {ballot ? radix_onesweep_kernel<true, 256, 16, kVals>
+                 : radix_onesweep_kernel<false, 256, 16, kVals>,
           256, sizeof(OnesweepSmem<256>)};
+}
+
+OnesweepVariant onesweep_variant(bool ballot, u32 block, bool vals) {
+  return vals ? onesweep_variant_t<true>(ballot, block) : onesweep_variant_t<false>(ballot, block);
 }
 
 }  // namespace
@@ -211,6 +221,8 @@ struct sufgpu_ctx {
   bool ballot_rank = true;
   // Ballot ranking only pays off on large sorts; smaller ones use match-any.
   u64 ballot_min_elems = u64(1) << 23;
+  // Largest instance index width for the packed (keys-only) seed; 0 = never.
+  u32 packed_max_bits = 24;
   // Onesweep block size (256 threads x 16 keys or 512 x 8).
   u32 sort_block = 256;
 };
@@ -228,6 +240,7 @@ struct Engine {
   // buffer (free for PHI flags and byte-coded primaries).
   u32* sa = nullptr;
   u32* spare = nullptr;
+  u32 seed_length = 0;  // symbols every seed group shares
 
   explicit Engine(sufgpu_ctx& ctx) : c(ctx) {}
 
@@ -325,8 +338,8 @@ struct Engine {
       if (!needed[p]) continue;
       zero(L.status, u64(total_tiles) * kRadixDigits * 8);
       zero(L.counters, 4);
-      const OnesweepVariant v =
-          onesweep_variant(c.ballot_rank && elems >= c.ballot_min_elems, c.sort_block);
+      const OnesweepVariant v = onesweep_variant(c.ballot_rank && elems >= c.ballot_min_elems,
+                                                 c.sort_block, vals != nullptr);
       launch(name, elems * 24, v.fn, total_tiles, v.block, v.smem,
              kin, vin, kout, vout, ss, begin_bit + p * kRadixBits, p, passes,
              L.digit_start, L.status, L.counters, L.flags);
@@ -372,6 +385,20 @@ struct Engine {
     const u32 bits = std::max<u32>(1, bits_for(sigma));
     u32 symbols = 64 / bits;
     if (c.seed_symbols) symbols = std::min(symbols, c.seed_symbols);
+    // Packed seed: when every instance fits 2^packed_max_bits symbols, its
+    // local index rides in the low key bits and the sort moves keys only.
+    u64 longest = 1;
+    for (u32 j = 0; j < segs; ++j) longest = std::max<u64>(longest, begin[j + 1] - begin[j]);
+    const u32 index_bits = std::max<u32>(1, bits_for(longest - 1));
+    u32 packed_shift = 0;
+    if (c.packed_max_bits && index_bits <= c.packed_max_bits) {
+      u32 packed_symbols = (64 - index_bits) / bits;
+      if (c.seed_symbols) packed_symbols = std::min(packed_symbols, c.seed_symbols);
+      if (packed_symbols >= std::min<u32>(symbols, 12)) {
+        packed_shift = index_bits;
+        symbols = packed_symbols;
+      }
+    }
     st.seed_symbols = symbols;
     upload(L.code, code, sizeof(code));
 
@@ -381,20 +408,30 @@ struct Engine {
     const u32 seed_bits = bits * symbols;
     const u32 seed_passes = (seed_bits + kRadixBits - 1) / kRadixBits;
     zero(L.hist, u64(segs) * seed_passes * kRadixDigits * 4);
-    launch("seed_keys", n * 13, seed_keys_kernel, (n + kSeedTile - 1) / kSeedTile, kSeedBlock,
-           sizeof(SeedSmem), L.text, n, segments(), static_cast<const u16*>(L.code), bits,
-           symbols, seed_passes, L.hist, L.k0, L.v0);
+    launch("seed_keys", packed_shift ? n * 9 : n * 13, seed_keys_kernel,
+           (n + kSeedTile - 1) / kSeedTile, kSeedBlock, sizeof(SeedSmem), L.text, n, segments(),
+           static_cast<const u16*>(L.code), bits, symbols, seed_passes, L.hist, packed_shift,
+           L.k0, L.v0);
     u64* keys = L.k0;
-    const bool swapped = radix_sort("seed_onesweep", L.k0, L.v0, L.k1, L.sa, L.seg_begin, L.seg_tiles,
-                                    segs, seed_tiles, n, 0, seed_bits, true, true);
-    if (swapped) {
-      keys = L.k1;
+    if (packed_shift) {
+      const bool swapped = radix_sort("seed_onesweep", L.k0, nullptr, L.k1, nullptr, L.seg_begin,
+                                      L.seg_tiles, segs, seed_tiles, n, packed_shift,
+                                      packed_shift + seed_bits, true, true);
+      keys = swapped ? L.k1 : L.k0;
       sa = L.sa;
       spare = L.v0;
     } else {
-      keys = L.k0;
-      sa = L.v0;
-      spare = L.sa;
+      const bool swapped = radix_sort("seed_onesweep", L.k0, L.v0, L.k1, L.sa, L.seg_begin,
+                                      L.seg_tiles, segs, seed_tiles, n, 0, seed_bits, true, true);
+      if (swapped) {
+        keys = L.k1;
+        sa = L.sa;
+        spare = L.v0;
+      } else {
+        keys = L.k0;
+        sa = L.v0;
+        spare = L.sa;
+      }
     }
     // Seed ranks and the initial active list (in x).
     const u64 scan_tiles = (n + kScanTile - 1) / kScanTile;
@@ -402,9 +439,11 @@ struct Engine {
     zero(L.counters, 4);
     u64* status_max = L.status;
     u64* status_sum = L.status + scan_tiles + 1;
-    launch("seed_rank", n * 16, seed_rank_kernel, scan_tiles, kScanBlock, 0, keys, sa, n,
-           segments(), L.rank, L.x, status_max, status_sum, L.counters, L.scalars + 0, L.flags);
+    launch("seed_rank", n * 16, seed_rank_kernel, scan_tiles, kScanBlock, 0,
+           static_cast<const u64*>(keys), sa, n, segments(), packed_shift, bits, symbols,
+           L.rank, L.lcp, L.x, status_max, status_sum, L.counters, L.scalars + 0, L.flags);
     u64 active = read_scalar(0);
+    st.active_first = active;
 
     // Rounds.  act and other alternate between x and the spare SA-sized
     // buffer; y holds the per-group tables.
@@ -412,6 +451,7 @@ struct Engine {
     u32* other = spare;
     const u32 second_bits = bits_for(n);
     u64 h = symbols;
+    seed_length = symbols;
     u32 rounds = 0;
     while (active > 0) {
       if (++rounds > 64) throw BuildError{SUFGPU_BUILD_FAILURE, "prefix doubling did not converge"};
@@ -464,15 +504,15 @@ struct Engine {
     u64 longs;
   };
   LcpPhase lcp_phase() {
-    u32* lcp = reinterpret_cast<u32*>(L.k1);
+    u32* lcp = L.lcp;
     LongRow* longs = reinterpret_cast<LongRow*>(L.x);  // x and y: 8n bytes
     const u64 long_cap = std::max<u64>(n, 1) * 8 / sizeof(LongRow);
     u32* pending = spare;
     const u64 pending_cap = n;
     zero(L.scalars + 5, 16);
-    launch("lcp_rows", n * 13, lcp_rows_kernel, grid_stride_blocks(n, 256), 256, 0, L.text,
-           static_cast<const u32*>(sa), n, segments(), lcp, longs, long_cap, L.scalars + 5,
-           pending, pending_cap, L.scalars + 6, L.flags);
+    launch("lcp_rows", n * 4 + st.active_first * 9, lcp_rows_kernel, grid_stride_blocks(n, 256),
+           256, 0, L.text, static_cast<const u32*>(sa), n, segments(), seed_length, lcp, longs,
+           long_cap, L.scalars + 5, pending, pending_cap, L.scalars + 6, L.flags);
     SG_CUDA(cudaMemcpyAsync(c.host_scalars + 5, L.scalars + 5, 16, cudaMemcpyDeviceToHost, c.stream));
     sync();
     const u64 q_all = c.host_scalars[5], pend_all = c.host_scalars[6];
@@ -483,7 +523,7 @@ struct Engine {
     st.irreducible_long = q;
     u64* spos = L.k0;
     u64* spos_alt = L.k0 + n / 2 + 1;
-    u32* sval = reinterpret_cast<u32*>(L.k1) + n;
+    u32* sval = reinterpret_cast<u32*>(L.k1);
     u32* sval_alt = sval + n / 2 + 1;
     const u64* sorted_pos = spos;
     const u32* sorted_val = sval;
@@ -683,9 +723,11 @@ sufgpu_status sufgpu_create(sufgpu_ctx** out, int device) {
     for (auto& ev : ctx->ev) SG_CUDA(cudaEventCreate(&ev));
     for (bool ballot : {true, false}) {
       for (u32 block : {256u, 512u}) {
-        const OnesweepVariant v = onesweep_variant(ballot, block);
-        SG_CUDA(cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(v.smem)));
+        for (bool vals : {true, false}) {
+          const OnesweepVariant v = onesweep_variant(ballot, block, vals);
+          SG_CUDA(cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(v.smem)));
+        }
       }
     }
   } catch (const CudaError& err) {
@@ -957,6 +999,9 @@ extern "C" sufgpu_status sufgpu_set_tuning(sufgpu_ctx* ctx, const char* key, int
   } else if (k == "ballot_min_elems") {
     if (value < 0) return fail(ctx, SUFGPU_INVALID_INPUT, "ballot_min_elems must be >= 0");
     ctx->ballot_min_elems = static_cast<u64>(value);
+  } else if (k == "packed_max_bits") {
+    if (value < 0 || value > 32) return fail(ctx, SUFGPU_INVALID_INPUT, "packed_max_bits out of range");
+    ctx->packed_max_bits = static_cast<u32>(value);
   } else if (k == "sort_block") {
     if (value != 256 && value != 512) return fail(ctx, SUFGPU_INVALID_INPUT, "sort_block must be 256 or 512");
     ctx->sort_block = static_cast<u32>(value);

@@ -1,8 +1,9 @@
 // LCP kernels (row order), byte coding and overflow anchors.
 //
-// LCP[r] = lcp(SA[r-1], SA[r]).  Every row first compares up to 64 bytes
-// directly (on genomic text almost every row ends there; the text is read
-// through L2).  A row whose first 64 bytes match is "long":
+// LCP[r] = lcp(SA[r-1], SA[r]).  Rows at seed-group boundaries already carry
+// their LCP (from the seed keys).  Every other row compares up to 64 bytes
+// past the seed length directly (on genomic text almost every row ends
+// there).  A row whose next 64 bytes also match is "long":
 //   * if its suffix b = SA[r] is irreducible (text[b-1] != text[a-1] for
 //     a = SA[r-1], or b or a starts its instance), a warp finishes the compare;
 //   * otherwise b is reducible: PLCP[b] = PLCP[b-1] - 1, and by induction
@@ -60,28 +61,34 @@ __device__ __forceinline__ u64 warp_append(u64* counter, bool take) {
 
 // Row pass.  lcp receives final values for short rows; long rows go to the
 // irreducible queue or the pending (reducible) list.
+// With known_prefix > 0, rows whose lcp[] is already set (seed-group heads,
+// resolved from the seed keys) are skipped and the others start comparing at
+// known_prefix, the seed length they are known to share.
 static __global__ void __launch_bounds__(256)
 lcp_rows_kernel(const u8* __restrict__ text, const u32* __restrict__ sa, u64 n,
-                Segments segs, u32* __restrict__ lcp, LongRow* __restrict__ longs,
-                u64 long_cap, u64* long_count, u32* __restrict__ pending,
-                u64 pending_cap, u64* pending_count, DeviceFlags* flags) {
+                Segments segs, u32 known_prefix, u32* __restrict__ lcp,
+                LongRow* __restrict__ longs, u64 long_cap, u64* long_count,
+                u32* __restrict__ pending, u64 pending_cap, u64* pending_count,
+                DeviceFlags* flags) {
   const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
   const u64 rows = (n + 31) / 32 * 32;  // whole warps stay converged
+  SegCursor cur;
   for (u64 r = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; r < rows; r += stride) {
     bool is_long = false, irreducible = false;
     u32 b = 0, a = 0, l = 0;
-    if (r < n) {
+    if (r < n && (known_prefix == 0 || lcp[r] == kLcpUnknown)) {
       b = sa[r];
-      const u64 seg_first = segs.count == 1 ? 0 : segs.begin[find_segment(segs.begin, segs.count, r)];
+      cur.locate(segs.begin, segs.count, r);
+      const u64 seg_first = cur.lo;
       if (r == seg_first) {
         lcp[r] = 0;
       } else {
         a = sa[r - 1];
-        const u64 end = segment_end(segs, r);
+        const u64 end = cur.hi;
         const u64 far = a > b ? a : b;
         const u64 limit = end - far;
-        const u64 budget = limit < kDirectLcpBytes ? limit : kDirectLcpBytes;
-        u64 m = 0;
+        const u64 budget = limit < known_prefix + kDirectLcpBytes ? limit : known_prefix + kDirectLcpBytes;
+        u64 m = known_prefix < limit ? known_prefix : limit;
         bool mismatch = false;
         while (m < budget) {
           const u64 x = load8(text, b + m) ^ load8(text, a + m);

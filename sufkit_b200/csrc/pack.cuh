@@ -15,9 +15,13 @@ static __global__ void __launch_bounds__(256)
 pack_kernel(const u32* __restrict__ values, u64 n, Segments segs, u32 bits,
             void* __restrict__ low, void* __restrict__ high) {
   const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+  SegCursor cur;
   for (u64 r = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; r < n; r += stride) {
     u64 v = values[r];
-    if (segs.count > 1) v -= segs.begin[find_segment(segs.begin, segs.count, r)];
+    if (segs.count > 1) {
+      cur.locate(segs.begin, segs.count, r);
+      v -= cur.lo;
+    }
     if (bits == 64) {
       static_cast<u64*>(low)[r] = v;
     } else {

@@ -125,7 +125,9 @@ struct OnesweepSmem {
   u32 tile;
 };
 
-template <bool kBallot, int kBlock, int kItems>
+// kVals = false sorts keys only (vals_in/vals_out unused): the packed seed
+// carries each suffix's instance-local index in the low key bits.
+template <bool kBallot, int kBlock, int kItems, bool kVals = true>
 static __global__ void __launch_bounds__(kBlock)
 radix_onesweep_kernel(const u64* __restrict__ keys_in,
                       const u32* __restrict__ vals_in,
@@ -249,10 +251,12 @@ radix_onesweep_kernel(const u64* __restrict__ keys_in,
     }
   }
   __syncthreads();
+  if (kVals) {
 #pragma unroll
-  for (int i = 0; i < kItems; ++i) {
-    const u32 slot = warp_base + i * 32 + lane;
-    if (slot < count) sm.vals[local_slot[i]] = vals_in[first + slot];
+    for (int i = 0; i < kItems; ++i) {
+      const u32 slot = warp_base + i * 32 + lane;
+      if (slot < count) sm.vals[local_slot[i]] = vals_in[first + slot];
+    }
   }
   __syncthreads();
   const u64 seg_first = segs.begin[seg];
@@ -266,7 +270,7 @@ radix_onesweep_kernel(const u64* __restrict__ keys_in,
       continue;
     }
     keys_out[out] = k;
-    vals_out[out] = sm.vals[s];
+    if (kVals) vals_out[out] = sm.vals[s];
   }
 }
 

@@ -152,3 +152,11 @@ def test_invalid_inputs(ctx):
     assert e.value.code == sg.ErrorCode.INVALID_INPUT
     r = ctx.build(np.zeros(0, np.uint8))
     assert r.sa_low.size == 0
+
+
+def test_workload3_scaled_low_memory(ctx):
+    """Workload 3 shape at 1% (31 Mbp, long N runs and segmental duplications):
+    split40 SA and byte-coded LCP word for word against the reference."""
+    t = synth.human_scale_3gbp(scale=0.01).logical_text()
+    r = check_full(ctx, t, sa_bits=40, isa_bits=0, lcp=sg.LcpEncoding.BYTE32)
+    assert r.stats["rounds"] >= 10
