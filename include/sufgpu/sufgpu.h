@@ -187,6 +187,66 @@ SUFGPU_API sufgpu_status sufgpu_profile_entry(const sufgpu_ctx *ctx, uint32_t in
  * Results are identical for every setting; only speed changes. */
 SUFGPU_API sufgpu_status sufgpu_set_tuning(sufgpu_ctx *ctx, const char *key, int64_t value);
 
+/* ------------------------------------------------------------------------
+ * Served builds (continuous batching).  A server owns one device arena and a
+ * worker thread.  Requests are admitted while a free arena range can hold
+ * them (HBM footprint); admitted references are seeded as a group and then
+ * advance one doubling round per engine iteration side by side with every
+ * other in-flight reference (each with its own prefix length), so requests
+ * that arrive while others are on the GPU join the running work at the next
+ * round.  A reference leaves as soon as it has no unsorted rows: its LCP is
+ * computed, its planes are copied into the caller's outputs and its arena
+ * range is freed.  Each result equals sufgpu_build of the same text.
+ * The reference (sufkit) has no counterpart; it builds one reference per
+ * SuffixArray::Build call on the calling thread.
+ * ---------------------------------------------------------------------- */
+typedef struct sufgpu_server sufgpu_server;
+
+typedef struct sufgpu_server_config {
+  uint64_t capacity_symbols; /* arena size in symbols (0 = 2^29); ~53 B each */
+  uint32_t max_instances;    /* in-flight references (0 = 1024) */
+  uint32_t flags;
+} sufgpu_server_config;
+
+typedef struct sufgpu_request_info {
+  double queue_seconds;   /* submit -> admitted */
+  double latency_seconds; /* submit -> outputs complete */
+  uint32_t rounds;        /* doubling rounds the reference took */
+  uint32_t seed_symbols;
+  sufgpu_anchors anchors; /* byte-coded encodings; valid until release */
+} sufgpu_request_info;
+
+typedef struct sufgpu_server_stats {
+  uint64_t completed;
+  uint64_t symbols;
+  uint64_t iterations;
+  uint64_t max_inflight;
+  uint64_t queued;
+  uint64_t inflight;
+  double p50_seconds;
+  double p99_seconds;
+  double span_seconds;      /* first submit -> last completion */
+  double symbols_per_second;
+} sufgpu_server_stats;
+
+SUFGPU_API sufgpu_status sufgpu_server_create(sufgpu_server **server, int device,
+                                              const sufgpu_server_config *config);
+/* Finishes every queued and in-flight request, then frees the server. */
+SUFGPU_API void sufgpu_server_destroy(sufgpu_server *server);
+/* text and the output planes are caller memory (host or device) that must
+ * stay valid until the request completes. */
+SUFGPU_API sufgpu_status sufgpu_server_submit(sufgpu_server *server, const uint8_t *text,
+                                              uint64_t n, const sufgpu_build_desc *desc,
+                                              const sufgpu_outputs *out, uint64_t *ticket);
+/* Blocks until the request completes; returns its status. */
+SUFGPU_API sufgpu_status sufgpu_server_wait(sufgpu_server *server, uint64_t ticket,
+                                            sufgpu_request_info *info);
+SUFGPU_API sufgpu_status sufgpu_server_poll(sufgpu_server *server, uint64_t ticket, int *done);
+/* Forgets a completed request (its anchors become invalid). */
+SUFGPU_API sufgpu_status sufgpu_server_release(sufgpu_server *server, uint64_t ticket);
+SUFGPU_API sufgpu_status sufgpu_server_get_stats(sufgpu_server *server,
+                                                 sufgpu_server_stats *stats);
+
 /* Pinned host memory helpers (fast transfers for callers that can use them). */
 SUFGPU_API void *sufgpu_host_alloc(uint64_t bytes);
 SUFGPU_API void sufgpu_host_free(void *ptr);

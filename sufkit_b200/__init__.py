@@ -91,6 +91,28 @@ class _Stats(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
 
 
+class _ServerConfig(ctypes.Structure):
+    _fields_ = [("capacity_symbols", ctypes.c_uint64), ("max_instances", ctypes.c_uint32),
+                ("flags", ctypes.c_uint32)]
+
+
+class _RequestInfo(ctypes.Structure):
+    _fields_ = [("queue_seconds", ctypes.c_double), ("latency_seconds", ctypes.c_double),
+                ("rounds", ctypes.c_uint32), ("seed_symbols", ctypes.c_uint32),
+                ("anchors", _Anchors)]
+
+
+class _ServerStats(ctypes.Structure):
+    _fields_ = [("completed", ctypes.c_uint64), ("symbols", ctypes.c_uint64),
+                ("iterations", ctypes.c_uint64), ("max_inflight", ctypes.c_uint64),
+                ("queued", ctypes.c_uint64), ("inflight", ctypes.c_uint64),
+                ("p50_seconds", ctypes.c_double), ("p99_seconds", ctypes.c_double),
+                ("span_seconds", ctypes.c_double), ("symbols_per_second", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 class _Instance(ctypes.Structure):
     _fields_ = [("text", ctypes.c_void_p), ("n", ctypes.c_uint64),
                 ("out", _Outputs), ("anchors", _Anchors)]
@@ -125,6 +147,18 @@ _SIGNATURES = {
     "sufgpu_set_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int64]),
     "sufgpu_lcp_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
                                           ctypes.c_void_p, ctypes.c_void_p]),
+    "sufgpu_server_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
+                                            ctypes.POINTER(_ServerConfig)]),
+    "sufgpu_server_destroy": (None, [ctypes.c_void_p]),
+    "sufgpu_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                            ctypes.POINTER(_Desc), ctypes.POINTER(_Outputs),
+                                            ctypes.POINTER(ctypes.c_uint64)]),
+    "sufgpu_server_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64,
+                                          ctypes.POINTER(_RequestInfo)]),
+    "sufgpu_server_poll": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64,
+                                          ctypes.POINTER(ctypes.c_int)]),
+    "sufgpu_server_release": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    "sufgpu_server_get_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(_ServerStats)]),
     "sufgpu_host_alloc": (ctypes.c_void_p, [ctypes.c_uint64]),
     "sufgpu_host_free": (None, [ctypes.c_void_p]),
     "sufgpu_encode_fasta": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_uint64,
@@ -396,6 +430,73 @@ class Context:
         if rc != 0:
             raise SufkitError(ErrorCode.BUILD_FAILURE, f"divsufsort returned {rc}: {self._error()}")
         return sa
+
+
+class Server:
+    """Continuously batched builds (sufgpu_server_*): submit references while
+    others are on the GPU; each result equals Context.build of the same text."""
+
+    def __init__(self, device: int = 0, capacity_symbols: int = 0, max_instances: int = 0):
+        lib = library()
+        handle = ctypes.c_void_p()
+        cfg = _ServerConfig(capacity_symbols, max_instances, 0)
+        status = lib.sufgpu_server_create(ctypes.byref(handle), device, ctypes.byref(cfg))
+        if status != 0:
+            _raise(status, "cannot create the build server: " + lib.sufgpu_last_error(None).decode())
+        self._lib = lib
+        self._h = handle
+        self._pending: dict[int, tuple] = {}
+
+    def submit(self, text, sa_bits: int = 32, isa_bits: int = 0,
+               lcp: LcpEncoding = LcpEncoding.RAW32, validate: bool = False) -> int:
+        t = np.ascontiguousarray(_as_text(text))
+        lcp = LcpEncoding(lcp)
+        planes = Context._alloc_outputs(None, int(t.size), sa_bits, isa_bits, lcp)
+        desc = _Desc(sa_bits, isa_bits, int(lcp), FLAG_VALIDATE if validate else 0)
+        out = Context._outputs(planes)
+        ticket = ctypes.c_uint64()
+        status = self._lib.sufgpu_server_submit(self._h, _ptr(t), int(t.size), ctypes.byref(desc),
+                                                ctypes.byref(out), ctypes.byref(ticket))
+        if status != 0:
+            _raise(status, "submit rejected")
+        # Keep the text and the planes alive until the request completes.
+        self._pending[ticket.value] = (t, planes, lcp)
+        return ticket.value
+
+    def wait(self, ticket: int) -> BuildResult:
+        info = _RequestInfo()
+        status = self._lib.sufgpu_server_wait(self._h, ticket, ctypes.byref(info))
+        t, planes, lcp = self._pending.pop(ticket)
+        if status != 0:
+            self._lib.sufgpu_server_release(self._h, ticket)
+            _raise(status, f"served build {ticket} failed")
+        pos, val = Context._anchors(info.anchors, lcp)
+        self._lib.sufgpu_server_release(self._h, ticket)
+        stats = {"queue_seconds": info.queue_seconds, "latency_seconds": info.latency_seconds,
+                 "rounds": info.rounds, "seed_symbols": info.seed_symbols}
+        return BuildResult(anchor_positions=pos, anchor_values=val, stats=stats, **planes)
+
+    def stats(self) -> dict:
+        st = _ServerStats()
+        self._lib.sufgpu_server_get_stats(self._h, ctypes.byref(st))
+        return st.as_dict()
+
+    def close(self):
+        if self._h:
+            self._lib.sufgpu_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 @dataclass

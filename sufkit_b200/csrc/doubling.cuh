@@ -23,12 +23,16 @@ constexpr int kScanTile = kScanBlock * kScanItems;
 
 // Segment bounds for one instance-aware kernel.  count == 1 with begin = {0, n}
 // for a single reference.
+// When `end` is set the segments need not be contiguous (the served engine's
+// arena): segment j is [begin[j], end[j]) and begin has count entries.
 struct Segments {
   const u64* begin;  // count+1 offsets into the concatenated text
   u32 count;
+  const u64* end = nullptr;
 };
 
 __device__ __forceinline__ u64 segment_end(const Segments& s, u64 x) {
+  if (s.end) return s.end[s.count == 1 ? 0 : find_segment(s.begin, s.count, x)];
   if (s.count == 1) return s.begin[1];
   return s.begin[find_segment(s.begin, s.count, x) + 1];
 }
@@ -281,9 +285,12 @@ seed_rank_kernel(const u64* __restrict__ keys, u32* __restrict__ sa,
 
 // Round step 1: composite keys for the active list.  counters: *group_count
 // receives the number of groups G.  ghead/gstart are indexed by dense id.
+// inst_h, when set, holds each segment's own prefix length h (the served
+// engine advances references admitted at different times side by side).
 static __global__ void __launch_bounds__(kScanBlock)
 round_keys_kernel(const u32* __restrict__ active, u64 count,
-                  const u32* __restrict__ rank, u64 h, Segments segs,
+                  const u32* __restrict__ rank, u64 h, const u64* __restrict__ inst_h,
+                  Segments segs,
                   u32 second_bits, u64* __restrict__ ckey,
                   u32* __restrict__ cval, u32* __restrict__ ghead,
                   u32* __restrict__ gstart, u64 group_cap, u64* status_sum,
@@ -335,8 +342,16 @@ round_keys_kernel(const u32* __restrict__ active, u64 count,
         ++dense;
       }
       const u64 p = pos[i];
-      const u64 q = p + h;
-      const u64 second = q < segment_end(segs, p) ? static_cast<u64>(rank[q]) + 1 : 0;
+      u64 end, q;
+      if (inst_h) {
+        const u32 j = segs.count == 1 ? 0 : find_segment(segs.begin, segs.count, p);
+        end = segs.end ? segs.end[j] : segs.begin[j + 1];
+        q = p + inst_h[j];
+      } else {
+        end = segment_end(segs, p);
+        q = p + h;
+      }
+      const u64 second = q < end ? static_cast<u64>(rank[q]) + 1 : 0;
       ckey[a] = ((dense - 1) << second_bits) | second;
       cval[a] = static_cast<u32>(p);
     }

@@ -11,9 +11,16 @@
 
 #include <algorithm>
 #include <chrono>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <string>
+#include <thread>
+#include <unordered_map>
 #include <utility>
 #include <vector>
 
@@ -23,6 +30,7 @@
 #include "lcp.cuh"
 #include "pack.cuh"
 #include "radix.cuh"
+#include "serve.cuh"
 
 using namespace sufgpu;
 
@@ -241,6 +249,7 @@ struct Engine {
   u32* sa = nullptr;
   u32* spare = nullptr;
   u32 seed_length = 0;  // symbols every seed group shares
+  u64 rank_rows = 0;    // rows a rank may name (n, or the arena capacity)
 
   explicit Engine(sufgpu_ctx& ctx) : c(ctx) {}
 
@@ -368,8 +377,11 @@ struct Engine {
   }
   u32 last_tiles = 0;
 
-  // ---- the doubling sort: leaves SA in `sa` and ISA (global rows) in rank.
-  void suffix_sort() {
+  // ---- Seed phase: alphabet remap, seed keys, the segmented seed sort and
+  // seed ranks.  Leaves SA in `sa` (sa_out when given), head-row ranks in
+  // L.rank, seed-boundary LCPs in L.lcp and the active list in L.x; returns
+  // the active count.
+  u64 seed_phase(u32* sa_out = nullptr) {
     // Alphabet remap.
     zero(L.alpha, 256 * 4);
     launch("alphabet_histogram", n, alphabet_histogram_kernel,
@@ -442,53 +454,71 @@ struct Engine {
     launch("seed_rank", n * 16, seed_rank_kernel, scan_tiles, kScanBlock, 0,
            static_cast<const u64*>(keys), sa, n, segments(), packed_shift, bits, symbols,
            L.rank, L.lcp, L.x, status_max, status_sum, L.counters, L.scalars + 0, L.flags);
-    u64 active = read_scalar(0);
+    if (sa_out && sa_out != sa) {
+      SG_CUDA(cudaMemcpyAsync(sa_out, sa, n * 4, cudaMemcpyDeviceToDevice, c.stream));
+      spare = sa;  // the scratch buffer the sort ended in is free again
+      sa = sa_out;
+    }
+    const u64 active = read_scalar(0);
     st.active_first = active;
+    seed_length = symbols;
+    return active;
+  }
 
+
+  // ---- One doubling round over the active list act[0, active): prefix h
+  // (or per-segment lengths inst_h with the segment table `segs`).  The next
+  // active list replaces act (act/other swap roles as needed).  Returns the
+  // next active count.
+  u64 round_step(u32*& act, u32*& other, u64 active, u64 h, const u64* inst_h,
+                 Segments segs) {
+    const u32 second_bits = bits_for(n);
+    st.active_rows += active;
+    const u64 tiles = (active + kScanTile - 1) / kScanTile;
+    u32* ghead = L.y;
+    u32* gstart = L.y + (n - n / 2);  // G <= active/2 <= n/2 entries each
+    zero(L.status, (tiles + 1) * 8);
+    zero(L.counters, 4);
+    launch("round_keys", active * 28, round_keys_kernel, tiles, kScanBlock, 0, act, active,
+           L.rank, h, inst_h, segs, second_bits, L.k0, other, ghead, gstart, u64(n / 2),
+           L.status, L.counters, L.scalars + 1, L.flags);
+    // Dense ids are < active/2 (every group has two or more rows).
+    const u32 id_bits = bits_for(active / 2 > 0 ? active / 2 - 1 : 0);
+    const u32 t = static_cast<u32>((active + kSortTile - 1) / kSortTile);
+    const u64 b2[2] = {0, active};
+    const u32 t2[2] = {0, t};
+    std::memcpy(c.host_small + 4096, b2, 16);
+    std::memcpy(c.host_small + 4096 + 16, t2, 8);
+    SG_CUDA(cudaMemcpyAsync(L.sort_begin, c.host_small + 4096, 16, cudaMemcpyHostToDevice, c.stream));
+    SG_CUDA(cudaMemcpyAsync(L.sort_tiles, c.host_small + 4096 + 16, 8, cudaMemcpyHostToDevice, c.stream));
+    const bool sw = radix_sort("round_onesweep", L.k0, other, L.k1, act, L.sort_begin, L.sort_tiles,
+                               1, t, active, 0, second_bits + id_bits, false);
+    u64* ck = sw ? L.k1 : L.k0;
+    u32* cv = sw ? act : other;
+    u32* next = sw ? other : act;
+    zero(L.status, 2 * (tiles + 1) * 8);
+    zero(L.counters, 4);
+    launch("round_rank", active * 32, round_rank_kernel, tiles, kScanBlock, 0, ck, cv, active,
+           second_bits, ghead, gstart, u64(n / 2), rank_rows, sa, L.rank, next, L.status,
+           L.status + tiles + 1, L.counters, L.scalars + 2, L.flags);
+    const u64 next_count = read_scalar(2);  // synchronizes: host_small may be reused
+    other = sw ? act : other;
+    act = next;
+    return next_count;
+  }
+
+  // ---- The doubling sort: leaves SA in `sa` and ISA (global rows) in rank.
+  void suffix_sort() {
+    u64 active = seed_phase();
     // Rounds.  act and other alternate between x and the spare SA-sized
     // buffer; y holds the per-group tables.
     u32* act = L.x;
     u32* other = spare;
-    const u32 second_bits = bits_for(n);
-    u64 h = symbols;
-    seed_length = symbols;
+    u64 h = seed_length;
     u32 rounds = 0;
     while (active > 0) {
       if (++rounds > 64) throw BuildError{SUFGPU_BUILD_FAILURE, "prefix doubling did not converge"};
-      st.active_rows += active;
-      const u64 tiles = (active + kScanTile - 1) / kScanTile;
-      u32* ghead = L.y;
-      u32* gstart = L.y + (n - n / 2);  // G <= active/2 <= n/2 entries each
-      zero(L.status, (tiles + 1) * 8);
-      zero(L.counters, 4);
-      launch("round_keys", active * 28, round_keys_kernel, tiles, kScanBlock, 0, act, active,
-             L.rank, h,
-             segments(), second_bits, L.k0, other, ghead, gstart, u64(n / 2),
-             L.status, L.counters, L.scalars + 1, L.flags);
-      // Dense ids are < active/2 (every group has two or more rows).
-      const u32 id_bits = bits_for(active / 2 > 0 ? active / 2 - 1 : 0);
-      const u32 t = static_cast<u32>((active + kSortTile - 1) / kSortTile);
-      const u64 b2[2] = {0, active};
-      const u32 t2[2] = {0, t};
-      std::memcpy(c.host_small + 4096, b2, 16);
-      std::memcpy(c.host_small + 4096 + 16, t2, 8);
-      SG_CUDA(cudaMemcpyAsync(L.sort_begin, c.host_small + 4096, 16, cudaMemcpyHostToDevice, c.stream));
-      SG_CUDA(cudaMemcpyAsync(L.sort_tiles, c.host_small + 4096 + 16, 8, cudaMemcpyHostToDevice, c.stream));
-      const bool sw = radix_sort("round_onesweep", L.k0, other, L.k1, act, L.sort_begin, L.sort_tiles, 1, t,
-                                 active, 0, second_bits + id_bits, false);
-      u64* ck = sw ? L.k1 : L.k0;
-      u32* cv = sw ? act : other;
-      u32* next = sw ? other : act;
-      zero(L.status, 2 * (tiles + 1) * 8);
-      zero(L.counters, 4);
-      launch("round_rank", active * 32, round_rank_kernel, tiles, kScanBlock, 0, ck, cv, active,
-             second_bits,
-             ghead, gstart, u64(n / 2), n, sa, L.rank, next, L.status,
-             L.status + tiles + 1,
-             L.counters, L.scalars + 2, L.flags);
-      active = read_scalar(2);  // synchronizes: host_small may be reused
-      other = sw ? act : other;
-      act = next;
+      active = round_step(act, other, active, h, nullptr, segments());
       h *= 2;
     }
     st.rounds = rounds;
@@ -572,16 +602,13 @@ void copy_out(sufgpu_ctx& c, void* dst, const void* src, u64 bytes) {
 u64 plane_bytes(u32 bits, u64 rows) { return rows * (bits == 64 ? 8 : 4); }
 u64 high_bytes(u32 bits, u64 rows) { return bits == 40 ? rows : bits == 48 ? 2 * rows : 0; }
 
-// Shared build body for one or many instances (already concatenated in
-// L.text).  outs[j] receives instance j's planes.
-void run_build(Engine& e, const sufgpu_build_desc& d, sufgpu_outputs* outs,
-               sufgpu_anchors* anchors, u32 count) {
+// Everything after the sort: ISA and SA packing, validation, LCP (raw or
+// byte-coded with anchors) and the copies into each instance's planes.
+void emit_outputs(Engine& e, const sufgpu_build_desc& d, sufgpu_outputs* outs,
+                  sufgpu_anchors* anchors, u32 count) {
   sufgpu_ctx& c = e.c;
   Layout& L = e.L;
   const u64 n = e.n;
-  SG_CUDA(cudaEventRecord(c.ev[1], c.stream));
-  e.suffix_sort();
-  SG_CUDA(cudaEventRecord(c.ev[2], c.stream));
 
   // ISA: rank holds global rows.  Stage packed planes in k0/k1 when the
   // layout differs from the device one, then copy each instance's rows.
@@ -696,6 +723,16 @@ void run_build(Engine& e, const sufgpu_build_desc& d, sufgpu_outputs* outs,
   }
   SG_CUDA(cudaEventRecord(c.ev[5], c.stream));
   e.sync();
+}
+
+// Shared build body for one or many instances (already concatenated in
+// L.text).  outs[j] receives instance j's planes.
+void run_build(Engine& e, const sufgpu_build_desc& d, sufgpu_outputs* outs,
+               sufgpu_anchors* anchors, u32 count) {
+  SG_CUDA(cudaEventRecord(e.c.ev[1], e.c.stream));
+  e.suffix_sort();
+  SG_CUDA(cudaEventRecord(e.c.ev[2], e.c.stream));
+  emit_outputs(e, d, outs, anchors, count);
 }
 
 }  // namespace
@@ -856,6 +893,7 @@ sufgpu_status sufgpu_build(sufgpu_ctx* ctx, const uint8_t* text, uint64_t n,
     SG_CUDA(cudaSetDevice(ctx->device));
     Engine e(*ctx);
     e.n = n;
+    e.rank_rows = n;
     e.segs = 1;
     e.begin = {0, n};
     const Layout probe = plan_layout(nullptr, n, 1);
@@ -934,6 +972,7 @@ extern "C" sufgpu_status sufgpu_build_batch(sufgpu_ctx* ctx, sufgpu_instance* in
     SG_CUDA(cudaSetDevice(ctx->device));
     Engine e(*ctx);
     e.n = begin[count];
+    e.rank_rows = e.n;
     e.segs = count;
     e.begin = begin;
     const Layout probe = plan_layout(nullptr, e.n, count);
@@ -1010,3 +1049,499 @@ extern "C" sufgpu_status sufgpu_set_tuning(sufgpu_ctx* ctx, const char* key, int
   }
   return SUFGPU_OK;
 }
+
+// ===========================================================================
+// Served build engine: continuous batching at doubling-round granularity.
+//
+// One persistent arena (text, SA, ranks, LCP indexed by arena position) holds
+// every in-flight reference.  Each iteration of the worker
+//   1. admits queued requests into one free arena range (HBM admission: a
+//      request waits while no range can hold it) and seeds them as a group;
+//      their ranks are relocated to arena rows and their unsorted rows are
+//      appended to the shared active list;
+//   2. runs one doubling round over the shared active list, every reference
+//      with its own prefix length h (references admitted at different times
+//      advance side by side in the same launches);
+//   3. finalizes references with no unsorted rows left (LCP, packing, copies
+//      into the caller's planes) and frees their arena range.
+// ===========================================================================
+namespace {
+
+struct ServedRequest {
+  u64 ticket = 0;
+  const u8* text = nullptr;
+  u64 n = 0;
+  sufgpu_build_desc desc{};
+  sufgpu_outputs out{};
+  u64 begin = 0;  // arena position while in flight
+  u64 h = 0;
+  u32 seed_length = 0;
+  u32 rounds = 0;
+  bool done = false;
+  sufgpu_status status = SUFGPU_OK;
+  std::string error;
+  std::vector<u8> anchor_pos, anchor_val;
+  u64 anchor_count = 0;
+  u32 anchor_bits = 0;
+  std::chrono::steady_clock::time_point submitted, admitted, finished;
+};
+
+using ReqPtr = std::shared_ptr<ServedRequest>;
+
+}  // namespace
+
+struct sufgpu_server {
+  sufgpu_ctx* ctx = nullptr;
+  u64 capacity = 0;
+  u32 max_instances = 0;
+  Layout L{};
+  u32* g0 = nullptr;  // shared active list (ping-pong pair)
+  u32* g1 = nullptr;
+  u32* w = nullptr;   // rebased ranks of a finishing reference
+  u32* rebased_sa = nullptr;
+  u8* text_copy = nullptr;  // aligned copy of a finishing reference's text
+  u64* inst_begin = nullptr;
+  u64* inst_end = nullptr;
+  u64* inst_h = nullptr;
+  u8* alive = nullptr;
+  std::mutex m;
+  std::condition_variable cv_work, cv_done;
+  std::deque<ReqPtr> queue;
+  std::unordered_map<u64, ReqPtr> requests;
+  std::vector<ReqPtr> inflight;  // sorted by arena position
+  std::map<u64, u64> free_ranges;  // begin -> length
+  u64 next_ticket = 1;
+  bool stopping = false;
+  std::thread worker;
+  std::vector<double> latencies;
+  u64 completed = 0, symbols_done = 0, iterations = 0, max_inflight = 0;
+  std::chrono::steady_clock::time_point first_submit, last_done;
+  bool any_submitted = false;
+  std::string fatal;
+};
+
+namespace {
+
+constexpr u64 kArenaAlign = 64;
+
+u64 align_up(u64 v, u64 a) { return (v + a - 1) / a * a; }
+
+void release_range(sufgpu_server* S, u64 begin, u64 length) {
+  auto it = S->free_ranges.emplace(begin, length).first;
+  auto next = std::next(it);
+  if (next != S->free_ranges.end() && it->first + it->second == next->first) {
+    it->second += next->second;
+    S->free_ranges.erase(next);
+  }
+  if (it != S->free_ranges.begin()) {
+    auto prev = std::prev(it);
+    if (prev->first + prev->second == it->first) {
+      prev->second += it->second;
+      S->free_ranges.erase(it);
+    }
+  }
+}
+
+// An Engine whose layout is the server arena, optionally viewed from an
+// offset (text/rank/sa/lcp shifted; scratch shared).
+Engine arena_engine(sufgpu_server* S, u64 offset, u64 n) {
+  Engine e(*S->ctx);
+  e.L = S->L;
+  e.L.text += offset;
+  e.L.rank += offset;
+  e.L.sa += offset;
+  e.L.lcp += offset;
+  e.n = n;
+  e.rank_rows = n;
+  e.sa = e.L.sa;
+  e.spare = e.L.v0;
+  return e;
+}
+
+void seed_group(sufgpu_server* S, std::vector<ReqPtr>& group, u32*& act, u64& active) {
+  sufgpu_ctx& c = *S->ctx;
+  const u64 R = group.front()->begin;
+  std::vector<u64> begin{0};
+  for (auto& r : group) begin.push_back(begin.back() + r->n);
+  const u64 m = begin.back();
+  for (auto& r : group) {
+    SG_CUDA(cudaMemcpyAsync(S->L.text + r->begin, r->text, r->n, cudaMemcpyDefault, c.stream));
+  }
+  Engine e = arena_engine(S, R, m);
+  e.segs = static_cast<u32>(group.size());
+  e.begin = begin;
+  const u64 fresh = e.seed_phase(S->L.sa + R);
+  // Arena coordinates: SA values and ranks shift by R; the group's active
+  // rows (in L.x) join the shared list after the current ones.
+  e.launch("serve_relocate", m * 16, relocate_kernel, e.grid_stride_blocks(m, 256), 256, 0,
+           S->L.sa + R, S->L.rank + R, m, static_cast<u32>(R));
+  if (fresh) {
+    e.launch("serve_append", fresh * 8, shift_kernel, e.grid_stride_blocks(fresh, 256), 256, 0,
+             static_cast<const u32*>(S->L.x), fresh, static_cast<long long>(R), act + active);
+    active += fresh;
+  }
+  for (auto& r : group) {
+    r->h = e.seed_length;
+    r->seed_length = e.seed_length;
+  }
+}
+
+void finalize(sufgpu_server* S, const ReqPtr& r, u32* free_list) {
+  sufgpu_ctx& c = *S->ctx;
+  const u64 b = r->begin, n = r->n;
+  Engine f(c);
+  f.L = S->L;
+  f.n = n;
+  f.rank_rows = n;
+  f.segs = 1;
+  f.begin = {0, n};
+  f.seed_length = r->seed_length;
+  // Local coordinates in scratch: aligned text copy, rebased SA and ranks.
+  SG_CUDA(cudaMemcpyAsync(S->text_copy, S->L.text + b, n, cudaMemcpyDeviceToDevice, c.stream));
+  f.zero(S->text_copy + n, kTextPad);
+  f.launch("serve_rebase", n * 16, shift_kernel, f.grid_stride_blocks(n, 256), 256, 0,
+           static_cast<const u32*>(S->L.sa + b), n, -static_cast<long long>(b), S->rebased_sa);
+  f.launch("serve_rebase", n * 16, shift_kernel, f.grid_stride_blocks(n, 256), 256, 0,
+           static_cast<const u32*>(S->L.rank + b), n, -static_cast<long long>(b), S->w);
+  f.L.text = S->text_copy;
+  f.L.rank = S->w;
+  f.L.lcp = S->L.lcp + b;
+  f.sa = S->rebased_sa;
+  f.spare = free_list;
+  // The single-instance segment table of this view.
+  f.upload_segments(f.begin);
+  sufgpu_anchors anchors{};
+  emit_outputs(f, r->desc, &r->out, &anchors, 1);
+  if (anchors.count) {
+    const u64 w = anchors.coordinate_bits / 8;
+    r->anchor_pos.assign(static_cast<const u8*>(anchors.positions),
+                         static_cast<const u8*>(anchors.positions) + anchors.count * w);
+    r->anchor_val.assign(static_cast<const u8*>(anchors.values),
+                         static_cast<const u8*>(anchors.values) + anchors.count * w);
+  }
+  r->anchor_count = anchors.count;
+  r->anchor_bits = anchors.coordinate_bits
+                       ? anchors.coordinate_bits
+                       : (r->desc.lcp_encoding == SUFGPU_LCP_BYTE64 ? 64 : 32);
+}
+
+void fail_request(sufgpu_server* S, const ReqPtr& r, sufgpu_status status, const std::string& why) {
+  r->status = status;
+  r->error = why;
+  r->done = true;
+  r->finished = std::chrono::steady_clock::now();
+  S->cv_done.notify_all();
+}
+
+void server_loop(sufgpu_server* S) {
+  cudaSetDevice(S->ctx->device);
+  u32* act = S->g0;
+  u32* other = S->g1;
+  u64 active = 0;
+  while (true) {
+    std::vector<ReqPtr> group;
+    {
+      std::unique_lock<std::mutex> lock(S->m);
+      S->cv_work.wait(lock, [&] {
+        return S->stopping || !S->queue.empty() || !S->inflight.empty();
+      });
+      if (S->queue.empty() && S->inflight.empty()) {
+        if (S->stopping) break;
+        continue;
+      }
+      // Admission: as many queued requests (in order) as one free range and
+      // the instance slots can hold.
+      u64 best_begin = 0, best_len = 0;
+      for (auto& fr : S->free_ranges) {
+        const u64 start = align_up(fr.first, kArenaAlign);
+        const u64 len = fr.first + fr.second > start ? fr.first + fr.second - start : 0;
+        if (len > best_len) {
+          best_len = len;
+          best_begin = start;
+        }
+      }
+      u64 total = 0;
+      while (!S->queue.empty() && S->inflight.size() + group.size() < S->max_instances) {
+        ReqPtr r = S->queue.front();
+        if (r->n + kArenaAlign > S->capacity) {
+          S->queue.pop_front();
+          fail_request(S, r, SUFGPU_INVALID_INPUT, "reference exceeds the server arena");
+          continue;
+        }
+        if (total + r->n > best_len) break;
+        r->begin = best_begin + total;
+        r->admitted = std::chrono::steady_clock::now();
+        total += r->n;
+        group.push_back(r);
+        S->queue.pop_front();
+      }
+      if (total) {
+        // Carve [best_begin, best_begin + total) out of its free range.
+        auto it = std::prev(S->free_ranges.upper_bound(best_begin));
+        const u64 fb = it->first, fl = it->second;
+        S->free_ranges.erase(it);
+        if (best_begin > fb) S->free_ranges.emplace(fb, best_begin - fb);
+        const u64 tail = best_begin + total;
+        if (fb + fl > tail) S->free_ranges.emplace(tail, fb + fl - tail);
+      }
+    }
+    std::vector<ReqPtr> finished;
+    try {
+      SG_CUDA(cudaMemsetAsync(S->L.flags, 0, sizeof(DeviceFlags), S->ctx->stream));
+      if (!group.empty()) {
+        seed_group(S, group, act, active);
+        std::lock_guard<std::mutex> lock(S->m);
+        for (auto& r : group) S->inflight.push_back(r);
+        std::sort(S->inflight.begin(), S->inflight.end(),
+                  [](const ReqPtr& a, const ReqPtr& b) { return a->begin < b->begin; });
+        S->max_inflight = std::max<u64>(S->max_inflight, S->inflight.size());
+      }
+      std::vector<ReqPtr> live;
+      {
+        std::lock_guard<std::mutex> lock(S->m);
+        live = S->inflight;
+      }
+      const u32 K = static_cast<u32>(live.size());
+      Engine e = arena_engine(S, 0, S->capacity);
+      std::vector<u64> hb(K), he(K), hh(K);
+      for (u32 j = 0; j < K; ++j) {
+        hb[j] = live[j]->begin;
+        he[j] = live[j]->begin + live[j]->n;
+        hh[j] = live[j]->h;
+      }
+      std::vector<u8> alive(K, 0);
+      if (K > 0) {
+        SG_CUDA(cudaMemcpyAsync(S->inst_begin, hb.data(), K * 8, cudaMemcpyHostToDevice, S->ctx->stream));
+        SG_CUDA(cudaMemcpyAsync(S->inst_end, he.data(), K * 8, cudaMemcpyHostToDevice, S->ctx->stream));
+        SG_CUDA(cudaMemcpyAsync(S->inst_h, hh.data(), K * 8, cudaMemcpyHostToDevice, S->ctx->stream));
+        const Segments segs{S->inst_begin, K, S->inst_end};
+        if (active > 0) {
+          active = e.round_step(act, other, active, 0, S->inst_h, segs);
+          ++S->iterations;
+          for (auto& r : live) {
+            r->h *= 2;
+            ++r->rounds;
+          }
+        }
+        e.zero(S->alive, K);
+        if (active > 0) {
+          e.launch("serve_alive", active * 4, alive_kernel, e.grid_stride_blocks(active, 256), 256, 0,
+                   static_cast<const u32*>(act), active, segs, S->alive);
+        }
+        SG_CUDA(cudaMemcpyAsync(alive.data(), S->alive, K, cudaMemcpyDeviceToHost, S->ctx->stream));
+        e.sync();
+        for (u32 j = 0; j < K; ++j) {
+          if (!alive[j]) finished.push_back(live[j]);
+        }
+      }
+      for (auto& r : finished) finalize(S, r, other);
+      DeviceFlags flags{};
+      SG_CUDA(cudaMemcpy(&flags, S->L.flags, sizeof(flags), cudaMemcpyDeviceToHost));
+      if (flags.error) throw BuildError{SUFGPU_BUILD_FAILURE, "device check failed in the served engine"};
+    } catch (const CudaError& err) {
+      cudaGetLastError();
+      S->fatal = std::string("CUDA error in ") + err.what + ": " + cudaGetErrorString(err.code);
+    } catch (const BuildError& err) {
+      S->fatal = err.message;
+    } catch (const std::exception& err) {
+      S->fatal = err.what();
+    }
+    std::lock_guard<std::mutex> lock(S->m);
+    const auto now = std::chrono::steady_clock::now();
+    if (!S->fatal.empty()) {
+      // Every in-flight reference fails with the error; the arena resets.
+      for (auto& r : S->inflight) fail_request(S, r, SUFGPU_BUILD_FAILURE, S->fatal);
+      for (auto& r : group) {
+        if (!r->done) fail_request(S, r, SUFGPU_BUILD_FAILURE, S->fatal);
+      }
+      S->inflight.clear();
+      S->free_ranges.clear();
+      S->free_ranges.emplace(0, S->capacity);
+      active = 0;
+      S->fatal.clear();
+      continue;
+    }
+    for (auto& r : finished) {
+      r->done = true;
+      r->finished = now;
+      S->latencies.push_back(std::chrono::duration<double>(now - r->submitted).count());
+      ++S->completed;
+      S->symbols_done += r->n;
+      S->last_done = now;
+      release_range(S, r->begin, r->n);
+      S->inflight.erase(std::find(S->inflight.begin(), S->inflight.end(), r));
+    }
+    if (!finished.empty()) S->cv_done.notify_all();
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+sufgpu_status sufgpu_server_create(sufgpu_server** out, int device,
+                                   const sufgpu_server_config* config) {
+  if (!out) return SUFGPU_INVALID_INPUT;
+  *out = nullptr;
+  auto* S = new sufgpu_server();
+  S->capacity = config && config->capacity_symbols ? config->capacity_symbols : (u64(1) << 29);
+  S->max_instances = config && config->max_instances ? config->max_instances : 1024;
+  if (S->capacity > sufgpu_max_symbols() || S->max_instances > kMaxSegmentsPerLaunch) {
+    delete S;
+    return SUFGPU_INVALID_INPUT;
+  }
+  sufgpu_status st = sufgpu_create(&S->ctx, device);
+  if (st != SUFGPU_OK) {
+    delete S;
+    return st;
+  }
+  try {
+    const u64 C = S->capacity;
+    const Layout probe = plan_layout(nullptr, C, S->max_instances);
+    const u64 extra = 4 * round_up(C * 4, 256) + round_up(C + kTextPad, 256) +
+                      3 * round_up(u64(S->max_instances) * 8, 256) + round_up(S->max_instances, 256);
+    S->ctx->arena.reserve(probe.total + extra);
+    u8* base = static_cast<u8*>(S->ctx->arena.base);
+    S->L = plan_layout(base, C, S->max_instances);
+    u8* p = base + probe.total;
+    auto take = [&](u64 bytes) {
+      u8* q = p;
+      p += round_up(bytes, 256);
+      return q;
+    };
+    S->g0 = reinterpret_cast<u32*>(take(C * 4));
+    S->g1 = reinterpret_cast<u32*>(take(C * 4));
+    S->w = reinterpret_cast<u32*>(take(C * 4));
+    S->rebased_sa = reinterpret_cast<u32*>(take(C * 4));
+    S->text_copy = take(C + kTextPad);
+    S->inst_begin = reinterpret_cast<u64*>(take(u64(S->max_instances) * 8));
+    S->inst_end = reinterpret_cast<u64*>(take(u64(S->max_instances) * 8));
+    S->inst_h = reinterpret_cast<u64*>(take(u64(S->max_instances) * 8));
+    S->alive = take(S->max_instances);
+    SG_CUDA(cudaMemsetAsync(S->L.text + C, 0, kTextPad, S->ctx->stream));
+    SG_CUDA(cudaStreamSynchronize(S->ctx->stream));
+  } catch (const BuildError& err) {
+    S->ctx->last_error = err.message;
+    sufgpu_destroy(S->ctx);
+    delete S;
+    return SUFGPU_BUILD_FAILURE;
+  } catch (const CudaError&) {
+    cudaGetLastError();
+    sufgpu_destroy(S->ctx);
+    delete S;
+    return SUFGPU_BUILD_FAILURE;
+  }
+  S->free_ranges.emplace(0, S->capacity);
+  S->worker = std::thread(server_loop, S);
+  *out = S;
+  return SUFGPU_OK;
+}
+
+void sufgpu_server_destroy(sufgpu_server* S) {
+  if (!S) return;
+  {
+    std::lock_guard<std::mutex> lock(S->m);
+    S->stopping = true;
+  }
+  S->cv_work.notify_all();
+  if (S->worker.joinable()) S->worker.join();
+  sufgpu_destroy(S->ctx);
+  delete S;
+}
+
+sufgpu_status sufgpu_server_submit(sufgpu_server* S, const uint8_t* text, uint64_t n,
+                                   const sufgpu_build_desc* desc, const sufgpu_outputs* out,
+                                   uint64_t* ticket) {
+  if (!S || !desc || !out || !ticket || (n && !text)) return SUFGPU_INVALID_INPUT;
+  if (auto s = check_desc(S->ctx, desc)) return s;
+  if (n == 0 || n > sufgpu_max_symbols()) return SUFGPU_INVALID_INPUT;
+  auto r = std::make_shared<ServedRequest>();
+  r->text = text;
+  r->n = n;
+  r->desc = *desc;
+  r->out = *out;
+  r->submitted = std::chrono::steady_clock::now();
+  {
+    std::lock_guard<std::mutex> lock(S->m);
+    r->ticket = S->next_ticket++;
+    S->requests.emplace(r->ticket, r);
+    S->queue.push_back(r);
+    if (!S->any_submitted) {
+      S->any_submitted = true;
+      S->first_submit = r->submitted;
+    }
+  }
+  S->cv_work.notify_all();
+  *ticket = r->ticket;
+  return SUFGPU_OK;
+}
+
+static sufgpu_status request_info(const ReqPtr& r, sufgpu_request_info* info) {
+  if (info) {
+    info->queue_seconds = std::chrono::duration<double>(r->admitted - r->submitted).count();
+    info->latency_seconds = std::chrono::duration<double>(r->finished - r->submitted).count();
+    info->rounds = r->rounds;
+    info->seed_symbols = r->seed_length;
+    info->anchors = sufgpu_anchors{r->anchor_pos.empty() ? nullptr : r->anchor_pos.data(),
+                                   r->anchor_val.empty() ? nullptr : r->anchor_val.data(),
+                                   r->anchor_count, r->anchor_bits};
+  }
+  return r->status;
+}
+
+sufgpu_status sufgpu_server_wait(sufgpu_server* S, uint64_t ticket, sufgpu_request_info* info) {
+  if (!S) return SUFGPU_INVALID_INPUT;
+  std::unique_lock<std::mutex> lock(S->m);
+  auto it = S->requests.find(ticket);
+  if (it == S->requests.end()) return SUFGPU_INVALID_INPUT;
+  ReqPtr r = it->second;
+  S->cv_done.wait(lock, [&] { return r->done; });
+  return request_info(r, info);
+}
+
+sufgpu_status sufgpu_server_poll(sufgpu_server* S, uint64_t ticket, int* done) {
+  if (!S || !done) return SUFGPU_INVALID_INPUT;
+  std::lock_guard<std::mutex> lock(S->m);
+  auto it = S->requests.find(ticket);
+  if (it == S->requests.end()) return SUFGPU_INVALID_INPUT;
+  *done = it->second->done ? 1 : 0;
+  return SUFGPU_OK;
+}
+
+sufgpu_status sufgpu_server_release(sufgpu_server* S, uint64_t ticket) {
+  if (!S) return SUFGPU_INVALID_INPUT;
+  std::lock_guard<std::mutex> lock(S->m);
+  auto it = S->requests.find(ticket);
+  if (it == S->requests.end() || !it->second->done) return SUFGPU_INVALID_INPUT;
+  S->requests.erase(it);
+  return SUFGPU_OK;
+}
+
+sufgpu_status sufgpu_server_get_stats(sufgpu_server* S, sufgpu_server_stats* out) {
+  if (!S || !out) return SUFGPU_INVALID_INPUT;
+  std::lock_guard<std::mutex> lock(S->m);
+  std::vector<double> lat = S->latencies;
+  std::sort(lat.begin(), lat.end());
+  auto pct = [&](double q) {
+    if (lat.empty()) return 0.0;
+    const size_t i = std::min(lat.size() - 1, static_cast<size_t>(q * (lat.size() - 1) + 0.5));
+    return lat[i];
+  };
+  *out = sufgpu_server_stats{};
+  out->completed = S->completed;
+  out->symbols = S->symbols_done;
+  out->iterations = S->iterations;
+  out->max_inflight = S->max_inflight;
+  out->p50_seconds = pct(0.50);
+  out->p99_seconds = pct(0.99);
+  const double span = S->completed
+                          ? std::chrono::duration<double>(S->last_done - S->first_submit).count()
+                          : 0.0;
+  out->span_seconds = span;
+  out->symbols_per_second = span > 0 ? S->symbols_done / span : 0.0;
+  out->queued = S->queue.size();
+  out->inflight = S->inflight.size();
+  return SUFGPU_OK;
+}
+
+}  // extern "C"
