@@ -448,10 +448,14 @@ class Server:
         self._pending: dict[int, tuple] = {}
 
     def submit(self, text, sa_bits: int = 32, isa_bits: int = 0,
-               lcp: LcpEncoding = LcpEncoding.RAW32, validate: bool = False) -> int:
+               lcp: LcpEncoding = LcpEncoding.RAW32, validate: bool = False,
+               planes: Optional[dict] = None) -> int:
+        """Queues one build.  ``planes`` may supply the output arrays (for
+        example pinned ones from pinned_array); otherwise they are allocated."""
         t = np.ascontiguousarray(_as_text(text))
         lcp = LcpEncoding(lcp)
-        planes = Context._alloc_outputs(None, int(t.size), sa_bits, isa_bits, lcp)
+        if planes is None:
+            planes = Context._alloc_outputs(None, int(t.size), sa_bits, isa_bits, lcp)
         desc = _Desc(sa_bits, isa_bits, int(lcp), FLAG_VALIDATE if validate else 0)
         out = Context._outputs(planes)
         ticket = ctypes.c_uint64()

@@ -1099,7 +1099,8 @@ struct sufgpu_server {
   u32* g1 = nullptr;
   u32* w = nullptr;   // rebased ranks of a finishing reference
   u32* rebased_sa = nullptr;
-  u8* text_copy = nullptr;  // aligned copy of a finishing reference's text
+  u8* text_copy = nullptr;  // compacted text of finishing references
+  u32* lcp_copy = nullptr;  // their LCP rows
   u64* inst_begin = nullptr;
   u64* inst_end = nullptr;
   u64* inst_h = nullptr;
@@ -1186,43 +1187,73 @@ void seed_group(sufgpu_server* S, std::vector<ReqPtr>& group, u32*& act, u64& ac
   }
 }
 
-void finalize(sufgpu_server* S, const ReqPtr& r, u32* free_list) {
+// Output phase for every reference that finished in this iteration: those
+// with the same descriptor are compacted into one contiguous batch and go
+// through the batched output path together.
+void finalize_batch(sufgpu_server* S, std::vector<ReqPtr>& done_now, u32* free_list) {
   sufgpu_ctx& c = *S->ctx;
-  const u64 b = r->begin, n = r->n;
-  Engine f(c);
-  f.L = S->L;
-  f.n = n;
-  f.rank_rows = n;
-  f.segs = 1;
-  f.begin = {0, n};
-  f.seed_length = r->seed_length;
-  // Local coordinates in scratch: aligned text copy, rebased SA and ranks.
-  SG_CUDA(cudaMemcpyAsync(S->text_copy, S->L.text + b, n, cudaMemcpyDeviceToDevice, c.stream));
-  f.zero(S->text_copy + n, kTextPad);
-  f.launch("serve_rebase", n * 16, shift_kernel, f.grid_stride_blocks(n, 256), 256, 0,
-           static_cast<const u32*>(S->L.sa + b), n, -static_cast<long long>(b), S->rebased_sa);
-  f.launch("serve_rebase", n * 16, shift_kernel, f.grid_stride_blocks(n, 256), 256, 0,
-           static_cast<const u32*>(S->L.rank + b), n, -static_cast<long long>(b), S->w);
-  f.L.text = S->text_copy;
-  f.L.rank = S->w;
-  f.L.lcp = S->L.lcp + b;
-  f.sa = S->rebased_sa;
-  f.spare = free_list;
-  // The single-instance segment table of this view.
-  f.upload_segments(f.begin);
-  sufgpu_anchors anchors{};
-  emit_outputs(f, r->desc, &r->out, &anchors, 1);
-  if (anchors.count) {
-    const u64 w = anchors.coordinate_bits / 8;
-    r->anchor_pos.assign(static_cast<const u8*>(anchors.positions),
-                         static_cast<const u8*>(anchors.positions) + anchors.count * w);
-    r->anchor_val.assign(static_cast<const u8*>(anchors.values),
-                         static_cast<const u8*>(anchors.values) + anchors.count * w);
+  std::vector<bool> taken(done_now.size(), false);
+  for (size_t i = 0; i < done_now.size(); ++i) {
+    if (taken[i]) continue;
+    const sufgpu_build_desc d = done_now[i]->desc;
+    std::vector<ReqPtr> group;
+    for (size_t k = i; k < done_now.size(); ++k) {
+      const sufgpu_build_desc& o = done_now[k]->desc;
+      if (!taken[k] && o.sa_storage_bits == d.sa_storage_bits &&
+          o.isa_storage_bits == d.isa_storage_bits && o.lcp_encoding == d.lcp_encoding &&
+          o.flags == d.flags) {
+        taken[k] = true;
+        group.push_back(done_now[k]);
+      }
+    }
+    const u32 count = static_cast<u32>(group.size());
+    std::vector<u64> dst{0}, src;
+    u32 seed_min = ~0u;
+    for (auto& r : group) {
+      src.push_back(r->begin);
+      dst.push_back(dst.back() + r->n);
+      seed_min = std::min(seed_min, r->seed_length);
+    }
+    const u64 m = dst.back();
+    Engine f(c);
+    f.L = S->L;
+    f.n = m;
+    f.rank_rows = m;
+    f.segs = count;
+    f.begin = dst;
+    f.seed_length = seed_min;  // every reference shares at least this prefix
+    f.upload_segments(dst);    // batch offsets -> L.seg_begin
+    SG_CUDA(cudaMemcpyAsync(S->inst_begin, src.data(), count * 8, cudaMemcpyHostToDevice, c.stream));
+    f.launch("serve_gather", m * 29, gather_finished_kernel, f.grid_stride_blocks(m, 256), 256, 0,
+             static_cast<const u8*>(S->L.text), static_cast<const u32*>(S->L.sa),
+             static_cast<const u32*>(S->L.rank), static_cast<const u32*>(S->L.lcp),
+             static_cast<const u64*>(S->L.seg_begin), static_cast<const u64*>(S->inst_begin),
+             count, m, S->text_copy, S->rebased_sa, S->w, S->lcp_copy);
+    f.zero(S->text_copy + m, kTextPad);
+    f.L.text = S->text_copy;
+    f.L.rank = S->w;
+    f.L.lcp = S->lcp_copy;
+    f.sa = S->rebased_sa;
+    f.spare = free_list;
+    std::vector<sufgpu_outputs> outs(count);
+    std::vector<sufgpu_anchors> anchors(count);
+    for (u32 j = 0; j < count; ++j) outs[j] = group[j]->out;
+    emit_outputs(f, d, outs.data(), anchors.data(), count);
+    for (u32 j = 0; j < count; ++j) {
+      auto& r = group[j];
+      const auto& a = anchors[j];
+      const u64 w = a.coordinate_bits / 8;
+      if (a.count) {
+        r->anchor_pos.assign(static_cast<const u8*>(a.positions),
+                             static_cast<const u8*>(a.positions) + a.count * w);
+        r->anchor_val.assign(static_cast<const u8*>(a.values),
+                             static_cast<const u8*>(a.values) + a.count * w);
+      }
+      r->anchor_count = a.count;
+      r->anchor_bits = a.coordinate_bits ? a.coordinate_bits
+                                         : (d.lcp_encoding == SUFGPU_LCP_BYTE64 ? 64 : 32);
+    }
   }
-  r->anchor_count = anchors.count;
-  r->anchor_bits = anchors.coordinate_bits
-                       ? anchors.coordinate_bits
-                       : (r->desc.lcp_encoding == SUFGPU_LCP_BYTE64 ? 64 : 32);
 }
 
 void fail_request(sufgpu_server* S, const ReqPtr& r, sufgpu_status status, const std::string& why) {
@@ -1334,7 +1365,7 @@ void server_loop(sufgpu_server* S) {
           if (!alive[j]) finished.push_back(live[j]);
         }
       }
-      for (auto& r : finished) finalize(S, r, other);
+      if (!finished.empty()) finalize_batch(S, finished, other);
       DeviceFlags flags{};
       SG_CUDA(cudaMemcpy(&flags, S->L.flags, sizeof(flags), cudaMemcpyDeviceToHost));
       if (flags.error) throw BuildError{SUFGPU_BUILD_FAILURE, "device check failed in the served engine"};
@@ -1398,7 +1429,7 @@ sufgpu_status sufgpu_server_create(sufgpu_server** out, int device,
   try {
     const u64 C = S->capacity;
     const Layout probe = plan_layout(nullptr, C, S->max_instances);
-    const u64 extra = 4 * round_up(C * 4, 256) + round_up(C + kTextPad, 256) +
+    const u64 extra = 5 * round_up(C * 4, 256) + round_up(C + kTextPad, 256) +
                       3 * round_up(u64(S->max_instances) * 8, 256) + round_up(S->max_instances, 256);
     S->ctx->arena.reserve(probe.total + extra);
     u8* base = static_cast<u8*>(S->ctx->arena.base);
@@ -1413,6 +1444,7 @@ sufgpu_status sufgpu_server_create(sufgpu_server** out, int device,
     S->g1 = reinterpret_cast<u32*>(take(C * 4));
     S->w = reinterpret_cast<u32*>(take(C * 4));
     S->rebased_sa = reinterpret_cast<u32*>(take(C * 4));
+    S->lcp_copy = reinterpret_cast<u32*>(take(C * 4));
     S->text_copy = take(C + kTextPad);
     S->inst_begin = reinterpret_cast<u64*>(take(u64(S->max_instances) * 8));
     S->inst_end = reinterpret_cast<u64*>(take(u64(S->max_instances) * 8));
