@@ -185,12 +185,14 @@ def build_bytes(text: np.ndarray, sa: np.ndarray, isa: np.ndarray, lcp: np.ndarr
 
 
 def load_traffic(kernel: str):
-    """ncu DRAM bytes per algorithmic byte for `kernel` from profiles/, if any."""
+    """DRAM bytes per algorithmic byte of `kernel`, from the committed ncu
+    summary (profiles/traffic.json, measured on a 30 Mbp capture and scaled
+    to a full launch by its algorithmic bytes), or None."""
     path = ROOT / "profiles" / "traffic.json"
     if not path.exists():
         return None
-    data = json.loads(path.read_text())
-    return data.get(kernel)
+    entry = json.loads(path.read_text()).get(kernel)
+    return entry["dram_per_algorithmic_byte"] if entry else None
 
 
 # ---------------------------------------------------------------------------

@@ -349,7 +349,7 @@ struct Engine {
       zero(L.counters, 4);
       const OnesweepVariant v = onesweep_variant(c.ballot_rank && elems >= c.ballot_min_elems,
                                                  c.sort_block, vals != nullptr);
-      launch(name, elems * 24, v.fn, total_tiles, v.block, v.smem,
+      launch(name, elems * (vals ? 24 : 16), v.fn, total_tiles, v.block, v.smem,
              kin, vin, kout, vout, ss, begin_bit + p * kRadixBits, p, passes,
              L.digit_start, L.status, L.counters, L.flags);
       std::swap(kin, kout);
@@ -451,7 +451,7 @@ struct Engine {
     zero(L.counters, 4);
     u64* status_max = L.status;
     u64* status_sum = L.status + scan_tiles + 1;
-    launch("seed_rank", n * 16, seed_rank_kernel, scan_tiles, kScanBlock, 0,
+    launch("seed_rank", n * 20, seed_rank_kernel, scan_tiles, kScanBlock, 0,
            static_cast<const u64*>(keys), sa, n, segments(), packed_shift, bits, symbols,
            L.rank, L.lcp, L.x, status_max, status_sum, L.counters, L.scalars + 0, L.flags);
     if (sa_out && sa_out != sa) {
