@@ -181,7 +181,9 @@ SUFGPU_API sufgpu_status sufgpu_profile_entry(const sufgpu_ctx *ctx, uint32_t in
  *   "seed_symbols"  symbols packed per seed key, 0 = as many as fit 64 bits;
  *   "ballot_rank"   1 = onesweep ranks digits with ballots, 0 = match-any;
  *   "ballot_min_elems" smallest sort that uses ballot ranking;
- *   "sort_block"    onesweep threads per 4096-key tile: 256 or 512;
+ *   "sort_tile"     keys per onesweep tile: 2048 or 4096;
+ *   "sort_block"    onesweep threads per 4096-key tile: 256 or 512 (2048-key
+ *                   tiles always use 256);
  *   "packed_max_bits" instances of at most 2^v symbols use the packed
  *                   keys-only seed (index in the low key bits); 0 = never.
  * Results are identical for every setting; only speed changes. */

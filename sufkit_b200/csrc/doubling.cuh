@@ -195,10 +195,12 @@ seed_keys_kernel(const u8* __restrict__ text, u64 n, Segments segs,
 // resolved from the text later (their LCP is at least the seed length).
 constexpr u32 kLcpUnknown = 0xffffffffu;
 
+// Ranks leave as (position << 32 | head row) words in row order (pairs), so
+// the write is coalesced; the window scatter below turns them into rank[].
 static __global__ void __launch_bounds__(kScanBlock)
 seed_rank_kernel(const u64* __restrict__ keys, u32* __restrict__ sa,
                  u64 n, Segments segs, u32 packed_shift, u32 bits, u32 symbols,
-                 u32* __restrict__ rank, u32* __restrict__ lcp,
+                 u64* __restrict__ pairs, u32* __restrict__ lcp,
                  u32* __restrict__ active, u64* status_max, u64* status_sum,
                  u32* tile_counter, u64* active_count, DeviceFlags* flags) {
   __shared__ u64 warp_smem[kScanBlock / 32];
@@ -275,12 +277,38 @@ seed_rank_kernel(const u64* __restrict__ keys, u32* __restrict__ sa,
         flag_error(flags, kErrBounds);
         continue;
       }
-      rank[p] = static_cast<u32>(running_max);
+      pairs[r] = (static_cast<u64>(p) << 32) | static_cast<u32>(running_max);
       if (!(head[i] && head[i + 1])) active[out++] = p;
     }
   }
   const u64 tiles = (n + kScanTile - 1) / kScanTile;
   if (tile == tiles - 1 && threadIdx.x == 0) *active_count = tile_prefix[1] + agg_sum;
+}
+
+// rank[pos] = head for (pos << 32 | head) pairs grouped by 2048-position
+// windows (pairs [w*2048, (w+1)*2048) hold exactly window w's positions: SA
+// is a permutation).  Each block stages one window in shared memory and writes
+// it out coalesced.
+constexpr u32 kWindowBits = 11;
+constexpr u32 kWindow = 1u << kWindowBits;
+
+static __global__ void __launch_bounds__(256)
+window_scatter_kernel(const u64* __restrict__ pairs, u64 n, u32* __restrict__ rank,
+                      DeviceFlags* flags) {
+  __shared__ u32 window[kWindow];
+  const u64 first = static_cast<u64>(blockIdx.x) * kWindow;
+  const u32 count = static_cast<u32>(n - first < kWindow ? n - first : kWindow);
+  for (u32 i = threadIdx.x; i < count; i += 256) {
+    const u64 v = pairs[first + i];
+    const u64 pos = v >> 32;
+    if ((pos >> kWindowBits) != blockIdx.x || (pos & (kWindow - 1)) >= count) {
+      flag_error(flags, kErrBounds);  // not a permutation
+      continue;
+    }
+    window[pos & (kWindow - 1)] = static_cast<u32>(v);
+  }
+  __syncthreads();
+  for (u32 i = threadIdx.x; i < count; i += 256) rank[first + i] = window[i];
 }
 
 // Round step 1: composite keys for the active list.  counters: *group_count

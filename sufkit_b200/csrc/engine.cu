@@ -127,7 +127,7 @@ Layout plan_layout(u8* base, u64 n, u32 segments) {
   l.x = reinterpret_cast<u32*>(take(n4));
   l.y = reinterpret_cast<u32*>(take(n4));
   l.lcp = reinterpret_cast<u32*>(take(n4));
-  const u64 radix_tiles = (n + kSortTile - 1) / kSortTile + segments;
+  const u64 radix_tiles = (n + 2047) / 2048 + segments;  // smallest tile size
   const u64 scan_tiles = (n + kScanTile - 1) / kScanTile + 1;
   l.status_words = std::max<u64>(radix_tiles * kRadixDigits, 2 * scan_tiles);
   l.status = reinterpret_cast<u64*>(take(l.status_words * 8));
@@ -157,20 +157,23 @@ struct OnesweepVariant {
   u64 smem;
 };
 
-template <bool kVals>
-OnesweepVariant onesweep_variant_t(bool ballot, u32 block) {
-  if (block == 512) {
-    return {ballot ? radix_onesweep_kernel<true, 512, 8, kVals>
-                   : radix_onesweep_kernel<false, 512, 8, kVals>,
-            512, sizeof(OnesweepSmem<512>)};
-  }
-  return {ballot ? radix_onesweep_kernel<true, 256, 16, kVals>
-                 : radix_onesweep_kernel<false, 256, 16, kVals>,
-          256, sizeof(OnesweepSmem<256>)};
+template <bool kBallot, int kBlock, int kItems, bool kVals>
+OnesweepVariant variant_of() {
+  return {radix_onesweep_kernel<kBallot, kBlock, kItems, kVals>, kBlock,
+          sizeof(OnesweepSmem<kBlock, kBlock * kItems>)};
 }
 
-OnesweepVariant onesweep_variant(bool ballot, u32 block, bool vals) {
-  return vals ? onesweep_variant_t<true>(ballot, block) : onesweep_variant_t<false>(ballot, block);
+template <bool kBallot, bool kVals>
+OnesweepVariant variant_for(u32 block, u32 tile) {
+  if (tile == 2048) return variant_of<kBallot, 256, 8, kVals>();
+  return block == 512 ? variant_of<kBallot, 512, 8, kVals>() : variant_of<kBallot, 256, 16, kVals>();
+}
+
+// Onesweep variants: ranking by ballots or match-any; 4096-key tiles (256x16,
+// 512x8) or 2048-key tiles (256x8); key-value pairs or keys only.
+OnesweepVariant onesweep_variant(bool ballot, u32 block, u32 tile, bool vals) {
+  if (ballot) return vals ? variant_for<true, true>(block, tile) : variant_for<true, false>(block, tile);
+  return vals ? variant_for<false, true>(block, tile) : variant_for<false, false>(block, tile);
 }
 
 }  // namespace
@@ -233,6 +236,8 @@ struct sufgpu_ctx {
   u32 packed_max_bits = 24;
   // Onesweep block size (256 threads x 16 keys or 512 x 8).
   u32 sort_block = 256;
+  // Keys per onesweep tile (2048 or 4096).
+  u32 sort_tile = 4096;
 };
 
 namespace {
@@ -312,7 +317,7 @@ struct Engine {
                   bool check_needed, bool hist_ready = false) {
     if (end_bit <= begin_bit || total_tiles == 0) return false;
     const u32 passes = (end_bit - begin_bit + kRadixBits - 1) / kRadixBits;
-    SortSegments ss{seg_begin, seg_tiles, seg_count, total_tiles};
+    SortSegments ss{seg_begin, seg_tiles, seg_count, total_tiles, c.sort_tile};
     const u64 elems = sort_elems;
     u32 needed[kMaxPasses];
     for (u32 p = 0; p < passes; ++p) needed[p] = 1;
@@ -348,7 +353,7 @@ struct Engine {
       zero(L.status, u64(total_tiles) * kRadixDigits * 8);
       zero(L.counters, 4);
       const OnesweepVariant v = onesweep_variant(c.ballot_rank && elems >= c.ballot_min_elems,
-                                                 c.sort_block, vals != nullptr);
+                                                 c.sort_block, c.sort_tile, vals != nullptr);
       launch(name, elems * (vals ? 24 : 16), v.fn, total_tiles, v.block, v.smem,
              kin, vin, kout, vout, ss, begin_bit + p * kRadixBits, p, passes,
              L.digit_start, L.status, L.counters, L.flags);
@@ -363,7 +368,7 @@ struct Engine {
     std::vector<u32> tiles(b.size());
     tiles[0] = 0;
     for (size_t j = 0; j + 1 < b.size(); ++j) {
-      tiles[j + 1] = tiles[j] + static_cast<u32>((b[j + 1] - b[j] + kSortTile - 1) / kSortTile);
+      tiles[j + 1] = tiles[j] + static_cast<u32>((b[j + 1] - b[j] + c.sort_tile - 1) / c.sort_tile);
     }
     std::vector<u8> blob(b.size() * 12);
     std::memcpy(blob.data(), b.data(), b.size() * 8);
@@ -451,9 +456,30 @@ struct Engine {
     zero(L.counters, 4);
     u64* status_max = L.status;
     u64* status_sum = L.status + scan_tiles + 1;
-    launch("seed_rank", n * 20, seed_rank_kernel, scan_tiles, kScanBlock, 0,
+    u64* pairs = keys == L.k0 ? L.k1 : L.k0;
+    launch("seed_rank", n * 24, seed_rank_kernel, scan_tiles, kScanBlock, 0,
            static_cast<const u64*>(keys), sa, n, segments(), packed_shift, bits, symbols,
-           L.rank, L.lcp, L.x, status_max, status_sum, L.counters, L.scalars + 0, L.flags);
+           pairs, L.lcp, L.x, status_max, status_sum, L.counters, L.scalars + 0, L.flags);
+    // rank[SA[r]] = head: group the pairs by 2048-position window (keys-only
+    // passes over the position's high bits), then one coalesced window write.
+    const u32 pos_bits = std::max<u32>(1, bits_for(n - 1));
+    u64* grouped = pairs;
+    if (pos_bits > kWindowBits) {
+      const u64 b2[2] = {0, n};
+      const u32 t = static_cast<u32>((n + c.sort_tile - 1) / c.sort_tile);
+      const u32 t2[2] = {0, t};
+      sync();
+      std::memcpy(c.host_small + 4096, b2, 16);
+      std::memcpy(c.host_small + 4096 + 16, t2, 8);
+      SG_CUDA(cudaMemcpyAsync(L.sort_begin, c.host_small + 4096, 16, cudaMemcpyHostToDevice, c.stream));
+      SG_CUDA(cudaMemcpyAsync(L.sort_tiles, c.host_small + 4096 + 16, 8, cudaMemcpyHostToDevice, c.stream));
+      u64* other_keys = pairs == L.k0 ? L.k1 : L.k0;
+      const bool sw = radix_sort("rank_group", pairs, nullptr, other_keys, nullptr, L.sort_begin,
+                                 L.sort_tiles, 1, t, n, 32 + kWindowBits, 32 + pos_bits, false);
+      grouped = sw ? other_keys : pairs;
+    }
+    launch("window_scatter", n * 12, window_scatter_kernel, (n + kWindow - 1) / kWindow, 256, 0,
+           static_cast<const u64*>(grouped), n, L.rank, L.flags);
     if (sa_out && sa_out != sa) {
       SG_CUDA(cudaMemcpyAsync(sa_out, sa, n * 4, cudaMemcpyDeviceToDevice, c.stream));
       spare = sa;  // the scratch buffer the sort ended in is free again
@@ -484,7 +510,7 @@ struct Engine {
            L.status, L.counters, L.scalars + 1, L.flags);
     // Dense ids are < active/2 (every group has two or more rows).
     const u32 id_bits = bits_for(active / 2 > 0 ? active / 2 - 1 : 0);
-    const u32 t = static_cast<u32>((active + kSortTile - 1) / kSortTile);
+    const u32 t = static_cast<u32>((active + c.sort_tile - 1) / c.sort_tile);
     const u64 b2[2] = {0, active};
     const u32 t2[2] = {0, t};
     std::memcpy(c.host_small + 4096, b2, 16);
@@ -561,7 +587,7 @@ struct Engine {
       launch("long_rows", 0, long_rows_kernel, u64(c.sm_count) * 8, 256, 0, L.text,
              static_cast<const LongRow*>(longs), static_cast<const u64*>(L.scalars + 5),
              long_cap, segments(), lcp, spos, sval);
-      const u32 t = static_cast<u32>((q + kSortTile - 1) / kSortTile);
+      const u32 t = static_cast<u32>((q + c.sort_tile - 1) / c.sort_tile);
       const u64 b2[2] = {0, q};
       const u32 t2[2] = {0, t};
       std::memcpy(c.host_small + 4096, b2, 16);
@@ -759,11 +785,13 @@ sufgpu_status sufgpu_create(sufgpu_ctx** out, int device) {
     SG_CUDA(cudaMallocHost(reinterpret_cast<void**>(&ctx->host_small), 1u << 20));
     for (auto& ev : ctx->ev) SG_CUDA(cudaEventCreate(&ev));
     for (bool ballot : {true, false}) {
-      for (u32 block : {256u, 512u}) {
-        for (bool vals : {true, false}) {
-          const OnesweepVariant v = onesweep_variant(ballot, block, vals);
-          SG_CUDA(cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(v.smem)));
+      for (u32 tile : {2048u, 4096u}) {
+        for (u32 block : {256u, 512u}) {
+          for (bool vals : {true, false}) {
+            const OnesweepVariant v = onesweep_variant(ballot, block, tile, vals);
+            SG_CUDA(cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(v.smem)));
+          }
         }
       }
     }
@@ -1041,6 +1069,9 @@ extern "C" sufgpu_status sufgpu_set_tuning(sufgpu_ctx* ctx, const char* key, int
   } else if (k == "packed_max_bits") {
     if (value < 0 || value > 32) return fail(ctx, SUFGPU_INVALID_INPUT, "packed_max_bits out of range");
     ctx->packed_max_bits = static_cast<u32>(value);
+  } else if (k == "sort_tile") {
+    if (value != 2048 && value != 4096) return fail(ctx, SUFGPU_INVALID_INPUT, "sort_tile must be 2048 or 4096");
+    ctx->sort_tile = static_cast<u32>(value);
   } else if (k == "sort_block") {
     if (value != 256 && value != 512) return fail(ctx, SUFGPU_INVALID_INPUT, "sort_block must be 256 or 512");
     ctx->sort_block = static_cast<u32>(value);

@@ -27,6 +27,7 @@ struct SortSegments {
   const u32* tile_begin;  // count+1 tile offsets
   u32 count;
   u32 total_tiles;
+  u32 tile_size = kSortTile;  // keys per tile (the onesweep variant's tile)
 };
 
 __device__ __forceinline__ void segment_of_tile(const SortSegments& s, u32 tile,
@@ -41,10 +42,10 @@ __device__ __forceinline__ void segment_of_tile(const SortSegments& s, u32 tile,
   // Skip empty segments that share the tile offset.
   while (lo + 1 < s.count && s.tile_begin[lo + 1] <= tile) ++lo;
   *seg = lo;
-  const u64 start = s.begin[lo] + static_cast<u64>(tile - s.tile_begin[lo]) * kSortTile;
+  const u64 start = s.begin[lo] + static_cast<u64>(tile - s.tile_begin[lo]) * s.tile_size;
   const u64 end_seg = s.begin[lo + 1];
   *first = start;
-  *last = start + kSortTile < end_seg ? start + kSortTile : end_seg;
+  *last = start + s.tile_size < end_seg ? start + s.tile_size : end_seg;
 }
 
 // hist layout: [segment][pass][digit], u32 counts.  Per item and pass a warp
@@ -62,8 +63,9 @@ radix_histogram_kernel(const u64* __restrict__ keys, SortSegments segs,
   u64 first, last;
   segment_of_tile(segs, blockIdx.x, &seg, &first, &last);
   const u32 lane = threadIdx.x & 31;
+  const int items = static_cast<int>(segs.tile_size / kSortBlock);
 #pragma unroll 4
-  for (int item = 0; item < kSortItems; ++item) {
+  for (int item = 0; item < items; ++item) {
     const u64 idx = first + static_cast<u64>(item) * kSortBlock + threadIdx.x;
     const bool valid = idx < last;
     const u64 key = valid ? keys[idx] : 0;
@@ -114,10 +116,10 @@ radix_offsets_kernel(const u32* __restrict__ hist, const u64* __restrict__ begin
 // One LSD pass over bits [shift, shift+8), for a tile of kSortTile pairs
 // handled by kBlock threads x kItems items.  Shared memory holds the tile's
 // keys and values in sorted-slot order and per-warp digit counters.
-template <int kBlock>
+template <int kBlock, int kTile = kSortTile>
 struct OnesweepSmem {
-  u64 keys[kSortTile];
-  u32 vals[kSortTile];
+  u64 keys[kTile];
+  u32 vals[kTile];
   u32 warp_hist[kBlock / 32][kRadixDigits];
   u32 digit_excl[kRadixDigits];
   long long digit_gbase[kRadixDigits];
@@ -127,18 +129,20 @@ struct OnesweepSmem {
 
 // kVals = false sorts keys only (vals_in/vals_out unused): the packed seed
 // carries each suffix's instance-local index in the low key bits.
+// Blocks per SM: three 256x16, four 256x8, two 512x8.  Registers are capped so
+// that occupancy, not the allocator, decides.
 template <bool kBallot, int kBlock, int kItems, bool kVals = true>
-static __global__ void __launch_bounds__(kBlock)
+static __global__ void __launch_bounds__(kBlock, kBlock == 512 ? 2 : (kItems <= 8 ? 4 : 3))
 radix_onesweep_kernel(const u64* __restrict__ keys_in,
                       const u32* __restrict__ vals_in,
                       u64* __restrict__ keys_out, u32* __restrict__ vals_out,
                       SortSegments segs, u32 shift, u32 pass, u32 passes,
                       const u64* __restrict__ digit_start, u64* status,
                       u32* tile_counter, DeviceFlags* flags) {
-  static_assert(kBlock * kItems == kSortTile, "tile size is fixed");
   static_assert(kBlock >= kRadixDigits, "one thread per digit");
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  OnesweepSmem<kBlock>& sm = *reinterpret_cast<OnesweepSmem<kBlock>*>(smem_raw);
+  OnesweepSmem<kBlock, kBlock * kItems>& sm =
+      *reinterpret_cast<OnesweepSmem<kBlock, kBlock * kItems>*>(smem_raw);
   constexpr int kWarps = kBlock / 32;
   const u32 lane = threadIdx.x & 31;
   const u32 warp = threadIdx.x >> 5;
