@@ -107,7 +107,7 @@ typedef struct sufgpu_build_stats {
   uint64_t irreducible_long;  /* PLCP positions finished by a warp */
   uint64_t anchors;
   uint32_t kernel_launches;   /* kernels launched by this call */
-  uint32_t reserved;
+  uint32_t long_runs;         /* single-symbol runs split directly after the seed */
 } sufgpu_build_stats;
 
 typedef struct sufgpu_ctx sufgpu_ctx;
@@ -185,7 +185,9 @@ SUFGPU_API sufgpu_status sufgpu_profile_entry(const sufgpu_ctx *ctx, uint32_t in
  *   "sort_block"    onesweep threads per 4096-key tile: 256 or 512 (2048-key
  *                   tiles always use 256);
  *   "packed_max_bits" instances of at most 2^v symbols use the packed
- *                   keys-only seed (index in the low key bits); 0 = never.
+ *                   keys-only seed (index in the low key bits); 0 = never;
+ *   "run_split"     1 = suffixes inside long single-symbol runs (N gaps) are
+ *                   ordered directly after the seed, 0 = by the rounds.
  * Results are identical for every setting; only speed changes. */
 SUFGPU_API sufgpu_status sufgpu_set_tuning(sufgpu_ctx *ctx, const char *key, int64_t value);
 

@@ -202,7 +202,8 @@ seed_rank_kernel(const u64* __restrict__ keys, u32* __restrict__ sa,
                  u64 n, Segments segs, u32 packed_shift, u32 bits, u32 symbols,
                  u64* __restrict__ pairs, u32* __restrict__ lcp,
                  u32* __restrict__ active, u64* status_max, u64* status_sum,
-                 u32* tile_counter, u64* active_count, DeviceFlags* flags) {
+                 u32* tile_counter, u64* active_count, DeviceFlags* flags,
+                 u32 run_keys = 0) {
   __shared__ u64 warp_smem[kScanBlock / 32];
   __shared__ u64 tile_prefix[2];
   __shared__ u32 tile_slot;
@@ -235,14 +236,22 @@ seed_rank_kernel(const u64* __restrict__ keys, u32* __restrict__ sa,
       lcp[r] = v;
     }
   }
+  // With run_keys set, rows whose seed key is one symbol repeated s times
+  // (members of long runs) stay off the active list: the run split places
+  // them (runs.cuh).
+  const u64 run_low = symbols > 1 ? (1ull << (bits * (symbols - 1))) - 1 : 0;
+  bool active_row[kScanItems];
   u64 head_max = 0;  // inclusive running max within the thread
   u32 act = 0;
 #pragma unroll
   for (int i = 0; i < kScanItems; ++i) {
     const u64 r = row0 + i;
+    active_row[i] = false;
     if (r < n) {
       if (head[i]) head_max = r;
-      if (!(head[i] && head[i + 1])) ++act;
+      const bool run_member = run_keys && (k[i + 1] >> bits) == (k[i + 1] & run_low);
+      active_row[i] = !(head[i] && head[i + 1]) && !run_member;
+      act += active_row[i];
     }
   }
   u64 agg_max, agg_sum;
@@ -278,7 +287,7 @@ seed_rank_kernel(const u64* __restrict__ keys, u32* __restrict__ sa,
         continue;
       }
       pairs[r] = (static_cast<u64>(p) << 32) | static_cast<u32>(running_max);
-      if (!(head[i] && head[i + 1])) active[out++] = p;
+      if (active_row[i]) active[out++] = p;
     }
   }
   const u64 tiles = (n + kScanTile - 1) / kScanTile;
@@ -311,6 +320,34 @@ window_scatter_kernel(const u64* __restrict__ pairs, u64 n, u32* __restrict__ ra
   for (u32 i = threadIdx.x; i < count; i += 256) rank[first + i] = window[i];
 }
 
+// Long-run lookup for the rounds (runs.cuh builds it): sorted run starts and
+// ends plus a bitmap of the 2^kRunBlockBits-position blocks that hold run
+// members.  count == 0 disables it.
+constexpr u32 kRunBlockBits = 12;
+
+struct RunIndex {
+  const u32* a = nullptr;     // sorted starts
+  const u32* e = nullptr;     // matching ends
+  const u32* bitmap = nullptr;
+  u32 count = 0;
+};
+
+// The run end e if p is a member with at least h symbols of run ahead, else 0.
+__device__ __forceinline__ u64 run_jump(const RunIndex& ri, u64 p, u64 h) {
+  if (ri.count == 0) return 0;
+  const u64 blk = p >> kRunBlockBits;
+  if (!((ri.bitmap[blk >> 5] >> (blk & 31)) & 1u)) return 0;
+  u32 lo = 0, hi = ri.count;  // last run with a <= p
+  if (ri.a[0] > p) return 0;
+  while (hi - lo > 1) {
+    const u32 mid = (lo + hi) >> 1;
+    if (ri.a[mid] <= p) lo = mid;
+    else hi = mid;
+  }
+  const u64 e = ri.e[lo];
+  return (p < e && e - p >= h) ? e : 0;
+}
+
 // Round step 1: composite keys for the active list.  counters: *group_count
 // receives the number of groups G.  ghead/gstart are indexed by dense id.
 // inst_h, when set, holds each segment's own prefix length h (the served
@@ -322,7 +359,8 @@ round_keys_kernel(const u32* __restrict__ active, u64 count,
                   u32 second_bits, u64* __restrict__ ckey,
                   u32* __restrict__ cval, u32* __restrict__ ghead,
                   u32* __restrict__ gstart, u64 group_cap, u64* status_sum,
-                  u32* tile_counter, u64* group_count, DeviceFlags* flags) {
+                  u32* tile_counter, u64* group_count, DeviceFlags* flags,
+                  RunIndex runs) {
   __shared__ u64 warp_smem[kScanBlock / 32];
   __shared__ u64 tile_prefix;
   __shared__ u32 tile_slot;
@@ -377,7 +415,8 @@ round_keys_kernel(const u32* __restrict__ active, u64 count,
         q = p + inst_h[j];
       } else {
         end = segment_end(segs, p);
-        q = p + h;
+        const u64 jump = run_jump(runs, p, h);  // a long-run member: its run end
+        q = jump ? jump : p + h;
       }
       const u64 second = q < end ? static_cast<u64>(rank[q]) + 1 : 0;
       ckey[a] = ((dense - 1) << second_bits) | second;

@@ -30,6 +30,7 @@
 #include "lcp.cuh"
 #include "pack.cuh"
 #include "radix.cuh"
+#include "runs.cuh"
 #include "serve.cuh"
 
 using namespace sufgpu;
@@ -106,8 +107,24 @@ struct Layout {
   u32* alpha;        // 256 byte counts
   u16* code;         // 256 symbol codes (1..sigma)
   DeviceFlags* flags;
+  // Long-run split (runs.cuh): boundary records, per-run and per-class
+  // layout, the round lookup (sorted starts/ends) and its block bitmap.
+  u64 run_cap;
+  u64* run_starts;
+  u64* run_ends;
+  RunRecord* run_recs;
+  RunClass* run_classes;
+  u32* run_len;
+  u64* run_prefix;
+  u32* run_a;
+  u32* run_e;
+  u32* run_bitmap;
+  u64 run_bitmap_words;
   u64 total;
 };
+
+// Most long runs one build splits directly (more are left to the rounds).
+u64 run_capacity(u64 n) { return std::min<u64>(u64(1) << 17, n / 8 + 64); }
 
 Layout plan_layout(u8* base, u64 n, u32 segments) {
   Layout l{};
@@ -142,6 +159,17 @@ Layout plan_layout(u8* base, u64 n, u32 segments) {
   l.alpha = reinterpret_cast<u32*>(take(256 * 4));
   l.code = reinterpret_cast<u16*>(take(512));
   l.flags = reinterpret_cast<DeviceFlags*>(take(sizeof(DeviceFlags)));
+  l.run_cap = run_capacity(n);
+  l.run_starts = reinterpret_cast<u64*>(take(l.run_cap * 8));
+  l.run_ends = reinterpret_cast<u64*>(take(l.run_cap * 8));
+  l.run_recs = reinterpret_cast<RunRecord*>(take(l.run_cap * sizeof(RunRecord)));
+  l.run_classes = reinterpret_cast<RunClass*>(take(2 * l.run_cap * sizeof(RunClass)));
+  l.run_len = reinterpret_cast<u32*>(take(l.run_cap * 4));
+  l.run_prefix = reinterpret_cast<u64*>(take(3 * l.run_cap * 8));
+  l.run_a = reinterpret_cast<u32*>(take(l.run_cap * 4));
+  l.run_e = reinterpret_cast<u32*>(take(l.run_cap * 4));
+  l.run_bitmap_words = ((std::max<u64>(n, 1) - 1) >> kRunBlockBits) / 32 + 1;
+  l.run_bitmap = reinterpret_cast<u32*>(take(l.run_bitmap_words * 4));
   l.total = off;
   return l;
 }
@@ -234,6 +262,8 @@ struct sufgpu_ctx {
   u64 ballot_min_elems = u64(1) << 23;
   // Largest instance index width for the packed (keys-only) seed; 0 = never.
   u32 packed_max_bits = 24;
+  // Split long single-symbol runs directly after the seed (runs.cuh).
+  bool run_split = true;
   // Onesweep block size (256 threads x 16 keys or 512 x 8).
   u32 sort_block = 256;
   // Keys per onesweep tile (2048 or 4096).
@@ -255,6 +285,18 @@ struct Engine {
   u32* spare = nullptr;
   u32 seed_length = 0;  // symbols every seed group shares
   u64 rank_rows = 0;    // rows a rank may name (n, or the arena capacity)
+  // Long-run split (runs.cuh): allowed by suffix_sort, on once runs were
+  // found and laid out.  The host vectors back the uploads until the build ends.
+  bool allow_runs = false;
+  bool runs_on = false;
+  u32 run_count = 0;
+  u64 run_members = 0;
+  u64 run_active = 0;
+  RunIndex run_index{};
+  std::vector<RunRecord> h_recs;
+  std::vector<RunClass> h_classes;
+  std::vector<u32> h_len, h_a, h_e, h_bitmap;
+  std::vector<u64> h_prefix;
 
   explicit Engine(sufgpu_ctx& ctx) : c(ctx) {}
 
@@ -382,6 +424,127 @@ struct Engine {
   }
   u32 last_tiles = 0;
 
+  // ---- Long runs of one symbol: find them, pair starts with ends and lay out
+  // their sub-groups (runs.cuh).  Leaves runs_on false when there are none,
+  // too many, or the seed is too short for the split to pay.
+  void plan_runs(u32 s) {
+    runs_on = false;
+    run_index = RunIndex{};
+    if (!allow_runs || !c.run_split || s < 8 || n < 2 * u64(s)) return;
+    zero(L.scalars + 8, 16);
+    launch("long_runs", n, long_runs_kernel,
+           grid_stride_blocks((n + kRunChunk - 1) / kRunChunk, 256), 256, 0, L.text, n,
+           segments(), s, L.run_starts, L.run_ends, L.run_cap, L.scalars + 8);
+    SG_CUDA(cudaMemcpyAsync(c.host_scalars + 8, L.scalars + 8, 16, cudaMemcpyDeviceToHost,
+                            c.stream));
+    sync();
+    const u64 count = c.host_scalars[8];
+    if (count != c.host_scalars[9]) {
+      throw BuildError{SUFGPU_BUILD_FAILURE, "long-run starts and ends do not pair"};
+    }
+    if (count == 0 || count > L.run_cap) return;
+    std::vector<u64> starts(count), ends(count);
+    SG_CUDA(cudaMemcpyAsync(starts.data(), L.run_starts, count * 8, cudaMemcpyDeviceToHost,
+                            c.stream));
+    SG_CUDA(cudaMemcpyAsync(ends.data(), L.run_ends, count * 8, cudaMemcpyDeviceToHost,
+                            c.stream));
+    sync();
+    std::sort(starts.begin(), starts.end());
+    std::sort(ends.begin(), ends.end());
+    // Runs in position order; key (instance, symbol, class) names the class.
+    std::vector<u64> key(count);
+    std::vector<u32> len(count);
+    h_a.resize(count);
+    h_e.resize(count);
+    for (u64 i = 0; i < count; ++i) {
+      const u64 a = starts[i] >> 8, e = ends[i] >> 1;
+      const u64 sym = starts[i] & 0xff, cls = ends[i] & 1;
+      if (e <= a || e - a < s || (i > 0 && a < h_e[i - 1])) {
+        throw BuildError{SUFGPU_BUILD_FAILURE, "inconsistent long-run boundaries"};
+      }
+      const u64 seg = segs == 1 ? 0
+          : static_cast<u64>(std::upper_bound(begin.begin(), begin.end(), a) - begin.begin()) - 1;
+      if (e > begin[seg + 1]) throw BuildError{SUFGPU_BUILD_FAILURE, "long run crosses an instance"};
+      h_a[i] = static_cast<u32>(a);
+      h_e[i] = static_cast<u32>(e);
+      len[i] = static_cast<u32>(e - a);
+      key[i] = (seg << 9) | (sym << 1) | cls;
+    }
+    std::map<u64, std::vector<u32>> classes;
+    for (u32 i = 0; i < count; ++i) classes[key[i]].push_back(i);
+    std::map<u64, u64> class0_size;  // per (instance, symbol)
+    for (const auto& kv : classes) {
+      if (kv.first & 1) continue;
+      u64 size = 0;
+      for (u32 i : kv.second) size += len[i] - s + 1;
+      class0_size[kv.first >> 1] = size;
+    }
+    h_recs.assign(count, RunRecord{});
+    h_classes.clear();
+    h_len.clear();
+    h_prefix.clear();
+    run_active = 0;
+    for (auto& kv : classes) {
+      std::vector<u32>& idx = kv.second;
+      std::stable_sort(idx.begin(), idx.end(), [&](u32 x, u32 y) { return len[x] < len[y]; });
+      RunClass k{};
+      k.cls = static_cast<u32>(kv.first & 1);
+      k.m = static_cast<u32>(idx.size());
+      k.off = static_cast<u32>(h_len.size());
+      k.poff = static_cast<u32>(h_prefix.size());
+      u64 acc = 0, size = 0;
+      h_prefix.push_back(0);
+      for (u32 t = 0; t < k.m; ++t) {
+        const u32 L_t = len[idx[t]];
+        h_len.push_back(L_t);
+        acc += k.cls == 0 ? L_t - s + 1 : L_t;
+        h_prefix.push_back(acc);
+        size += L_t - s + 1;
+        h_recs[idx[t]].slot = k.m - 1 - t;
+        h_recs[idx[t]].desc = static_cast<u32>(h_classes.size());
+      }
+      // Sub-groups of two or more rows: d <= the second-longest run.
+      u64 act = 0;
+      if (k.m >= 2) {
+        const u64 second = h_len[k.off + k.m - 2];
+        for (u32 t = 0; t < k.m; ++t) act += std::min<u64>(len[idx[t]], second) - s + 1;
+      }
+      k.size = size;
+      k.act_count = act;
+      k.base_rel = k.cls == 0 ? 0 : class0_size[kv.first >> 1];
+      k.act_first_rel = k.cls == 0 ? 0 : size - act;
+      k.act_off = run_active;
+      run_active += act;
+      h_classes.push_back(k);
+    }
+    run_members = 0;
+    h_bitmap.assign(L.run_bitmap_words, 0);
+    for (u64 i = 0; i < count; ++i) {
+      h_recs[i].first_member = run_members;
+      h_recs[i].a = h_a[i];
+      h_recs[i].e = h_e[i];
+      run_members += len[i] - s + 1;
+      const u64 last_member = h_e[i] - s;
+      for (u64 b = h_a[i] >> kRunBlockBits; b <= (last_member >> kRunBlockBits); ++b) {
+        h_bitmap[b >> 5] |= 1u << (b & 31);
+      }
+    }
+    auto put = [&](void* dst, const void* src, u64 bytes) {
+      SG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c.stream));
+    };
+    put(L.run_recs, h_recs.data(), count * sizeof(RunRecord));
+    put(L.run_classes, h_classes.data(), h_classes.size() * sizeof(RunClass));
+    put(L.run_len, h_len.data(), h_len.size() * 4);
+    put(L.run_prefix, h_prefix.data(), h_prefix.size() * 8);
+    put(L.run_a, h_a.data(), count * 4);
+    put(L.run_e, h_e.data(), count * 4);
+    put(L.run_bitmap, h_bitmap.data(), h_bitmap.size() * 4);
+    run_count = static_cast<u32>(count);
+    run_index = RunIndex{L.run_a, L.run_e, L.run_bitmap, run_count};
+    runs_on = true;
+    st.long_runs = count;
+  }
+
   // ---- Seed phase: alphabet remap, seed keys, the segmented seed sort and
   // seed ranks.  Leaves SA in `sa` (sa_out when given), head-row ranks in
   // L.rank, seed-boundary LCPs in L.lcp and the active list in L.x; returns
@@ -422,6 +585,7 @@ struct Engine {
     // Seed keys and the segmented seed sort.
     upload_segments(begin);
     const u32 seed_tiles = last_tiles;
+    plan_runs(symbols);
     const u32 seed_bits = bits * symbols;
     const u32 seed_passes = (seed_bits + kRadixBits - 1) / kRadixBits;
     zero(L.hist, u64(segs) * seed_passes * kRadixDigits * 4);
@@ -459,7 +623,8 @@ struct Engine {
     u64* pairs = keys == L.k0 ? L.k1 : L.k0;
     launch("seed_rank", n * 24, seed_rank_kernel, scan_tiles, kScanBlock, 0,
            static_cast<const u64*>(keys), sa, n, segments(), packed_shift, bits, symbols,
-           pairs, L.lcp, L.x, status_max, status_sum, L.counters, L.scalars + 0, L.flags);
+           pairs, L.lcp, L.x, status_max, status_sum, L.counters, L.scalars + 0, L.flags,
+           runs_on ? 1u : 0u);
     // rank[SA[r]] = head: group the pairs by 2048-position window (keys-only
     // passes over the position's high bits), then one coalesced window write.
     const u32 pos_bits = std::max<u32>(1, bits_for(n - 1));
@@ -480,12 +645,24 @@ struct Engine {
     }
     launch("window_scatter", n * 12, window_scatter_kernel, (n + kWindow - 1) / kWindow, 256, 0,
            static_cast<const u64*>(grouped), n, L.rank, L.flags);
+    u64 active = read_scalar(0);
+    if (runs_on) {
+      // Members of long runs: sub-group rows and ranks, and the rows in
+      // sub-groups of two or more appended to the active list.
+      launch("run_heads", u64(run_count) * 8, run_heads_kernel, (run_count + 255) / 256, 256, 0,
+             L.run_recs, run_count, static_cast<const u32*>(L.rank));
+      launch("run_split", run_members * 12, run_split_kernel, grid_stride_blocks(run_members, 256),
+             256, 0, static_cast<const RunRecord*>(L.run_recs), run_count,
+             static_cast<const RunClass*>(L.run_classes), static_cast<const u32*>(L.run_len),
+             static_cast<const u64*>(L.run_prefix), symbols, run_members, n, sa, L.rank, L.x,
+             active, L.flags);
+      active += run_active;
+    }
     if (sa_out && sa_out != sa) {
       SG_CUDA(cudaMemcpyAsync(sa_out, sa, n * 4, cudaMemcpyDeviceToDevice, c.stream));
       spare = sa;  // the scratch buffer the sort ended in is free again
       sa = sa_out;
     }
-    const u64 active = read_scalar(0);
     st.active_first = active;
     seed_length = symbols;
     return active;
@@ -507,7 +684,7 @@ struct Engine {
     zero(L.counters, 4);
     launch("round_keys", active * 28, round_keys_kernel, tiles, kScanBlock, 0, act, active,
            L.rank, h, inst_h, segs, second_bits, L.k0, other, ghead, gstart, u64(n / 2),
-           L.status, L.counters, L.scalars + 1, L.flags);
+           L.status, L.counters, L.scalars + 1, L.flags, inst_h ? RunIndex{} : run_index);
     // Dense ids are < active/2 (every group has two or more rows).
     const u32 id_bits = bits_for(active / 2 > 0 ? active / 2 - 1 : 0);
     const u32 t = static_cast<u32>((active + c.sort_tile - 1) / c.sort_tile);
@@ -535,6 +712,7 @@ struct Engine {
 
   // ---- The doubling sort: leaves SA in `sa` and ISA (global rows) in rank.
   void suffix_sort() {
+    allow_runs = true;
     u64 active = seed_phase();
     // Rounds.  act and other alternate between x and the spare SA-sized
     // buffer; y holds the per-group tables.
@@ -1072,6 +1250,8 @@ extern "C" sufgpu_status sufgpu_set_tuning(sufgpu_ctx* ctx, const char* key, int
   } else if (k == "sort_tile") {
     if (value != 2048 && value != 4096) return fail(ctx, SUFGPU_INVALID_INPUT, "sort_tile must be 2048 or 4096");
     ctx->sort_tile = static_cast<u32>(value);
+  } else if (k == "run_split") {
+    ctx->run_split = value != 0;
   } else if (k == "sort_block") {
     if (value != 256 && value != 512) return fail(ctx, SUFGPU_INVALID_INPUT, "sort_block must be 256 or 512");
     ctx->sort_block = static_cast<u32>(value);

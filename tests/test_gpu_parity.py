@@ -159,4 +159,5 @@ def test_workload3_scaled_low_memory(ctx):
     split40 SA and byte-coded LCP word for word against the reference."""
     t = synth.human_scale_3gbp(scale=0.01).logical_text()
     r = check_full(ctx, t, sa_bits=40, isa_bits=0, lcp=sg.LcpEncoding.BYTE32)
-    assert r.stats["rounds"] >= 10
+    # The N runs are split directly after the seed instead of by ~17 rounds.
+    assert r.stats["long_runs"] > 0 and r.stats["rounds"] < 10
