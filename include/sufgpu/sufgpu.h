@@ -108,6 +108,8 @@ typedef struct sufgpu_build_stats {
   uint64_t anchors;
   uint32_t kernel_launches;   /* kernels launched by this call */
   uint32_t long_runs;         /* single-symbol runs split directly after the seed */
+  uint32_t seg_sort_fallbacks;/* rounds whose groups did not fit the shared-memory sort */
+  uint32_t reserved;
 } sufgpu_build_stats;
 
 typedef struct sufgpu_ctx sufgpu_ctx;
@@ -187,7 +189,10 @@ SUFGPU_API sufgpu_status sufgpu_profile_entry(const sufgpu_ctx *ctx, uint32_t in
  *   "packed_max_bits" instances of at most 2^v symbols use the packed
  *                   keys-only seed (index in the low key bits); 0 = never;
  *   "run_split"     1 = suffixes inside long single-symbol runs (N gaps) are
- *                   ordered directly after the seed, 0 = by the rounds.
+ *                   ordered directly after the seed, 0 = by the rounds;
+ *   "seg_sort"      1 = each round sorts its groups inside shared memory
+ *                   (global passes only when a group exceeds a block), 0 =
+ *                   every round takes the global passes.
  * Results are identical for every setting; only speed changes. */
 SUFGPU_API sufgpu_status sufgpu_set_tuning(sufgpu_ctx *ctx, const char *key, int64_t value);
 

@@ -85,10 +85,11 @@ class _Stats(ctypes.Structure):
                 ("active_rows", ctypes.c_uint64), ("active_first", ctypes.c_uint64),
                 ("irreducible_long", ctypes.c_uint64),
                 ("anchors", ctypes.c_uint64), ("kernel_launches", ctypes.c_uint32),
-                ("long_runs", ctypes.c_uint32)]
+                ("long_runs", ctypes.c_uint32), ("seg_sort_fallbacks", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
 
     def as_dict(self) -> dict:
-        return {name: getattr(self, name) for name, _ in self._fields_}
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
 
 
 class _ServerConfig(ctypes.Structure):

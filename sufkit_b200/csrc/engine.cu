@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <chrono>
 #include <condition_variable>
 #include <cstdio>
@@ -31,6 +32,7 @@
 #include "pack.cuh"
 #include "radix.cuh"
 #include "runs.cuh"
+#include "segsort.cuh"
 #include "serve.cuh"
 
 using namespace sufgpu;
@@ -264,6 +266,8 @@ struct sufgpu_ctx {
   u32 packed_max_bits = 24;
   // Split long single-symbol runs directly after the seed (runs.cuh).
   bool run_split = true;
+  // Sort each round's groups in shared memory (segsort.cuh).
+  bool seg_sort = true;
   // Onesweep block size (256 threads x 16 keys or 512 x 8).
   u32 sort_block = 256;
   // Keys per onesweep tile (2048 or 4096).
@@ -564,11 +568,33 @@ struct Engine {
     for (int b = 0; b < 256; ++b) code[b] = counts[b] ? static_cast<u16>(++sigma) : 0;
     const u32 bits = std::max<u32>(1, bits_for(sigma));
     u32 symbols = 64 / bits;
-    if (c.seed_symbols) symbols = std::min(symbols, c.seed_symbols);
-    // Packed seed: when every instance fits 2^packed_max_bits symbols, its
-    // local index rides in the low key bits and the sort moves keys only.
     u64 longest = 1;
     for (u32 j = 0; j < segs; ++j) longest = std::max<u64>(longest, begin[j + 1] - begin[j]);
+    if (c.seed_symbols) {
+      symbols = std::min(symbols, c.seed_symbols);
+    } else {
+      // Enough symbols that two seed keys of one instance rarely collide by
+      // chance, log2(longest) / H + 2.5 with H the text's entropy in bits per
+      // symbol, plus one per doubling beyond 2^27 symbols (larger genomes
+      // hold more repeat copies), rounded up to whole 8-bit radix passes.
+      // Longer seeds cost a pass per 8 bits; shorter ones leave more rows to
+      // the rounds.
+      double entropy = 0;
+      for (int b = 0; b < 256; ++b) {
+        if (!counts[b]) continue;
+        const double q = static_cast<double>(counts[b]) / static_cast<double>(n);
+        entropy -= q * std::log2(q);
+      }
+      if (entropy > 0.5) {
+        const double lg = std::log2(static_cast<double>(longest));
+        const double want = lg / entropy + 2.5 + std::max(0.0, lg - 27.0);
+        const u32 need = static_cast<u32>(std::ceil(want));
+        const u32 passes = (need * bits + kRadixBits - 1) / kRadixBits;
+        symbols = std::min(symbols, std::max<u32>(1, passes * kRadixBits / bits));
+      }
+    }
+    // Packed seed: when every instance fits 2^packed_max_bits symbols, its
+    // local index rides in the low key bits and the sort moves keys only.
     const u32 index_bits = std::max<u32>(1, bits_for(longest - 1));
     u32 packed_shift = 0;
     if (c.packed_max_bits && index_bits <= c.packed_max_bits) {
@@ -694,8 +720,34 @@ struct Engine {
     std::memcpy(c.host_small + 4096 + 16, t2, 8);
     SG_CUDA(cudaMemcpyAsync(L.sort_begin, c.host_small + 4096, 16, cudaMemcpyHostToDevice, c.stream));
     SG_CUDA(cudaMemcpyAsync(L.sort_tiles, c.host_small + 4096 + 16, 8, cudaMemcpyHostToDevice, c.stream));
-    const bool sw = radix_sort("round_onesweep", L.k0, other, L.k1, act, L.sort_begin, L.sort_tiles,
-                               1, t, active, 0, second_bits + id_bits, false);
+    // Rows only move inside their groups: sort whole groups in shared memory
+    // (segsort.cuh) unless some group is too large for a block, in which case
+    // the round takes the global passes over (id, second) bits.
+    bool sw = false;
+    bool sorted = false;
+    if (c.seg_sort) {
+      zero(L.counters + 48, 4);
+      launch("seg_sort", active * 24, seg_sort_kernel, (active + kSegWindow - 1) / kSegWindow,
+             kSegBlock, sizeof(SegSortSmem), static_cast<const u64*>(L.k0),
+             static_cast<const u32*>(other), active, static_cast<const u32*>(gstart),
+             static_cast<const u64*>(L.scalars + 1), second_bits, L.k1, act, L.counters + 48,
+             L.flags);
+      SG_CUDA(cudaMemcpyAsync(c.host_small + 8192, L.counters + 48, 4, cudaMemcpyDeviceToHost,
+                              c.stream));
+      sync();
+      u32 big = 0;
+      std::memcpy(&big, c.host_small + 8192, 4);
+      if (big == 0) {
+        sw = true;
+        sorted = true;
+      } else {
+        ++st.seg_sort_fallbacks;
+      }
+    }
+    if (!sorted) {
+      sw = radix_sort("round_onesweep", L.k0, other, L.k1, act, L.sort_begin, L.sort_tiles, 1, t,
+                      active, 0, second_bits + id_bits, false);
+    }
     u64* ck = sw ? L.k1 : L.k0;
     u32* cv = sw ? act : other;
     u32* next = sw ? other : act;
@@ -962,6 +1014,8 @@ sufgpu_status sufgpu_create(sufgpu_ctx** out, int device) {
     SG_CUDA(cudaMallocHost(reinterpret_cast<void**>(&ctx->host_scalars), 64 * 8));
     SG_CUDA(cudaMallocHost(reinterpret_cast<void**>(&ctx->host_small), 1u << 20));
     for (auto& ev : ctx->ev) SG_CUDA(cudaEventCreate(&ev));
+    SG_CUDA(cudaFuncSetAttribute(seg_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(sizeof(SegSortSmem))));
     for (bool ballot : {true, false}) {
       for (u32 tile : {2048u, 4096u}) {
         for (u32 block : {256u, 512u}) {
@@ -1250,6 +1304,8 @@ extern "C" sufgpu_status sufgpu_set_tuning(sufgpu_ctx* ctx, const char* key, int
   } else if (k == "sort_tile") {
     if (value != 2048 && value != 4096) return fail(ctx, SUFGPU_INVALID_INPUT, "sort_tile must be 2048 or 4096");
     ctx->sort_tile = static_cast<u32>(value);
+  } else if (k == "seg_sort") {
+    ctx->seg_sort = value != 0;
   } else if (k == "run_split") {
     ctx->run_split = value != 0;
   } else if (k == "sort_block") {

@@ -46,6 +46,9 @@ long_runs_kernel(const u8* __restrict__ text, u64 n, Segments segs, u32 s,
     // A run of >= 16 identical bytes covers a whole aligned 8-byte word, so
     // with s >= 16 a chunk that starts or ends one sees a uniform word among
     // the chunk's two and its neighbours' (random sequence: almost never).
+    // With 11 <= s < 16 a run covers two consecutive aligned 4-byte words
+    // in [base - 8, base + 24); with 8 <= s < 11 one aligned 4-byte word in
+    // [base - 4, base + 20).
     if (s >= 16) {
       const u64* w8 = reinterpret_cast<const u64*>(text + base);
       const u64 around[4] = {base >= 8 ? w8[-1] : 0x0102030405060708ull,
@@ -56,6 +59,23 @@ long_runs_kernel(const u8* __restrict__ text, u64 n, Segments segs, u32 s,
       for (int k = 0; k < 4; ++k) {
         any |= around[k] == (around[k] & 0xffull) * 0x0101010101010101ull;
       }
+      if (!any) continue;
+    } else if (s >= 11) {
+      const u32* w4 = reinterpret_cast<const u32*>(text + base);
+      const u32 around[8] = {base >= 8 ? w4[-2] : 0x01020304u, base >= 4 ? w4[-1] : 0x05060708u,
+                             v.x, v.y, v.z, v.w, w4[4], w4[5]};
+      bool any = false;
+#pragma unroll
+      for (int k = 0; k + 1 < 8; ++k) {
+        any |= around[k] == around[k + 1] && around[k] == (around[k] & 0xffu) * 0x01010101u;
+      }
+      if (!any) continue;
+    } else {
+      const u32* w4 = reinterpret_cast<const u32*>(text + base);
+      const u32 around[6] = {base >= 4 ? w4[-1] : 0x01020304u, v.x, v.y, v.z, v.w, w4[4]};
+      bool any = false;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) any |= around[k] == (around[k] & 0xffu) * 0x01010101u;
       if (!any) continue;
     }
     const u8 before = base > 0 ? text[base - 1] : 0;

@@ -1,0 +1,65 @@
+"""GPU: doubling rounds sort their groups in shared memory; rounds with a group
+too large for one block take the global passes.  Both give the oracle's
+output word for word, and the two strategies agree with each other."""
+import numpy as np
+import pytest
+
+import oracle
+import sufkit_b200 as sg
+from sufkit_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def expected(text):
+    if oracle.ref() is not None:
+        sa, isa, lcp, _ = oracle.ref_adapter(text, 64)
+        return sa, isa, lcp
+    return oracle.full_build(text)
+
+
+def build(ctx, text, seg_sort=1):
+    ctx.set_tuning("seg_sort", seg_sort)
+    try:
+        return ctx.build(text, sa_bits=32, isa_bits=32, lcp=sg.LcpEncoding.RAW32, validate=True)
+    finally:
+        ctx.set_tuning("seg_sort", 1)
+
+
+def test_small_groups_stay_in_shared_memory(ctx):
+    t = synth.repeat_rich_100mbp(scale=0.01).logical_text()
+    r = build(ctx, t)
+    sa, isa, lcp = expected(t)
+    assert r.stats["rounds"] > 0 and r.stats["seg_sort_fallbacks"] == 0
+    assert (r.sa_low == sa).all() and (r.isa_low == isa).all() and (r.lcp == lcp).all()
+    g = build(ctx, t, seg_sort=0)
+    assert (g.sa_low == r.sa_low).all() and (g.lcp == r.lcp).all()
+
+
+@pytest.mark.parametrize("period", [2, 5, 33])
+def test_large_groups_fall_back(ctx, period):
+    rng = np.random.default_rng(period)
+    unit = rng.integers(2, 6, size=period).astype(np.uint8)
+    tandem = np.tile(unit, 150_000 // period)
+    flank = rng.integers(2, 6, size=5000).astype(np.uint8)
+    t = np.concatenate([flank, tandem, flank[::-1], tandem, np.array([1, 0], np.uint8)])
+    r = build(ctx, t)
+    sa, isa, lcp = expected(t)
+    assert r.stats["seg_sort_fallbacks"] > 0
+    assert (r.sa_low == sa).all() and (r.isa_low == isa).all() and (r.lcp == lcp).all()
+
+
+def test_groups_of_every_size_up_to_a_block(ctx):
+    # Repeat families with 2..3000 copies of one 40-symbol unit and random
+    # context: groups straddle windows and fill blocks to the limit.
+    rng = np.random.default_rng(21)
+    parts = []
+    for copies in (2, 3, 17, 255, 1024, 2047, 2048, 2049, 3000):
+        unit = rng.integers(2, 6, size=40).astype(np.uint8)
+        for _ in range(copies):
+            parts.append(unit)
+            parts.append(rng.integers(2, 6, size=int(rng.integers(1, 9))).astype(np.uint8))
+    t = np.concatenate(parts + [np.array([1, 0], np.uint8)])
+    r = build(ctx, t)
+    sa, isa, lcp = expected(t)
+    assert (r.sa_low == sa).all() and (r.isa_low == isa).all() and (r.lcp == lcp).all()
