@@ -179,7 +179,9 @@ SUFGPU_API sufgpu_status sufgpu_profile_entry(const sufgpu_ctx *ctx, uint32_t in
                                               const char **name, uint64_t *launches,
                                               double *seconds, uint64_t *bytes);
 
-/* Tuning knobs (picked by the autotuner, sufkit_b200/autotune.py):
+/* Tuning knobs (the autotuner, python -m sufkit_b200.autotune, sweeps them
+ * per size class and writes sufkit_b200/tuning.json, which the Python
+ * Context loads into sufgpu_set_tuning_class):
  *   "seed_symbols"  symbols packed per seed key, 0 = as many as fit 64 bits;
  *   "ballot_rank"   1 = onesweep ranks digits with ballots, 0 = match-any;
  *   "ballot_min_elems" smallest sort that uses ballot ranking;
@@ -195,6 +197,14 @@ SUFGPU_API sufgpu_status sufgpu_profile_entry(const sufgpu_ctx *ctx, uint32_t in
  *                   every round takes the global passes.
  * Results are identical for every setting; only speed changes. */
 SUFGPU_API sufgpu_status sufgpu_set_tuning(sufgpu_ctx *ctx, const char *key, int64_t value);
+
+/* Per-size overrides (the autotuner's table): a build whose longest instance
+ * has at most max_symbols symbols applies the settings of the smallest such
+ * class on top of the context's knobs, for that build only.  Keys and values
+ * as for sufgpu_set_tuning (checked here). */
+SUFGPU_API sufgpu_status sufgpu_set_tuning_class(sufgpu_ctx *ctx, uint64_t max_symbols,
+                                                 const char *key, int64_t value);
+SUFGPU_API void sufgpu_clear_tuning_classes(sufgpu_ctx *ctx);
 
 /* ------------------------------------------------------------------------
  * Served builds (continuous batching).  A server owns one device arena and a

@@ -23,6 +23,8 @@ import numpy as np
 
 _HERE = Path(__file__).resolve().parent
 LIBRARY_PATH = _HERE / "libsufgpu.so"
+# Per-size knob table written by the autotuner (python -m sufkit_b200.autotune).
+TUNING_PATH = _HERE / "tuning.json"
 
 
 class ErrorCode(enum.IntEnum):
@@ -146,6 +148,9 @@ _SIGNATURES = {
                                             ctypes.POINTER(ctypes.c_double),
                                             ctypes.POINTER(ctypes.c_uint64)]),
     "sufgpu_set_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int64]),
+    "sufgpu_set_tuning_class": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_char_p,
+                                               ctypes.c_int64]),
+    "sufgpu_clear_tuning_classes": (None, [ctypes.c_void_p]),
     "sufgpu_lcp_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
                                           ctypes.c_void_p, ctypes.c_void_p]),
     "sufgpu_server_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
@@ -247,9 +252,13 @@ class BuildResult:
 
 
 class Context:
-    """One CUDA device with its stream and grown device buffers."""
+    """One CUDA device with its stream and grown device buffers.
 
-    def __init__(self, device: int = 0):
+    ``tuning`` names a knob table from the autotuner (default: the packaged
+    sufkit_b200/tuning.json when it exists); ``None`` keeps the library's
+    built-in defaults.  Knobs change speed only, never results."""
+
+    def __init__(self, device: int = 0, tuning="default"):
         lib = library()
         handle = ctypes.c_void_p()
         status = lib.sufgpu_create(ctypes.byref(handle), device)
@@ -258,6 +267,29 @@ class Context:
         self._lib = lib
         self._h = handle
         self.last_stats: dict = {}
+        if tuning == "default":
+            tuning = TUNING_PATH if TUNING_PATH.exists() else None
+        if tuning is not None:
+            self.load_tuning(tuning)
+
+    def load_tuning(self, path) -> None:
+        """Applies an autotuner table: {"classes": [{"max_symbols": m,
+        "settings": {key: value}}, ...]} (replaces earlier classes)."""
+        import json
+        table = json.loads(Path(path).read_text())
+        self._lib.sufgpu_clear_tuning_classes(self._h)
+        for cls in table.get("classes", []):
+            for key, value in cls.get("settings", {}).items():
+                self.set_tuning_class(int(cls["max_symbols"]), key, int(value))
+
+    def set_tuning_class(self, max_symbols: int, key: str, value: int) -> None:
+        status = self._lib.sufgpu_set_tuning_class(self._h, int(max_symbols), key.encode(),
+                                                   int(value))
+        if status != 0:
+            _raise(status, self._error())
+
+    def clear_tuning_classes(self) -> None:
+        self._lib.sufgpu_clear_tuning_classes(self._h)
 
     def close(self):
         if self._h:

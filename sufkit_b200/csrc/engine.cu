@@ -206,6 +206,61 @@ OnesweepVariant onesweep_variant(bool ballot, u32 block, u32 tile, bool vals) {
   return vals ? variant_for<false, true>(block, tile) : variant_for<false, false>(block, tile);
 }
 
+// Build knobs.  Results are identical for every setting; only speed changes.
+struct Tuning {
+  // Symbols per seed key (0 = chosen from the instance size and entropy).
+  u32 seed_symbols = 0;
+  // Onesweep ranking: ballots over digit bits (true) or match-any (false).
+  bool ballot_rank = true;
+  // Ballot ranking only pays off on large sorts; smaller ones use match-any.
+  u64 ballot_min_elems = u64(1) << 23;
+  // Largest instance index width for the packed (keys-only) seed; 0 = never.
+  u32 packed_max_bits = 24;
+  // Split long single-symbol runs directly after the seed (runs.cuh).
+  bool run_split = true;
+  // Sort each round's groups in shared memory (segsort.cuh).
+  bool seg_sort = true;
+  // Onesweep block size (256 threads x 16 keys or 512 x 8).
+  u32 sort_block = 256;
+  // Keys per onesweep tile (2048 or 4096).
+  u32 sort_tile = 4096;
+};
+
+// Overrides for builds whose longest instance has at most max_symbols symbols.
+struct TuningClass {
+  u64 max_symbols;
+  std::vector<std::pair<std::string, int64_t>> settings;
+};
+
+// Applies one knob; returns an error message or an empty string.
+std::string apply_tuning(Tuning& t, const std::string& k, int64_t value) {
+  if (k == "seed_symbols") {
+    if (value < 0 || value > 64) return "seed_symbols out of range";
+    t.seed_symbols = static_cast<u32>(value);
+  } else if (k == "ballot_rank") {
+    t.ballot_rank = value != 0;
+  } else if (k == "ballot_min_elems") {
+    if (value < 0) return "ballot_min_elems must be >= 0";
+    t.ballot_min_elems = static_cast<u64>(value);
+  } else if (k == "packed_max_bits") {
+    if (value < 0 || value > 32) return "packed_max_bits out of range";
+    t.packed_max_bits = static_cast<u32>(value);
+  } else if (k == "sort_tile") {
+    if (value != 2048 && value != 4096) return "sort_tile must be 2048 or 4096";
+    t.sort_tile = static_cast<u32>(value);
+  } else if (k == "seg_sort") {
+    t.seg_sort = value != 0;
+  } else if (k == "run_split") {
+    t.run_split = value != 0;
+  } else if (k == "sort_block") {
+    if (value != 256 && value != 512) return "sort_block must be 256 or 512";
+    t.sort_block = static_cast<u32>(value);
+  } else {
+    return "unknown tuning key " + k;
+  }
+  return {};
+}
+
 }  // namespace
 
 struct PendingLaunch {
@@ -255,23 +310,10 @@ struct sufgpu_ctx {
   std::vector<u8> anchor_val;
   cudaEvent_t ev[8] = {};
   u32 launches = 0;
-  // Tunables (the autotuner may change them): symbols per seed key (0 = as
-  // many as fit in 64 bits).
-  u32 seed_symbols = 0;
-  // Onesweep ranking: ballots over digit bits (true) or match-any (false).
-  bool ballot_rank = true;
-  // Ballot ranking only pays off on large sorts; smaller ones use match-any.
-  u64 ballot_min_elems = u64(1) << 23;
-  // Largest instance index width for the packed (keys-only) seed; 0 = never.
-  u32 packed_max_bits = 24;
-  // Split long single-symbol runs directly after the seed (runs.cuh).
-  bool run_split = true;
-  // Sort each round's groups in shared memory (segsort.cuh).
-  bool seg_sort = true;
-  // Onesweep block size (256 threads x 16 keys or 512 x 8).
-  u32 sort_block = 256;
-  // Keys per onesweep tile (2048 or 4096).
-  u32 sort_tile = 4096;
+  // Build knobs (sufgpu_set_tuning) and per-size overrides
+  // (sufgpu_set_tuning_class, written by the autotuner).
+  Tuning tune;
+  std::vector<TuningClass> tuning_classes;
 };
 
 namespace {
@@ -363,7 +405,7 @@ struct Engine {
                   bool check_needed, bool hist_ready = false) {
     if (end_bit <= begin_bit || total_tiles == 0) return false;
     const u32 passes = (end_bit - begin_bit + kRadixBits - 1) / kRadixBits;
-    SortSegments ss{seg_begin, seg_tiles, seg_count, total_tiles, c.sort_tile};
+    SortSegments ss{seg_begin, seg_tiles, seg_count, total_tiles, c.tune.sort_tile};
     const u64 elems = sort_elems;
     u32 needed[kMaxPasses];
     for (u32 p = 0; p < passes; ++p) needed[p] = 1;
@@ -398,8 +440,8 @@ struct Engine {
       if (!needed[p]) continue;
       zero(L.status, u64(total_tiles) * kRadixDigits * 8);
       zero(L.counters, 4);
-      const OnesweepVariant v = onesweep_variant(c.ballot_rank && elems >= c.ballot_min_elems,
-                                                 c.sort_block, c.sort_tile, vals != nullptr);
+      const OnesweepVariant v = onesweep_variant(c.tune.ballot_rank && elems >= c.tune.ballot_min_elems,
+                                                 c.tune.sort_block, c.tune.sort_tile, vals != nullptr);
       launch(name, elems * (vals ? 24 : 16), v.fn, total_tiles, v.block, v.smem,
              kin, vin, kout, vout, ss, begin_bit + p * kRadixBits, p, passes,
              L.digit_start, L.status, L.counters, L.flags);
@@ -414,7 +456,7 @@ struct Engine {
     std::vector<u32> tiles(b.size());
     tiles[0] = 0;
     for (size_t j = 0; j + 1 < b.size(); ++j) {
-      tiles[j + 1] = tiles[j] + static_cast<u32>((b[j + 1] - b[j] + c.sort_tile - 1) / c.sort_tile);
+      tiles[j + 1] = tiles[j] + static_cast<u32>((b[j + 1] - b[j] + c.tune.sort_tile - 1) / c.tune.sort_tile);
     }
     std::vector<u8> blob(b.size() * 12);
     std::memcpy(blob.data(), b.data(), b.size() * 8);
@@ -434,7 +476,7 @@ struct Engine {
   void plan_runs(u32 s) {
     runs_on = false;
     run_index = RunIndex{};
-    if (!allow_runs || !c.run_split || s < 8 || n < 2 * u64(s)) return;
+    if (!allow_runs || !c.tune.run_split || s < 8 || n < 2 * u64(s)) return;
     zero(L.scalars + 8, 16);
     launch("long_runs", n, long_runs_kernel,
            grid_stride_blocks((n + kRunChunk - 1) / kRunChunk, 256), 256, 0, L.text, n,
@@ -570,8 +612,8 @@ struct Engine {
     u32 symbols = 64 / bits;
     u64 longest = 1;
     for (u32 j = 0; j < segs; ++j) longest = std::max<u64>(longest, begin[j + 1] - begin[j]);
-    if (c.seed_symbols) {
-      symbols = std::min(symbols, c.seed_symbols);
+    if (c.tune.seed_symbols) {
+      symbols = std::min(symbols, c.tune.seed_symbols);
     } else {
       // Enough symbols that two seed keys of one instance rarely collide by
       // chance, log2(longest) / H + 2.5 with H the text's entropy in bits per
@@ -597,9 +639,9 @@ struct Engine {
     // local index rides in the low key bits and the sort moves keys only.
     const u32 index_bits = std::max<u32>(1, bits_for(longest - 1));
     u32 packed_shift = 0;
-    if (c.packed_max_bits && index_bits <= c.packed_max_bits) {
+    if (c.tune.packed_max_bits && index_bits <= c.tune.packed_max_bits) {
       u32 packed_symbols = (64 - index_bits) / bits;
-      if (c.seed_symbols) packed_symbols = std::min(packed_symbols, c.seed_symbols);
+      if (c.tune.seed_symbols) packed_symbols = std::min(packed_symbols, c.tune.seed_symbols);
       if (packed_symbols >= std::min<u32>(symbols, 12)) {
         packed_shift = index_bits;
         symbols = packed_symbols;
@@ -657,7 +699,7 @@ struct Engine {
     u64* grouped = pairs;
     if (pos_bits > kWindowBits) {
       const u64 b2[2] = {0, n};
-      const u32 t = static_cast<u32>((n + c.sort_tile - 1) / c.sort_tile);
+      const u32 t = static_cast<u32>((n + c.tune.sort_tile - 1) / c.tune.sort_tile);
       const u32 t2[2] = {0, t};
       sync();
       std::memcpy(c.host_small + 4096, b2, 16);
@@ -713,7 +755,7 @@ struct Engine {
            L.status, L.counters, L.scalars + 1, L.flags, inst_h ? RunIndex{} : run_index);
     // Dense ids are < active/2 (every group has two or more rows).
     const u32 id_bits = bits_for(active / 2 > 0 ? active / 2 - 1 : 0);
-    const u32 t = static_cast<u32>((active + c.sort_tile - 1) / c.sort_tile);
+    const u32 t = static_cast<u32>((active + c.tune.sort_tile - 1) / c.tune.sort_tile);
     const u64 b2[2] = {0, active};
     const u32 t2[2] = {0, t};
     std::memcpy(c.host_small + 4096, b2, 16);
@@ -725,7 +767,7 @@ struct Engine {
     // the round takes the global passes over (id, second) bits.
     bool sw = false;
     bool sorted = false;
-    if (c.seg_sort) {
+    if (c.tune.seg_sort) {
       zero(L.counters + 48, 4);
       launch("seg_sort", active * 24, seg_sort_kernel, (active + kSegWindow - 1) / kSegWindow,
              kSegBlock, sizeof(SegSortSmem), static_cast<const u64*>(L.k0),
@@ -817,7 +859,7 @@ struct Engine {
       launch("long_rows", 0, long_rows_kernel, u64(c.sm_count) * 8, 256, 0, L.text,
              static_cast<const LongRow*>(longs), static_cast<const u64*>(L.scalars + 5),
              long_cap, segments(), lcp, spos, sval);
-      const u32 t = static_cast<u32>((q + c.sort_tile - 1) / c.sort_tile);
+      const u32 t = static_cast<u32>((q + c.tune.sort_tile - 1) / c.tune.sort_tile);
       const u64 b2[2] = {0, q};
       const u32 t2[2] = {0, t};
       std::memcpy(c.host_small + 4096, b2, 16);
@@ -980,6 +1022,21 @@ void emit_outputs(Engine& e, const sufgpu_build_desc& d, sufgpu_outputs* outs,
   SG_CUDA(cudaEventRecord(c.ev[5], c.stream));
   e.sync();
 }
+
+// The knobs of one build: the context's, overridden by the first size class
+// that holds the build's longest instance; restored when the build ends.
+struct TuningScope {
+  sufgpu_ctx& c;
+  Tuning saved;
+  TuningScope(sufgpu_ctx& ctx, u64 longest) : c(ctx), saved(ctx.tune) {
+    for (const TuningClass& k : ctx.tuning_classes) {
+      if (longest > k.max_symbols) continue;
+      for (const auto& kv : k.settings) apply_tuning(ctx.tune, kv.first, kv.second);
+      break;
+    }
+  }
+  ~TuningScope() { c.tune = saved; }
+};
 
 // Shared build body for one or many instances (already concatenated in
 // L.text).  outs[j] receives instance j's planes.
@@ -1151,6 +1208,7 @@ sufgpu_status sufgpu_build(sufgpu_ctx* ctx, const uint8_t* text, uint64_t n,
   }
   try {
     SG_CUDA(cudaSetDevice(ctx->device));
+    TuningScope scope(*ctx, n);
     Engine e(*ctx);
     e.n = n;
     e.rank_rows = n;
@@ -1230,6 +1288,9 @@ extern "C" sufgpu_status sufgpu_build_batch(sufgpu_ctx* ctx, sufgpu_instance* in
   ctx->event_pool.reset();
   try {
     SG_CUDA(cudaSetDevice(ctx->device));
+    u64 longest = 0;
+    for (u32 j = 0; j < count; ++j) longest = std::max<u64>(longest, instances[j].n);
+    TuningScope scope(*ctx, longest);
     Engine e(*ctx);
     e.n = begin[count];
     e.rank_rows = e.n;
@@ -1289,32 +1350,33 @@ extern "C" sufgpu_status sufgpu_profile_entry(const sufgpu_ctx* ctx, uint32_t in
 
 extern "C" sufgpu_status sufgpu_set_tuning(sufgpu_ctx* ctx, const char* key, int64_t value) {
   if (!ctx || !key) return SUFGPU_INVALID_INPUT;
-  const std::string k(key);
-  if (k == "seed_symbols") {
-    if (value < 0 || value > 64) return fail(ctx, SUFGPU_INVALID_INPUT, "seed_symbols out of range");
-    ctx->seed_symbols = static_cast<u32>(value);
-  } else if (k == "ballot_rank") {
-    ctx->ballot_rank = value != 0;
-  } else if (k == "ballot_min_elems") {
-    if (value < 0) return fail(ctx, SUFGPU_INVALID_INPUT, "ballot_min_elems must be >= 0");
-    ctx->ballot_min_elems = static_cast<u64>(value);
-  } else if (k == "packed_max_bits") {
-    if (value < 0 || value > 32) return fail(ctx, SUFGPU_INVALID_INPUT, "packed_max_bits out of range");
-    ctx->packed_max_bits = static_cast<u32>(value);
-  } else if (k == "sort_tile") {
-    if (value != 2048 && value != 4096) return fail(ctx, SUFGPU_INVALID_INPUT, "sort_tile must be 2048 or 4096");
-    ctx->sort_tile = static_cast<u32>(value);
-  } else if (k == "seg_sort") {
-    ctx->seg_sort = value != 0;
-  } else if (k == "run_split") {
-    ctx->run_split = value != 0;
-  } else if (k == "sort_block") {
-    if (value != 256 && value != 512) return fail(ctx, SUFGPU_INVALID_INPUT, "sort_block must be 256 or 512");
-    ctx->sort_block = static_cast<u32>(value);
-  } else {
-    return fail(ctx, SUFGPU_INVALID_INPUT, "unknown tuning key " + k);
-  }
+  const std::string err = apply_tuning(ctx->tune, key, value);
+  if (!err.empty()) return fail(ctx, SUFGPU_INVALID_INPUT, err);
   return SUFGPU_OK;
+}
+
+extern "C" sufgpu_status sufgpu_set_tuning_class(sufgpu_ctx* ctx, uint64_t max_symbols,
+                                                 const char* key, int64_t value) {
+  if (!ctx || !key) return SUFGPU_INVALID_INPUT;
+  Tuning probe = ctx->tune;
+  const std::string err = apply_tuning(probe, key, value);
+  if (!err.empty()) return fail(ctx, SUFGPU_INVALID_INPUT, err);
+  auto& classes = ctx->tuning_classes;
+  auto it = std::find_if(classes.begin(), classes.end(),
+                         [&](const TuningClass& c) { return c.max_symbols == max_symbols; });
+  if (it == classes.end()) {
+    classes.push_back(TuningClass{max_symbols, {}});
+    std::sort(classes.begin(), classes.end(),
+              [](const TuningClass& a, const TuningClass& b) { return a.max_symbols < b.max_symbols; });
+    it = std::find_if(classes.begin(), classes.end(),
+                      [&](const TuningClass& c) { return c.max_symbols == max_symbols; });
+  }
+  it->settings.emplace_back(key, value);
+  return SUFGPU_OK;
+}
+
+extern "C" void sufgpu_clear_tuning_classes(sufgpu_ctx* ctx) {
+  if (ctx) ctx->tuning_classes.clear();
 }
 
 // ===========================================================================
