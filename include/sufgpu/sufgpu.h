@@ -194,7 +194,11 @@ SUFGPU_API sufgpu_status sufgpu_profile_entry(const sufgpu_ctx *ctx, uint32_t in
  *                   ordered directly after the seed, 0 = by the rounds;
  *   "seg_sort"      1 = each round sorts its groups inside shared memory
  *                   (global passes only when a group exceeds a block), 0 =
- *                   every round takes the global passes.
+ *                   every round takes the global passes;
+ *   "graph_rounds"  1 = a layout built before runs its rounds as a cached
+ *                   CUDA graph of two rounds (one host synchronization per
+ *                   pair), 0 = the host drives every round.  Builds with the
+ *                   per-kernel profile on are always host-driven.
  * Results are identical for every setting; only speed changes. */
 SUFGPU_API sufgpu_status sufgpu_set_tuning(sufgpu_ctx *ctx, const char *key, int64_t value);
 

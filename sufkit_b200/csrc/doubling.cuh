@@ -348,13 +348,32 @@ __device__ __forceinline__ u64 run_jump(const RunIndex& ri, u64 p, u64 h) {
   return (p < e && e - p >= h) ? e : 0;
 }
 
+// Device-side round state, so that a sequence of rounds can run without the
+// host (and be captured in a CUDA graph): the active count of the round (read
+// by its kernels, which are launched for an upper bound and skip the rest),
+// the prefix length h, and an abort word that a round sets when its groups
+// need the host (the kernels after it then do nothing).
+struct RoundState {
+  const u64* count;  // active rows of this round
+  u64* next_count;   // written by round_rank
+  u64* h;            // prefix length; doubled by round_rank when double_h
+  const u64* abort;  // nonzero: skip (null: never)
+  u64* totals;       // [0] += active rows, [1] += rounds (null: not kept)
+  u32 double_h;
+};
+
+__device__ __forceinline__ bool round_skipped(const RoundState& rs) {
+  return rs.abort && *rs.abort;
+}
+
 // Round step 1: composite keys for the active list.  counters: *group_count
 // receives the number of groups G.  ghead/gstart are indexed by dense id.
 // inst_h, when set, holds each segment's own prefix length h (the served
-// engine advances references admitted at different times side by side).
+// engine advances references admitted at different times side by side);
+// otherwise *rs.h is the round's prefix length.
 static __global__ void __launch_bounds__(kScanBlock)
-round_keys_kernel(const u32* __restrict__ active, u64 count,
-                  const u32* __restrict__ rank, u64 h, const u64* __restrict__ inst_h,
+round_keys_kernel(const u32* __restrict__ active, RoundState rs,
+                  const u32* __restrict__ rank, const u64* __restrict__ inst_h,
                   Segments segs,
                   u32 second_bits, u64* __restrict__ ckey,
                   u32* __restrict__ cval, u32* __restrict__ ghead,
@@ -364,7 +383,13 @@ round_keys_kernel(const u32* __restrict__ active, u64 count,
   __shared__ u64 warp_smem[kScanBlock / 32];
   __shared__ u64 tile_prefix;
   __shared__ u32 tile_slot;
+  if (round_skipped(rs)) return;
+  const u64 count = *rs.count;
+  const u64 h = inst_h ? 0 : *rs.h;
   const u32 tile = claim_tile(tile_counter, &tile_slot);
+  // Launched for an upper bound: tiles past the count (after every real
+  // tile, so no look-back waits on them) leave at once.
+  if (static_cast<u64>(tile) * kScanTile >= count) return;
   const u64 a0 = static_cast<u64>(tile) * kScanTile + threadIdx.x * kScanItems;
 
   u32 pos[kScanItems];
@@ -431,16 +456,23 @@ round_keys_kernel(const u32* __restrict__ active, u64 count,
 // and the next active list.
 static __global__ void __launch_bounds__(kScanBlock)
 round_rank_kernel(const u64* __restrict__ ckey, const u32* __restrict__ cval,
-                  u64 count, u32 second_bits, const u32* __restrict__ ghead,
+                  RoundState rs, u32 second_bits, const u32* __restrict__ ghead,
                   const u32* __restrict__ gstart, u64 group_cap, u64 rows,
                   u32* __restrict__ sa,
                   u32* __restrict__ rank, u32* __restrict__ next_active,
                   u64* status_max, u64* status_sum, u32* tile_counter,
-                  u64* next_count, DeviceFlags* flags) {
+                  DeviceFlags* flags) {
   __shared__ u64 warp_smem[kScanBlock / 32];
   __shared__ u64 tile_prefix[2];
   __shared__ u32 tile_slot;
+  if (round_skipped(rs)) return;
+  const u64 count = *rs.count;
+  if (count == 0) {  // converged: the next round has nothing either
+    if (blockIdx.x == 0 && threadIdx.x == 0) *rs.next_count = 0;
+    return;
+  }
   const u32 tile = claim_tile(tile_counter, &tile_slot);
+  if (static_cast<u64>(tile) * kScanTile >= count) return;
   const u64 a0 = static_cast<u64>(tile) * kScanTile + threadIdx.x * kScanItems;
 
   u64 k[kScanItems + 2];
@@ -503,7 +535,14 @@ round_rank_kernel(const u64* __restrict__ ckey, const u32* __restrict__ cval,
     }
   }
   const u64 tiles = (count + kScanTile - 1) / kScanTile;
-  if (tile == tiles - 1 && threadIdx.x == 0) *next_count = tile_prefix[1] + agg_sum;
+  if (tile == tiles - 1 && threadIdx.x == 0) {
+    *rs.next_count = tile_prefix[1] + agg_sum;
+    if (rs.double_h) *rs.h *= 2;
+    if (rs.totals) {
+      rs.totals[0] += count;
+      rs.totals[1] += 1;
+    }
+  }
 }
 
 }  // namespace sufgpu

@@ -220,6 +220,9 @@ struct Tuning {
   bool run_split = true;
   // Sort each round's groups in shared memory (segsort.cuh).
   bool seg_sort = true;
+  // Run the rounds as captured CUDA graphs of two rounds (needs seg_sort;
+  // builds with the per-kernel profile on are driven round by round).
+  bool graph_rounds = true;
   // Onesweep block size (256 threads x 16 keys or 512 x 8).
   u32 sort_block = 256;
   // Keys per onesweep tile (2048 or 4096).
@@ -250,6 +253,8 @@ std::string apply_tuning(Tuning& t, const std::string& k, int64_t value) {
     t.sort_tile = static_cast<u32>(value);
   } else if (k == "seg_sort") {
     t.seg_sort = value != 0;
+  } else if (k == "graph_rounds") {
+    t.graph_rounds = value != 0;
   } else if (k == "run_split") {
     t.run_split = value != 0;
   } else if (k == "sort_block") {
@@ -314,6 +319,21 @@ struct sufgpu_ctx {
   // (sufgpu_set_tuning_class, written by the autotuner).
   Tuning tune;
   std::vector<TuningClass> tuning_classes;
+  // Instantiated round-pair graphs, reused by later builds with the same
+  // layout (most recent last; the oldest is dropped beyond a few).
+  struct CachedGraph {
+    std::vector<u64> key;
+    cudaGraphExec_t exec;
+    u32 kernels;
+  };
+  std::vector<CachedGraph> round_graphs;
+  // Layouts of recent builds: a layout's rounds are captured from its second
+  // build on, so one-off builds never pay for a capture.
+  std::vector<std::vector<u64>> seen_layouts;
+  void drop_round_graphs() {
+    for (auto& g : round_graphs) cudaGraphExecDestroy(g.exec);
+    round_graphs.clear();
+  }
 };
 
 namespace {
@@ -737,43 +757,98 @@ struct Engine {
   }
 
 
-  // ---- One doubling round over the active list act[0, active): prefix h
-  // (or per-segment lengths inst_h with the segment table `segs`).  The next
-  // active list replaces act (act/other swap roles as needed).  Returns the
-  // next active count.
-  u64 round_step(u32*& act, u32*& other, u64 active, u64 h, const u64* inst_h,
-                 Segments segs) {
-    const u32 second_bits = bits_for(n);
-    st.active_rows += active;
-    const u64 tiles = (active + kScanTile - 1) / kScanTile;
-    u32* ghead = L.y;
-    u32* gstart = L.y + (n - n / 2);  // G <= active/2 <= n/2 entries each
+  // ---- Doubling rounds.  Device round state lives in L.scalars:
+  // [16]/[17] the active count read / written by a round (they alternate),
+  // [18] h, [19] abort (a round whose groups need the host), [20]/[21]
+  // totals (active rows, rounds).  The kernels read the count there and are
+  // launched for an upper bound, so rounds can run without the host.
+  static constexpr int kCountA = 16, kCountB = 17, kH = 18, kAbort = 19, kTotals = 20;
+
+  u32* ghead() const { return L.y; }
+  u32* gstart() const { return L.y + (n - n / 2); }  // G <= active/2 <= n/2 each
+
+  RoundState round_state(int in, bool graph) {
+    return RoundState{L.scalars + in, L.scalars + (in == kCountA ? kCountB : kCountA),
+                      L.scalars + kH, graph ? L.scalars + kAbort : nullptr,
+                      L.scalars + kTotals, 1u};
+  }
+
+  // Round step 1 (composite keys) for up to `bound` active rows.
+  void round_keys(const u32* act, u32* other, const RoundState& rs, u64 bound,
+                  const u64* inst_h, Segments segs) {
+    const u64 tiles = (bound + kScanTile - 1) / kScanTile;
     zero(L.status, (tiles + 1) * 8);
     zero(L.counters, 4);
-    launch("round_keys", active * 28, round_keys_kernel, tiles, kScanBlock, 0, act, active,
-           L.rank, h, inst_h, segs, second_bits, L.k0, other, ghead, gstart, u64(n / 2),
-           L.status, L.counters, L.scalars + 1, L.flags, inst_h ? RunIndex{} : run_index);
-    // Dense ids are < active/2 (every group has two or more rows).
+    launch("round_keys", bound * 28, round_keys_kernel, tiles, kScanBlock, 0, act, rs,
+           static_cast<const u32*>(L.rank), inst_h, segs, bits_for(n), L.k0, other, ghead(),
+           gstart(), u64(n / 2), L.status, L.counters, L.scalars + 1, L.flags,
+           inst_h ? RunIndex{} : run_index);
+  }
+
+  // Shared-memory group sort: (k0, other) -> (k1, act).  abort: the device
+  // abort word (graph rounds) or null.
+  void round_seg_sort(const u32* other, u32* act, const RoundState& rs, u64 bound, u64* abort,
+                      u64 tag) {
+    zero(L.counters + 48, 4);
+    launch("seg_sort", bound * 24, seg_sort_kernel, (bound + kSegWindow - 1) / kSegWindow,
+           kSegBlock, sizeof(SegSortSmem), static_cast<const u64*>(L.k0), other, rs.count,
+           static_cast<const u32*>(gstart()), static_cast<const u64*>(L.scalars + 1),
+           bits_for(n), L.k1, act, L.counters + 48, abort, tag, L.flags);
+  }
+
+  // Global passes over (id, second) bits for `active` rows: (k0, other) ->
+  // (k1, act) or back in place; returns true when the result is in (k1, act).
+  bool round_global_sort(u32* act, u32* other, u64 active) {
     const u32 id_bits = bits_for(active / 2 > 0 ? active / 2 - 1 : 0);
     const u32 t = static_cast<u32>((active + c.tune.sort_tile - 1) / c.tune.sort_tile);
     const u64 b2[2] = {0, active};
     const u32 t2[2] = {0, t};
+    sync();
     std::memcpy(c.host_small + 4096, b2, 16);
     std::memcpy(c.host_small + 4096 + 16, t2, 8);
     SG_CUDA(cudaMemcpyAsync(L.sort_begin, c.host_small + 4096, 16, cudaMemcpyHostToDevice, c.stream));
     SG_CUDA(cudaMemcpyAsync(L.sort_tiles, c.host_small + 4096 + 16, 8, cudaMemcpyHostToDevice, c.stream));
+    return radix_sort("round_onesweep", L.k0, other, L.k1, act, L.sort_begin, L.sort_tiles, 1, t,
+                      active, 0, bits_for(n) + id_bits, false);
+  }
+
+  // Round step 2 (ranks, SA rows, next active list) from (ck, cv) into next.
+  void round_rank(const u64* ck, const u32* cv, u32* next, const RoundState& rs, u64 bound) {
+    const u64 tiles = (bound + kScanTile - 1) / kScanTile;
+    zero(L.status, 2 * (tiles + 1) * 8);
+    zero(L.counters, 4);
+    launch("round_rank", bound * 32, round_rank_kernel, tiles, kScanBlock, 0, ck, cv, rs,
+           bits_for(n), static_cast<const u32*>(ghead()), static_cast<const u32*>(gstart()),
+           u64(n / 2), rank_rows, sa, L.rank, next, L.status, L.status + tiles + 1, L.counters,
+           L.flags);
+  }
+
+  void put_scalar(int slot, u64 value) {
+    c.host_scalars[40 + slot - kCountA] = value;
+    SG_CUDA(cudaMemcpyAsync(L.scalars + slot, c.host_scalars + 40 + slot - kCountA, 8,
+                            cudaMemcpyHostToDevice, c.stream));
+  }
+
+  // ---- One doubling round over the active list act[0, active), driven by
+  // the host: prefix h (or per-segment lengths inst_h with the segment table
+  // `segs`).  The next active list replaces act (act/other swap roles as
+  // needed).  Returns the next active count.
+  u64 round_step(u32*& act, u32*& other, u64 active, u64 h, const u64* inst_h,
+                 Segments segs) {
+    st.active_rows += active;
+    put_scalar(kCountA, active);
+    put_scalar(kH, h);
+    RoundState rs = round_state(kCountA, false);
+    rs.totals = nullptr;
+    rs.double_h = 0;
+    round_keys(act, other, rs, active, inst_h, segs);
     // Rows only move inside their groups: sort whole groups in shared memory
     // (segsort.cuh) unless some group is too large for a block, in which case
     // the round takes the global passes over (id, second) bits.
     bool sw = false;
     bool sorted = false;
     if (c.tune.seg_sort) {
-      zero(L.counters + 48, 4);
-      launch("seg_sort", active * 24, seg_sort_kernel, (active + kSegWindow - 1) / kSegWindow,
-             kSegBlock, sizeof(SegSortSmem), static_cast<const u64*>(L.k0),
-             static_cast<const u32*>(other), active, static_cast<const u32*>(gstart),
-             static_cast<const u64*>(L.scalars + 1), second_bits, L.k1, act, L.counters + 48,
-             L.flags);
+      round_seg_sort(other, act, rs, active, nullptr, 0);
       SG_CUDA(cudaMemcpyAsync(c.host_small + 8192, L.counters + 48, 4, cudaMemcpyDeviceToHost,
                               c.stream));
       sync();
@@ -786,22 +861,136 @@ struct Engine {
         ++st.seg_sort_fallbacks;
       }
     }
-    if (!sorted) {
-      sw = radix_sort("round_onesweep", L.k0, other, L.k1, act, L.sort_begin, L.sort_tiles, 1, t,
-                      active, 0, second_bits + id_bits, false);
-    }
+    if (!sorted) sw = round_global_sort(act, other, active);
     u64* ck = sw ? L.k1 : L.k0;
     u32* cv = sw ? act : other;
     u32* next = sw ? other : act;
-    zero(L.status, 2 * (tiles + 1) * 8);
-    zero(L.counters, 4);
-    launch("round_rank", active * 32, round_rank_kernel, tiles, kScanBlock, 0, ck, cv, active,
-           second_bits, ghead, gstart, u64(n / 2), rank_rows, sa, L.rank, next, L.status,
-           L.status + tiles + 1, L.counters, L.scalars + 2, L.flags);
-    const u64 next_count = read_scalar(2);  // synchronizes: host_small may be reused
+    round_rank(ck, cv, next, rs, active);
+    const u64 next_count = read_scalar(kCountB);  // synchronizes: host_small may be reused
     other = sw ? act : other;
     act = next;
     return next_count;
+  }
+
+  // ---- Host-free rounds: two rounds (their buffers swap roles twice, so the
+  // pair returns to its starting roles) captured once as a CUDA graph for an
+  // upper bound on the active count and launched until the count reaches
+  // zero, one synchronization per pair.  A round whose groups do not fit the
+  // shared-memory sort stops the pair (abort); the host finishes that round
+  // with the global passes and the graph continues from there.
+  // The graph of a round pair for `bound` active rows with these buffers:
+  // from the context's cache when an earlier build had the same layout,
+  // else captured and cached.
+  const sufgpu_ctx::CachedGraph& round_graph(u32* act, u32* other, u64 bound) {
+    const std::vector<u64> key = {reinterpret_cast<u64>(c.arena.base), n, segs, bound,
+                                  reinterpret_cast<u64>(act), reinterpret_cast<u64>(other),
+                                  run_count, reinterpret_cast<u64>(L.seg_begin)};
+    auto& cache = c.round_graphs;
+    for (size_t i = 0; i < cache.size(); ++i) {
+      if (cache[i].key == key) {
+        std::rotate(cache.begin() + i, cache.begin() + i + 1, cache.end());
+        return cache.back();
+      }
+    }
+    const u32 before = c.launches;
+    SG_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+    cudaGraph_t graph = nullptr;
+    try {
+      for (int r = 0; r < 2; ++r) {
+        const RoundState rs = round_state(r == 0 ? kCountA : kCountB, true);
+        round_keys(act, other, rs, bound, nullptr, segments());
+        round_seg_sort(other, act, rs, bound, L.scalars + kAbort, r + 1);
+        round_rank(L.k1, act, other, rs, bound);
+        std::swap(act, other);
+      }
+    } catch (...) {
+      cudaStreamEndCapture(c.stream, &graph);
+      if (graph) cudaGraphDestroy(graph);
+      c.launches = before;
+      throw;
+    }
+    SG_CUDA(cudaStreamEndCapture(c.stream, &graph));
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t err = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    SG_CUDA(err);
+    const u32 kernels = c.launches - before;
+    c.launches = before;
+    if (cache.size() >= 8) {
+      cudaGraphExecDestroy(cache.front().exec);
+      cache.erase(cache.begin());
+    }
+    cache.push_back(sufgpu_ctx::CachedGraph{key, exec, kernels});
+    return cache.back();
+  }
+
+  void graph_rounds(u32*& act, u32*& other, u64 active, u64 h) {
+    put_scalar(kCountA, active);
+    put_scalar(kH, h);
+    zero(L.scalars + kAbort, 24);  // abort and the two totals
+    // Bounds are powers of two, so builds of similar sizes share graphs.
+    auto pow2 = [](u64 v) { return u64(1) << bits_for(v > 1 ? v - 1 : 1); };
+    u64 bound = pow2(active);
+    u64 fallback_rows = 0, fallback_rounds = 0;
+    for (u32 pairs = 0;; ++pairs) {
+      if (pairs > 64) throw BuildError{SUFGPU_BUILD_FAILURE, "prefix doubling did not converge"};
+      const sufgpu_ctx::CachedGraph& g = round_graph(act, other, std::min<u64>(bound, n));
+      SG_CUDA(cudaGraphLaunch(g.exec, c.stream));
+      c.launches += g.kernels;
+      SG_CUDA(cudaMemcpyAsync(c.host_scalars + kCountA, L.scalars + kCountA, 32,
+                              cudaMemcpyDeviceToHost, c.stream));
+      sync();
+      const u64 abort = c.host_scalars[kAbort];
+      if (abort) {
+        // Round abort-1 of the pair stopped after its keys; rounds before it
+        // are complete.  Its active count is in A (first round) or B.
+        ++st.seg_sort_fallbacks;
+        const int in = abort == 1 ? kCountA : kCountB;
+        if (abort == 2) std::swap(act, other);
+        const u64 count = c.host_scalars[in];
+        fallback_rows += count;
+        ++fallback_rounds;
+        const bool sw = round_global_sort(act, other, count);
+        RoundState rs = round_state(in, false);
+        rs.totals = nullptr;
+        u64* ck = sw ? L.k1 : L.k0;
+        u32* cv = sw ? act : other;
+        u32* next = sw ? other : act;
+        round_rank(ck, cv, next, rs, count);
+        other = sw ? act : other;
+        act = next;
+        // Continue from a clean state: the next count in A, abort cleared.
+        const u64 next_count = read_scalar(in == kCountA ? kCountB : kCountA);
+        put_scalar(kCountA, next_count);
+        zero(L.scalars + kAbort, 8);
+        if (next_count == 0) break;
+        bound = std::min(bound, pow2(next_count));
+        continue;
+      }
+      const u64 count = c.host_scalars[kCountA];
+      if (count == 0) break;
+      // A much smaller count than the graph's bound wastes empty blocks:
+      // switch to the graph of a smaller bound.
+      if (count < bound / 4) bound = pow2(count);
+    }
+    SG_CUDA(cudaMemcpyAsync(c.host_scalars + kTotals, L.scalars + kTotals, 16,
+                            cudaMemcpyDeviceToHost, c.stream));
+    sync();
+    st.active_rows += c.host_scalars[kTotals] + fallback_rows;
+    st.rounds = static_cast<u32>(c.host_scalars[kTotals + 1] + fallback_rounds);
+  }
+
+  // True when a recent build had this build's layout (and remembers it).
+  bool layout_seen() {
+    const std::vector<u64> key = {reinterpret_cast<u64>(c.arena.base), n, segs, run_count,
+                                  reinterpret_cast<u64>(spare)};
+    auto& seen = c.seen_layouts;
+    for (size_t i = 0; i < seen.size(); ++i) {
+      if (seen[i] == key) return true;
+    }
+    if (seen.size() >= 16) seen.erase(seen.begin());
+    seen.push_back(key);
+    return false;
   }
 
   // ---- The doubling sort: leaves SA in `sa` and ISA (global rows) in rank.
@@ -813,6 +1002,10 @@ struct Engine {
     u32* act = L.x;
     u32* other = spare;
     u64 h = seed_length;
+    if (active > 0 && c.tune.graph_rounds && c.tune.seg_sort && !c.profiling && layout_seen()) {
+      graph_rounds(act, other, active, h);
+      return;
+    }
     u32 rounds = 0;
     while (active > 0) {
       if (++rounds > 64) throw BuildError{SUFGPU_BUILD_FAILURE, "prefix doubling did not converge"};
@@ -1100,6 +1293,7 @@ void sufgpu_destroy(sufgpu_ctx* ctx) {
   for (auto& ev : ctx->ev) {
     if (ev) cudaEventDestroy(ev);
   }
+  ctx->drop_round_graphs();
   if (ctx->host_scalars) cudaFreeHost(ctx->host_scalars);
   if (ctx->host_small) cudaFreeHost(ctx->host_small);
   if (ctx->arena.base) {

@@ -47,16 +47,23 @@ __device__ __forceinline__ u64 first_group_at(const u32* gstart, u64 groups, u64
 // the first row of group g and *group_count the number of groups.  Writes the
 // sorted keys and values of every window that fits (all of them unless
 // *big > 0 afterwards).
+// count_ptr: the round's active rows (the grid covers an upper bound).  With
+// abort set, a window too large for a block also writes abort_tag there so
+// that the rest of a host-free round sequence stands still.
 static __global__ void __launch_bounds__(kSegBlock, 2)
-seg_sort_kernel(const u64* __restrict__ ckey, const u32* __restrict__ cval, u64 count,
+seg_sort_kernel(const u64* __restrict__ ckey, const u32* __restrict__ cval,
+                const u64* __restrict__ count_ptr,
                 const u32* __restrict__ gstart, const u64* __restrict__ group_count,
                 u32 second_bits, u64* __restrict__ out_keys, u32* __restrict__ out_vals,
-                u32* big, DeviceFlags* flags) {
+                u32* big, u64* abort, u64 abort_tag, DeviceFlags* flags) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SegSortSmem& sm = *reinterpret_cast<SegSortSmem*>(smem_raw);
   constexpr int kWarps = kSegBlock / 32;
   const u32 lane = threadIdx.x & 31;
   const u32 warp = threadIdx.x >> 5;
+  if (abort && *abort) return;
+  const u64 count = *count_ptr;
+  if (static_cast<u64>(blockIdx.x) * kSegWindow >= count) return;
   if (threadIdx.x == 0) {
     const u64 groups = *group_count;
     const u64 w0 = static_cast<u64>(blockIdx.x) * kSegWindow;
@@ -80,7 +87,10 @@ seg_sort_kernel(const u64* __restrict__ ckey, const u32* __restrict__ cval, u64 
   const u32 n_groups = sm.range[3];
   if (n_rows == 0) return;
   if (n_rows > static_cast<u32>(kSegCap)) {
-    if (threadIdx.x == 0) atomicAdd(big, 1u);
+    if (threadIdx.x == 0) {
+      atomicAdd(big, 1u);
+      if (abort) *abort = abort_tag;
+    }
     return;
   }
   // Tile-local composite keys: (local group << second_bits) | second.

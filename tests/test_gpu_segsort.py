@@ -63,3 +63,31 @@ def test_groups_of_every_size_up_to_a_block(ctx):
     r = build(ctx, t)
     sa, isa, lcp = expected(t)
     assert (r.sa_low == sa).all() and (r.isa_low == isa).all() and (r.lcp == lcp).all()
+
+
+@pytest.mark.parametrize("kind", ["repeats", "tandem"])
+def test_graph_rounds_equal_host_rounds(ctx, kind):
+    """Repeated builds of one layout replay captured round graphs (from the
+    second build on); a round with a group beyond a block stops the graph and
+    is finished by the host.  Every build equals the host-driven one."""
+    if kind == "repeats":
+        t = synth.repeat_rich_100mbp(scale=0.01).logical_text()
+    else:
+        rng = np.random.default_rng(3)
+        unit = rng.integers(2, 6, size=3).astype(np.uint8)
+        t = np.concatenate([rng.integers(2, 6, size=3000).astype(np.uint8),
+                            np.tile(unit, 40_000), np.array([1, 0], np.uint8)])
+    ctx.set_tuning("graph_rounds", 0)
+    try:
+        host = ctx.build(t, sa_bits=32, isa_bits=32, lcp=sg.LcpEncoding.RAW32, validate=True)
+    finally:
+        ctx.set_tuning("graph_rounds", 1)
+    for _ in range(3):
+        r = ctx.build(t, sa_bits=32, isa_bits=32, lcp=sg.LcpEncoding.RAW32, validate=True)
+        assert (r.sa_low == host.sa_low).all() and (r.isa_low == host.isa_low).all()
+        assert (r.lcp == host.lcp).all()
+        assert r.stats["rounds"] == host.stats["rounds"]
+        assert r.stats["active_rows"] == host.stats["active_rows"]
+        assert r.stats["seg_sort_fallbacks"] == host.stats["seg_sort_fallbacks"]
+    if kind == "tandem":
+        assert host.stats["seg_sort_fallbacks"] > 0
