@@ -63,6 +63,12 @@ typedef struct sufgpu_build_desc {
   uint32_t isa_storage_bits; /* 0 = no ISA output, else 32, 40, 48 or 64 */
   uint32_t lcp_encoding;     /* sufgpu_lcp_encoding */
   uint32_t flags;            /* SUFGPU_FLAG_* */
+  /* 0 or 1 = complete arrays.  K > 1 keeps the suffixes at positions that are
+   * multiples of K, as BuildDivsufsort's sampling_rate does
+   * (src/divsufsort_backend.cpp:62-150): every plane then has ceil(n / K)
+   * rows per instance, ISA[p / K] = sampled row, LCP = lcp of consecutive
+   * sampled rows (raw LCP only). */
+  uint32_t sampling_rate;
 } sufgpu_build_desc;
 
 /* Caller-owned output planes of one instance (n rows each).  Each pointer may

@@ -68,6 +68,9 @@ def ref() -> Optional[ctypes.CDLL]:
         lib.sufref_last_error.restype = ctypes.c_char_p
         lib.sufref_divsufsort64.argtypes = [P, P, ctypes.c_int64]
         lib.sufref_divsufsort32.argtypes = [P, P, ctypes.c_int32]
+        lib.sufref_adapter_build_sampled.argtypes = [ctypes.c_int, P, U64, ctypes.c_uint32,
+                                                     ctypes.c_int, ctypes.c_int, ctypes.c_uint32,
+                                                     P, P, P, P]
         lib.sufref_adapter_build.argtypes = [ctypes.c_int, P, U64, ctypes.c_int, ctypes.c_int,
                                              ctypes.c_uint32, P, P, P, P]
         lib.sufref_pack.argtypes = [P, U64, U64, ctypes.c_int, P, P, P, P]
@@ -188,6 +191,41 @@ def ref_adapter(text: np.ndarray, width: int = 64, threads: int = 1):
     _check(lib, lib.sufref_adapter_build(width, _p(t), t.size, 1, 1, threads, _p(sa), _p(isa),
                                          _p(lcp), sec))
     return sa, isa, lcp, list(sec)
+
+
+def ref_adapter_sampled(text: np.ndarray, rate: int, width: int = 64, threads: int = 1):
+    """detail::BuildDivsufsort{width} with sampling rate K: (sa, isa, lcp) of
+    the ceil(n / K) sampled rows."""
+    lib = ref()
+    t = np.ascontiguousarray(text, np.uint8)
+    cap = max(1, (t.size + rate - 1) // rate)
+    sa = np.empty(cap, np.uint64)
+    isa = np.empty(cap, np.uint64)
+    lcp = np.empty(cap, np.uint64)
+    rows = ctypes.c_uint64()
+    _check(lib, lib.sufref_adapter_build_sampled(width, _p(t), t.size, rate, 1, 1, threads,
+                                                 _p(sa), _p(isa), _p(lcp), ctypes.byref(rows)))
+    k = rows.value
+    return sa[:k].copy(), isa[:k].copy(), lcp[:k].copy()
+
+
+def sample(sa: np.ndarray, lcp: np.ndarray, rate: int):
+    """Restatement of the sampling of src/divsufsort_backend.cpp:62-150 from a
+    complete (sa, lcp): keep rows with sa % K == 0; ISA[p / K] = sampled row;
+    LCP of consecutive sampled rows = min of the complete LCP over the rows
+    after the previous sampled row up to this one (0 for the first)."""
+    sa = np.asarray(sa, np.int64)
+    lcp = np.asarray(lcp, np.int64)
+    rows = np.flatnonzero(sa % rate == 0)
+    sa_k = sa[rows]
+    isa_k = np.empty(sa_k.size, np.int64)
+    isa_k[sa_k // rate] = np.arange(sa_k.size)
+    lcp_k = np.zeros(sa_k.size, np.int64)
+    if rows.size > 1:
+        # Segment j >= 1 is rows[j-1]+1 .. rows[j]: [starts[j-1], starts[j]).
+        starts = rows + 1
+        lcp_k[1:] = np.minimum.reduceat(np.append(lcp, 0), starts)[: rows.size - 1]
+    return sa_k, isa_k, lcp_k
 
 
 def ref_divsufsort64(text: np.ndarray) -> np.ndarray:

@@ -182,6 +182,39 @@ int sufref_adapter_build(int width, const uint8_t* text, uint64_t n,
   }
 }
 
+// detail::BuildDivsufsort32/64 with sampling rate K: *rows_out receives the
+// number of sampled rows written to sa_out/isa_out/lcp_out (ceil(n / K)).
+int sufref_adapter_build_sampled(int width, const uint8_t* text, uint64_t n, uint32_t rate,
+                                 int retain_lcp, int retain_isa, uint32_t threads,
+                                 uint64_t* sa_out, uint64_t* isa_out, uint64_t* lcp_out,
+                                 uint64_t* rows_out) {
+  try {
+    std::vector<std::uint8_t> input(text, text + n);
+    auto run = [&](auto built) {
+      *rows_out = built.suffix_array.size();
+      for (std::size_t i = 0; i < built.suffix_array.size(); ++i) {
+        sa_out[i] = static_cast<uint64_t>(built.suffix_array[i]);
+      }
+      if (isa_out != nullptr && !built.isa.empty()) {
+        std::copy(built.isa.begin(), built.isa.end(), isa_out);
+      }
+      if (lcp_out != nullptr && !built.lcp.empty()) {
+        std::copy(built.lcp.begin(), built.lcp.end(), lcp_out);
+      }
+    };
+    if (width == 32) {
+      run(sufkit::detail::BuildDivsufsort32(input, rate, retain_lcp != 0, retain_isa != 0,
+                                            threads));
+    } else {
+      run(sufkit::detail::BuildDivsufsort64(input, rate, retain_lcp != 0, retain_isa != 0,
+                                            threads));
+    }
+    return 0;
+  } catch (const std::exception& error) {
+    return Fail(error);
+  }
+}
+
 // CoordinateStorage::FromUInt64 (the validating packer used by
 // RepackSuffixArray and BuildIsa).  Writes the planes of the resolved width;
 // *width_out receives that width in bits.

@@ -63,7 +63,8 @@ class _Desc(ctypes.Structure):
     _fields_ = [("sa_storage_bits", ctypes.c_uint32),
                 ("isa_storage_bits", ctypes.c_uint32),
                 ("lcp_encoding", ctypes.c_uint32),
-                ("flags", ctypes.c_uint32)]
+                ("flags", ctypes.c_uint32),
+                ("sampling_rate", ctypes.c_uint32)]
 
 
 class _Outputs(ctypes.Structure):
@@ -343,14 +344,18 @@ class Context:
         return pos, val
 
     def build(self, text, sa_bits: int = 32, isa_bits: int = 32,
-              lcp: LcpEncoding = LcpEncoding.RAW32, validate: bool = False) -> BuildResult:
+              lcp: LcpEncoding = LcpEncoding.RAW32, validate: bool = False,
+              sampling_rate: int = 1) -> BuildResult:
         """One complete build of ``text`` (the logical text including its
-        sentinel).  Returns host planes; see include/sufgpu/sufgpu.h."""
+        sentinel).  Returns host planes; see include/sufgpu/sufgpu.h.  With
+        sampling_rate K > 1 the planes hold the ceil(n / K) suffixes at
+        positions that are multiples of K."""
         t = _as_text(text)
         n = int(t.size)
         lcp = LcpEncoding(lcp)
-        planes = self._alloc_outputs(n, sa_bits, isa_bits, lcp)
-        desc = _Desc(sa_bits, isa_bits, int(lcp), FLAG_VALIDATE if validate else 0)
+        planes = self._alloc_outputs(_rows(n, sampling_rate), sa_bits, isa_bits, lcp)
+        desc = _Desc(sa_bits, isa_bits, int(lcp), FLAG_VALIDATE if validate else 0,
+                     int(sampling_rate))
         out = self._outputs(planes)
         anchors = _Anchors()
         stats = _Stats()
@@ -366,17 +371,19 @@ class Context:
 
     def build_batch(self, texts: Sequence, sa_bits: int = 32, isa_bits: int = 0,
                     lcp: LcpEncoding = LcpEncoding.RAW32,
-                    validate: bool = False) -> list[BuildResult]:
+                    validate: bool = False, sampling_rate: int = 1) -> list[BuildResult]:
         """Builds many independent references with the same launches."""
         ts = [_as_text(t) for t in texts]
         lcp = LcpEncoding(lcp)
-        all_planes = [self._alloc_outputs(int(t.size), sa_bits, isa_bits, lcp) for t in ts]
+        all_planes = [self._alloc_outputs(_rows(int(t.size), sampling_rate), sa_bits, isa_bits,
+                                          lcp) for t in ts]
         arr = (_Instance * len(ts))()
         for j, (t, planes) in enumerate(zip(ts, all_planes)):
             arr[j].text = _ptr(t)
             arr[j].n = int(t.size)
             arr[j].out = self._outputs(planes)
-        desc = _Desc(sa_bits, isa_bits, int(lcp), FLAG_VALIDATE if validate else 0)
+        desc = _Desc(sa_bits, isa_bits, int(lcp), FLAG_VALIDATE if validate else 0,
+                     int(sampling_rate))
         stats = _Stats()
         status = self._lib.sufgpu_build_batch(self._h, arr, len(ts), ctypes.byref(desc),
                                               ctypes.byref(stats))
@@ -559,14 +566,19 @@ def default_context() -> Context:
     return _default_ctx
 
 
+def _rows(n: int, sampling_rate: int) -> int:
+    """Rows of a plane: n, or ceil(n / K) for sampling rate K > 1."""
+    return n if sampling_rate <= 1 else (n + sampling_rate - 1) // sampling_rate
+
+
 def _build_cuda(width: int, text, sampling_rate: int, retain_lcp: bool, retain_isa: bool,
                 threads: int) -> CudaBuildResult:
-    """Same contract as BuildDivsufsort<Index> (src/divsufsort_backend.cpp:24-157)
-    for sampling_rate 1: SA in Index, ISA/LCP as uint64 when retained."""
+    """Same contract as BuildDivsufsort<Index> (src/divsufsort_backend.cpp:24-157):
+    SA in Index (the suffixes at multiples of sampling_rate), ISA/LCP as uint64
+    when retained."""
     t = _as_text(text)
-    if sampling_rate != 1:
-        raise SufkitError(ErrorCode.UNSUPPORTED_BACKEND,
-                          "the GPU constructor builds complete suffix arrays (K=1)")
+    if sampling_rate < 1:
+        raise SufkitError(ErrorCode.INVALID_INPUT, "sampling rate must be at least 1")
     if threads == 0:
         raise SufkitError(ErrorCode.INVALID_INPUT, "thread count must be greater than zero")
     limit = np.iinfo(np.int32).max if width == 32 else np.iinfo(np.int64).max
@@ -576,7 +588,8 @@ def _build_cuda(width: int, text, sampling_rate: int, retain_lcp: bool, retain_i
     ctx = default_context()
     r = ctx.build(t, sa_bits=64 if width == 64 else 32,
                   isa_bits=64 if (retain_isa or retain_lcp) else 0,
-                  lcp=LcpEncoding.RAW64 if retain_lcp else LcpEncoding.NONE)
+                  lcp=LcpEncoding.RAW64 if retain_lcp else LcpEncoding.NONE,
+                  sampling_rate=sampling_rate)
     sa = r.sa_low.astype(np.int32 if width == 32 else np.int64, copy=False)
     st = r.stats
     return CudaBuildResult(

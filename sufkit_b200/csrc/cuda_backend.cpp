@@ -46,9 +46,7 @@ CudaBuildResult<Index> BuildCuda(const std::vector<std::uint8_t>& text,
                                  bool retain_isa, std::uint32_t threads) {
   // Same argument checks as BuildDivsufsort (src/divsufsort_backend.cpp:29-42).
   if (threads == 0) throw Error(ErrorCode::kInvalidInput, "thread count must be greater than zero");
-  if (sampling_rate != 1) {
-    throw Error(ErrorCode::kUnsupportedBackend, "the CUDA constructor builds complete suffix arrays");
-  }
+  if (sampling_rate == 0) throw Error(ErrorCode::kInvalidInput, "sampling rate must be at least 1");
   const std::uint64_t limit = std::is_same_v<Index, std::int32_t>
                                   ? std::uint64_t(std::numeric_limits<std::int32_t>::max())
                                   : std::uint64_t(std::numeric_limits<std::int64_t>::max());
@@ -62,14 +60,17 @@ CudaBuildResult<Index> BuildCuda(const std::vector<std::uint8_t>& text,
   }
   CudaBuildResult<Index> result;
   const std::uint64_t n = text.size();
-  result.suffix_array.resize(n);
-  if (retain_isa || retain_lcp) result.isa.resize(n);
-  if (retain_lcp) result.lcp.resize(n);
+  // Sampled rows: the suffixes at multiples of the rate (divsufsort_backend.cpp:62-73).
+  const std::uint64_t rows = (n + sampling_rate - 1) / sampling_rate;
+  result.suffix_array.resize(rows);
+  if (retain_isa || retain_lcp) result.isa.resize(rows);
+  if (retain_lcp) result.lcp.resize(rows);
   sufgpu_build_desc desc{};
   desc.sa_storage_bits = sizeof(Index) * 8;
   desc.isa_storage_bits = (retain_isa || retain_lcp) ? 64 : 0;
   desc.lcp_encoding = retain_lcp ? SUFGPU_LCP_RAW64 : SUFGPU_LCP_NONE;
   desc.flags = SUFGPU_FLAG_VALIDATE;
+  desc.sampling_rate = sampling_rate;
   sufgpu_outputs out{};
   out.sa_low = result.suffix_array.data();
   out.isa_low = result.isa.empty() ? nullptr : result.isa.data();

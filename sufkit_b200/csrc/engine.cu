@@ -1095,11 +1095,92 @@ u64 high_bytes(u32 bits, u64 rows) { return bits == 40 ? rows : bits == 48 ? 2 *
 
 // Everything after the sort: ISA and SA packing, validation, LCP (raw or
 // byte-coded with anchors) and the copies into each instance's planes.
+// Sampled outputs (rate K > 1): complete SA, ISA and row LCP first, then the
+// kept rows (sample_kernel) packed into each instance's planes of
+// ceil(n_i / K) rows.
+void emit_sampled(Engine& e, const sufgpu_build_desc& d, sufgpu_outputs* outs, u32 count) {
+  sufgpu_ctx& c = e.c;
+  Layout& L = e.L;
+  const u64 n = e.n;
+  const u32 rate = d.sampling_rate;
+  if (d.flags & SUFGPU_FLAG_VALIDATE) {
+    e.launch("validate", n * 8, validate_kernel, e.grid_stride_blocks(n, 256), 256, 0, e.sa,
+             L.rank, n, e.segments(), L.flags);
+  }
+  SG_CUDA(cudaEventRecord(c.ev[3], c.stream));
+  const bool want_lcp = d.lcp_encoding != SUFGPU_LCP_NONE;
+  const u32* lcp = want_lcp ? e.lcp_phase().lcp : nullptr;
+  // Per-instance sampled offsets.
+  std::vector<u64> off(count + 1, 0);
+  for (u32 j = 0; j < count; ++j) {
+    off[j + 1] = off[j] + (e.begin[j + 1] - e.begin[j] + rate - 1) / rate;
+  }
+  const u64 kept = off[count];
+  e.sync();
+  std::memcpy(c.host_small, off.data(), (count + 1) * 8);
+  SG_CUDA(cudaMemcpyAsync(L.digit_start, c.host_small, (count + 1) * 8, cudaMemcpyHostToDevice,
+                          c.stream));
+  u32* sa_k = reinterpret_cast<u32*>(L.k0);
+  u32* isa_k = sa_k + kept;
+  u32* lcp_k = isa_k + kept;
+  if (want_lcp) SG_CUDA(cudaMemsetAsync(lcp_k, 0xff, kept * 4, c.stream));
+  const u64 tiles = (n + kScanTile - 1) / kScanTile;
+  e.zero(L.status, (tiles + 1) * 8);
+  e.zero(L.counters, 4);
+  e.launch("sample", n * (want_lcp ? 12 : 8) + kept * 12, sample_kernel, tiles, kScanBlock, 0,
+           static_cast<const u32*>(e.sa), lcp, n, e.segments(), rate,
+           static_cast<const u64*>(L.digit_start), kept, sa_k, isa_k, lcp_k, L.status,
+           L.counters, L.flags);
+  // Pack and copy: sampled values are instance-local already (one segment).
+  const u64 b2[2] = {0, kept};
+  std::memcpy(c.host_small + 4096, b2, 16);
+  SG_CUDA(cudaMemcpyAsync(L.sort_begin, c.host_small + 4096, 16, cudaMemcpyHostToDevice, c.stream));
+  const Segments whole{L.sort_begin, 1};
+  u8* low = reinterpret_cast<u8*>(L.k1);
+  u8* high = low + kept * 8;
+  auto emit = [&](const u32* values, u32 bits, bool isa) {
+    const u64 w = bits == 64 ? 8 : 4;
+    e.launch("pack", kept * (4 + w + high_bytes(bits, 1)), pack_kernel,
+             e.grid_stride_blocks(kept, 256), 256, 0, values, kept, whole, bits,
+             static_cast<void*>(low), static_cast<void*>(high));
+    for (u32 j = 0; j < count; ++j) {
+      const u64 rows = off[j + 1] - off[j];
+      copy_out(c, isa ? outs[j].isa_low : outs[j].sa_low, low + off[j] * w, rows * w);
+      if (high_bytes(bits, 1)) {
+        copy_out(c, isa ? outs[j].isa_high : outs[j].sa_high, high + high_bytes(bits, off[j]),
+                 high_bytes(bits, rows));
+      }
+    }
+  };
+  if (d.isa_storage_bits) emit(isa_k, d.isa_storage_bits, true);
+  emit(sa_k, d.sa_storage_bits, false);
+  SG_CUDA(cudaEventRecord(c.ev[4], c.stream));
+  if (want_lcp) {
+    const bool wide = d.lcp_encoding == SUFGPU_LCP_RAW64;
+    const u8* src = reinterpret_cast<const u8*>(lcp_k);
+    if (wide) {
+      e.launch("lcp_widen", kept * 12, widen_kernel<u64>, e.grid_stride_blocks(kept, 256), 256, 0,
+               static_cast<const u32*>(lcp_k), kept, reinterpret_cast<u64*>(low));
+      src = low;
+    }
+    const u64 w = wide ? 8 : 4;
+    for (u32 j = 0; j < count; ++j) {
+      copy_out(c, outs[j].lcp, src + off[j] * w, (off[j + 1] - off[j]) * w);
+    }
+  }
+  SG_CUDA(cudaEventRecord(c.ev[5], c.stream));
+  e.sync();
+}
+
 void emit_outputs(Engine& e, const sufgpu_build_desc& d, sufgpu_outputs* outs,
                   sufgpu_anchors* anchors, u32 count) {
   sufgpu_ctx& c = e.c;
   Layout& L = e.L;
   const u64 n = e.n;
+  if (d.sampling_rate > 1) {
+    emit_sampled(e, d, outs, count);
+    return;
+  }
 
   // ISA: rank holds global rows.  Stage packed planes in k0/k1 when the
   // layout differs from the device one, then copy each instance's rows.
@@ -1329,6 +1410,10 @@ void sufgpu_host_free(void* p) {
 
 static sufgpu_status check_desc(sufgpu_ctx* ctx, const sufgpu_build_desc* d) {
   if (!d) return fail(ctx, SUFGPU_INVALID_INPUT, "build descriptor is null");
+  if (d->sampling_rate > 1 && d->lcp_encoding != SUFGPU_LCP_NONE &&
+      d->lcp_encoding != SUFGPU_LCP_RAW32 && d->lcp_encoding != SUFGPU_LCP_RAW64) {
+    return fail(ctx, SUFGPU_INVALID_INPUT, "sampled builds keep raw LCP only");
+  }
   if (!valid_width(d->sa_storage_bits)) return fail(ctx, SUFGPU_INVALID_INPUT, "invalid SA storage width");
   if (d->isa_storage_bits && !valid_width(d->isa_storage_bits))
     return fail(ctx, SUFGPU_INVALID_INPUT, "invalid ISA storage width");

@@ -42,12 +42,17 @@ int main(int argc, char** argv) {
   dump(prefix + ".primary", lowmem.lcp_primary);
   dump(prefix + ".anchor_pos", lowmem.anchor_positions);
   dump(prefix + ".anchor_val", lowmem.anchor_values);
+  // Sampling rate 4: the suffixes at multiples of 4 (ISA and LCP retained).
+  auto sampled = sufgpu::BuildCuda64(text, 4, true, true, 1);
+  dump(prefix + ".sa_k4", sampled.suffix_array);
+  dump(prefix + ".isa_k4", sampled.isa);
+  dump(prefix + ".lcp_k4", sampled.lcp);
   // Error categories match sufkit::ErrorCode.
   int checks = 0;
   try {
-    sufgpu::BuildCuda32(text, 4, true, false, 1);
+    sufgpu::BuildCuda32(text, 0, true, false, 1);
   } catch (const sufgpu::Error& e) {
-    checks += e.Code() == sufgpu::ErrorCode::kUnsupportedBackend;
+    checks += e.Code() == sufgpu::ErrorCode::kInvalidInput;
   }
   try {
     sufgpu::BuildCuda64(text, 1, true, false, 0);

@@ -40,3 +40,10 @@ def test_cpp_adapter_matches_reference(tmp_path):
     assert (load(tmp_path / "o.primary") == primary).all()
     assert (load(tmp_path / "o.anchor_pos") == pos).all()
     assert (load(tmp_path / "o.anchor_val") == val).all()
+    if oracle.ref() is not None:
+        sa_k, isa_k, lcp_k = oracle.ref_adapter_sampled(text, 4, 64)
+    else:
+        sa_k, isa_k, lcp_k = oracle.sample(sa, lcp, 4)
+    assert (load(tmp_path / "o.sa_k4") == sa_k).all()
+    assert (load(tmp_path / "o.isa_k4") == isa_k).all()
+    assert (load(tmp_path / "o.lcp_k4") == lcp_k).all()

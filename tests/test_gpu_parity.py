@@ -140,9 +140,12 @@ def test_build_cuda_mirror(ctx):
     r32 = sg.build_cuda32(t, 1, True, False, 1)
     assert r32.suffix_array.dtype == np.int32 and (r32.lcp == lcp).all()
     assert r32.isa.size == 0
+    sa_k, isa_k, lcp_k = oracle.sample(sa, lcp, 2)
+    r2 = sg.build_cuda32(t, 2, True, True, 1)
+    assert (r2.suffix_array == sa_k).all() and (r2.isa == isa_k).all() and (r2.lcp == lcp_k).all()
     with pytest.raises(sg.SufkitError) as e:
-        sg.build_cuda32(t, 2, True, False, 1)
-    assert e.value.code == sg.ErrorCode.UNSUPPORTED_BACKEND
+        sg.build_cuda32(t, 0, True, False, 1)
+    assert e.value.code == sg.ErrorCode.INVALID_INPUT
 
 
 def test_invalid_inputs(ctx):

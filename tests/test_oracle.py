@@ -94,3 +94,22 @@ def test_pack_rejects_out_of_range():
         oracle.pack(np.array([5], np.uint64), 5, 32)  # value >= symbol count
     with pytest.raises(ValueError):
         oracle.pack(np.array([1], np.uint64), (1 << 32) + 2, 32)  # text too big for 32
+
+
+@pytest.mark.parametrize("rate", [2, 3, 7, 32])
+def test_sampling_restatement_matches_reference(golden, rate):
+    """The sampling of a complete build (oracle.sample) equals the reference's
+    BuildDivsufsort64 with sampling_rate K (SA, ISA, LCP of sampled rows)."""
+    if oracle.ref() is None:
+        pytest.skip("reference library not built")
+    rng = np.random.default_rng(rate)
+    texts = [case["text"] for case in list(golden.values())[:20]]
+    texts += [np.concatenate([rng.integers(2, 6, size=n).astype(np.uint8), [0]]).astype(np.uint8)
+              for n in (1, 2, 5, 100, 5000)]
+    for t in texts:
+        sa, isa, lcp, _ = oracle.ref_adapter(t, 64)
+        sa_k, isa_k, lcp_k = oracle.sample(sa, lcp, rate)
+        r_sa, r_isa, r_lcp = oracle.ref_adapter_sampled(t, rate, 64)
+        assert (sa_k == r_sa.astype(np.int64)).all()
+        assert (isa_k == r_isa.astype(np.int64)).all()
+        assert (lcp_k == r_lcp.astype(np.int64)).all()
