@@ -69,6 +69,12 @@ typedef struct sufgpu_build_desc {
    * rows per instance, ISA[p / K] = sampled row, LCP = lcp of consecutive
    * sampled rows (raw LCP only). */
   uint32_t sampling_rate;
+  /* 0 = none.  1..10 = also build the Fast index's exact k-mer prefix
+   * directory for this k (FastPrefixIndex, src/fast_prefix_index.cpp) into
+   * outputs.prefix_intervals: 4^k uint64 entries begin | end << 32, (n, n) for
+   * k-mers that do not occur (single complete builds; pick k with
+   * sufgpu_prefix_select_k). */
+  uint32_t prefix_k;
 } sufgpu_build_desc;
 
 /* Caller-owned output planes of one instance (n rows each).  Each pointer may
@@ -83,6 +89,7 @@ typedef struct sufgpu_outputs {
   void *isa_low;
   void *isa_high;
   void *lcp;
+  void *prefix_intervals; /* 4^prefix_k uint64 entries (desc.prefix_k > 0) */
 } sufgpu_outputs;
 
 /* Byte-coded overflow anchors (text-ordered positions with their LCP values,
@@ -116,6 +123,8 @@ typedef struct sufgpu_build_stats {
   uint32_t long_runs;         /* single-symbol runs split directly after the seed */
   uint32_t seg_sort_fallbacks;/* rounds whose groups did not fit the shared-memory sort */
   uint32_t reserved;
+  uint64_t prefix_kmers;      /* rows with a canonical k-mer (FastPrefixIndex::IndexedKmers) */
+  uint64_t prefix_entries;    /* k-mers present (FastPrefixIndex::NonemptyEntries) */
 } sufgpu_build_stats;
 
 typedef struct sufgpu_ctx sufgpu_ctx;
@@ -130,6 +139,12 @@ SUFGPU_API const char *sufgpu_last_error(const sufgpu_ctx *ctx);
 
 /* Largest text (symbols, sentinel included) one build accepts. */
 SUFGPU_API uint64_t sufgpu_max_symbols(void);
+
+/* k of the Fast index's prefix directory, as FastPrefixIndex::SelectK with
+ * its default options (src/fast_prefix_index.cpp:280-301): the largest k in
+ * 8..10 whose directory (4^k entries of two 32-bit rows) fits 25% of
+ * resident_core_bytes; 0 (no directory) below 2^16 suffixes. */
+SUFGPU_API uint32_t sufgpu_prefix_select_k(uint64_t suffix_count, uint64_t resident_core_bytes);
 
 /* Device bytes one build of n symbols needs with this descriptor. */
 SUFGPU_API uint64_t sufgpu_device_bytes(uint64_t n, const sufgpu_build_desc *desc);

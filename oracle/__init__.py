@@ -68,6 +68,7 @@ def ref() -> Optional[ctypes.CDLL]:
         lib.sufref_last_error.restype = ctypes.c_char_p
         lib.sufref_divsufsort64.argtypes = [P, P, ctypes.c_int64]
         lib.sufref_divsufsort32.argtypes = [P, P, ctypes.c_int32]
+        lib.sufref_prefix_directory.argtypes = [P, U64, U64, P, P, P, P]
         lib.sufref_adapter_build_sampled.argtypes = [ctypes.c_int, P, U64, ctypes.c_uint32,
                                                      ctypes.c_int, ctypes.c_int, ctypes.c_uint32,
                                                      P, P, P, P]
@@ -226,6 +227,52 @@ def sample(sa: np.ndarray, lcp: np.ndarray, rate: int):
         starts = rows + 1
         lcp_k[1:] = np.minimum.reduceat(np.append(lcp, 0), starts)[: rows.size - 1]
     return sa_k, isa_k, lcp_k
+
+
+def ref_prefix_directory(text: np.ndarray, resident_core_bytes: int):
+    """FastPrefixIndex::Build with default options over the reference's SA:
+    (k, intervals[4^k] as begin | end << 32 with (n, n) for absent k-mers,
+    indexed k-mers, nonempty entries)."""
+    lib = ref()
+    t = np.ascontiguousarray(text, np.uint8)
+    out = np.empty(1 << 20, np.uint64)
+    k = ctypes.c_uint32()
+    kmers = ctypes.c_uint64()
+    entries = ctypes.c_uint64()
+    _check(lib, lib.sufref_prefix_directory(_p(t), t.size, int(resident_core_bytes),
+                                            ctypes.byref(k), _p(out), ctypes.byref(kmers),
+                                            ctypes.byref(entries)))
+    return k.value, out[: (1 << (2 * k.value)) if k.value else 0].copy(), kmers.value, entries.value
+
+
+def prefix_directory(text: np.ndarray, sa: np.ndarray, k: int) -> np.ndarray:
+    """Restatement of the Fast index's k-mer directory
+    (src/fast_prefix_index.cpp:131-205): for each k-mer of bytes 2..5 the SA
+    rows [begin, end) of the suffixes starting with it, packed
+    begin | end << 32, (n, n) where absent."""
+    t = np.ascontiguousarray(text, np.uint8)
+    n = t.size
+    sa = np.asarray(sa, np.int64)
+    table = np.full(1 << (2 * k), n | (n << 32), np.uint64)
+    if n < k:
+        return table
+    windows = np.lib.stride_tricks.sliding_window_view(t, k)  # position p: t[p:p+k]
+    canonical = ((windows >= 2) & (windows <= 5)).all(axis=1)
+    weights = (1 << (2 * np.arange(k - 1, -1, -1))).astype(np.int64)
+    keys = ((windows.astype(np.int64) - 2) & 3) @ weights
+    rows_pos = sa  # row r -> position sa[r]
+    valid_rows = np.flatnonzero((rows_pos <= n - k) & canonical[np.minimum(rows_pos, n - k)])
+    if valid_rows.size == 0:
+        return table
+    row_keys = keys[rows_pos[valid_rows]]
+    first = np.ones(valid_rows.size, bool)
+    first[1:] = (row_keys[1:] != row_keys[:-1]) | (valid_rows[1:] != valid_rows[:-1] + 1)
+    last = np.ones(valid_rows.size, bool)
+    last[:-1] = first[1:]
+    begins = valid_rows[first].astype(np.uint64)
+    ends = (valid_rows[last] + 1).astype(np.uint64)
+    table[row_keys[first]] = begins | (ends << np.uint64(32))
+    return table
 
 
 def ref_divsufsort64(text: np.ndarray) -> np.ndarray:

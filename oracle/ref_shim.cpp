@@ -33,6 +33,7 @@
 
 #include "coordinate_storage.hpp"
 #include "divsufsort_backend.hpp"
+#include "fast_prefix_index.hpp"
 #include "genome_reference_internal.hpp"
 #include "lcp_storage.hpp"
 
@@ -208,6 +209,63 @@ int sufref_adapter_build_sampled(int width, const uint8_t* text, uint64_t n, uin
     } else {
       run(sufkit::detail::BuildDivsufsort64(input, rate, retain_lcp != 0, retain_isa != 0,
                                             threads));
+    }
+    return 0;
+  } catch (const std::exception& error) {
+    return Fail(error);
+  }
+}
+
+// FastPrefixIndex::Build (default options) over the reference's own
+// divsufsort64 SA/ISA of a logical text (contigs split at separators, one
+// final sentinel).  *k_out receives the selected k (0 = no directory) and
+// intervals_out (4^k entries) begin | end << 32 per k-mer from Lookup, with
+// (n, n) for k-mers that do not occur.
+int sufref_prefix_directory(const uint8_t* text, uint64_t n, uint64_t resident_core_bytes,
+                            uint32_t* k_out, uint64_t* intervals_out, uint64_t* kmers_out,
+                            uint64_t* entries_out) {
+  try {
+    std::vector<std::uint8_t> input(text, text + n);
+    std::vector<int64_t> sa(n);
+    if (divsufsort64(text, reinterpret_cast<saidx64_t*>(sa.data()), static_cast<saidx64_t>(n)) != 0) {
+      throw std::runtime_error("divsufsort64 failed");
+    }
+    std::vector<std::uint64_t> sa64(n), isa64(n);
+    for (uint64_t r = 0; r < n; ++r) {
+      sa64[r] = static_cast<std::uint64_t>(sa[r]);
+      isa64[sa64[r]] = r;
+    }
+    auto sa_s = CoordinateStorage::FromUInt64(std::move(sa64), WidthFromBits(64), n,
+                                              ErrorCode::kBuildFailure, "suffix array");
+    auto isa_s = CoordinateStorage::FromUInt64(std::move(isa64), WidthFromBits(64), n,
+                                               ErrorCode::kBuildFailure, "inverse suffix array");
+    std::vector<sufkit::Position> starts, lengths;
+    sufkit::Position start = 0;
+    for (uint64_t i = 0; i + 1 < n; ++i) {
+      if (text[i] == 1) {
+        starts.push_back(start);
+        lengths.push_back(i - start);
+        start = i + 1;
+      }
+    }
+    auto index = sufkit::detail::FastPrefixIndex::Build(input, sa_s, isa_s, starts, lengths,
+                                                resident_core_bytes);
+    *k_out = index.K();
+    *kmers_out = index.IndexedKmers();
+    *entries_out = index.NonemptyEntries();
+    const uint32_t k = index.K();
+    if (k == 0) return 0;
+    std::vector<std::uint8_t> pattern(k);
+    for (uint64_t key = 0; key < (uint64_t{1} << (2 * k)); ++key) {
+      for (uint32_t j = 0; j < k; ++j) {
+        pattern[j] = static_cast<std::uint8_t>(2 + ((key >> (2 * (k - 1 - j))) & 3));
+      }
+      const auto interval = index.Lookup(pattern);
+      if (!interval || interval->Empty()) {
+        intervals_out[key] = n | (n << 32);
+      } else {
+        intervals_out[key] = interval->begin | (interval->end << 32);
+      }
     }
     return 0;
   } catch (const std::exception& error) {

@@ -64,13 +64,14 @@ class _Desc(ctypes.Structure):
                 ("isa_storage_bits", ctypes.c_uint32),
                 ("lcp_encoding", ctypes.c_uint32),
                 ("flags", ctypes.c_uint32),
-                ("sampling_rate", ctypes.c_uint32)]
+                ("sampling_rate", ctypes.c_uint32),
+                ("prefix_k", ctypes.c_uint32)]
 
 
 class _Outputs(ctypes.Structure):
     _fields_ = [("sa_low", ctypes.c_void_p), ("sa_high", ctypes.c_void_p),
                 ("isa_low", ctypes.c_void_p), ("isa_high", ctypes.c_void_p),
-                ("lcp", ctypes.c_void_p)]
+                ("lcp", ctypes.c_void_p), ("prefix_intervals", ctypes.c_void_p)]
 
 
 class _Anchors(ctypes.Structure):
@@ -89,7 +90,8 @@ class _Stats(ctypes.Structure):
                 ("irreducible_long", ctypes.c_uint64),
                 ("anchors", ctypes.c_uint64), ("kernel_launches", ctypes.c_uint32),
                 ("long_runs", ctypes.c_uint32), ("seg_sort_fallbacks", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32)]
+                ("reserved", ctypes.c_uint32), ("prefix_kmers", ctypes.c_uint64),
+                ("prefix_entries", ctypes.c_uint64)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
@@ -149,6 +151,7 @@ _SIGNATURES = {
                                             ctypes.POINTER(ctypes.c_double),
                                             ctypes.POINTER(ctypes.c_uint64)]),
     "sufgpu_set_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int64]),
+    "sufgpu_prefix_select_k": (ctypes.c_uint32, [ctypes.c_uint64, ctypes.c_uint64]),
     "sufgpu_set_tuning_class": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_char_p,
                                                ctypes.c_int64]),
     "sufgpu_clear_tuning_classes": (None, [ctypes.c_void_p]),
@@ -241,6 +244,7 @@ class BuildResult:
     lcp: Optional[np.ndarray] = None
     anchor_positions: Optional[np.ndarray] = None
     anchor_values: Optional[np.ndarray] = None
+    prefix_intervals: Optional[np.ndarray] = None
     stats: dict = field(default_factory=dict)
 
     @property
@@ -329,7 +333,8 @@ class Context:
     @staticmethod
     def _outputs(planes: dict) -> _Outputs:
         return _Outputs(*(_ptr(planes.get(k)) for k in
-                          ("sa_low", "sa_high", "isa_low", "isa_high", "lcp")))
+                          ("sa_low", "sa_high", "isa_low", "isa_high", "lcp",
+                           "prefix_intervals")))
 
     @staticmethod
     def _anchors(a: _Anchors, lcp: LcpEncoding):
@@ -345,17 +350,20 @@ class Context:
 
     def build(self, text, sa_bits: int = 32, isa_bits: int = 32,
               lcp: LcpEncoding = LcpEncoding.RAW32, validate: bool = False,
-              sampling_rate: int = 1) -> BuildResult:
+              sampling_rate: int = 1, prefix_k: int = 0) -> BuildResult:
         """One complete build of ``text`` (the logical text including its
         sentinel).  Returns host planes; see include/sufgpu/sufgpu.h.  With
         sampling_rate K > 1 the planes hold the ceil(n / K) suffixes at
-        positions that are multiples of K."""
+        positions that are multiples of K.  prefix_k > 0 also returns the Fast
+        index's k-mer directory (4^k entries begin | end << 32)."""
         t = _as_text(text)
         n = int(t.size)
         lcp = LcpEncoding(lcp)
         planes = self._alloc_outputs(_rows(n, sampling_rate), sa_bits, isa_bits, lcp)
+        if prefix_k:
+            planes["prefix_intervals"] = np.empty(1 << (2 * prefix_k), np.uint64)
         desc = _Desc(sa_bits, isa_bits, int(lcp), FLAG_VALIDATE if validate else 0,
-                     int(sampling_rate))
+                     int(sampling_rate), int(prefix_k))
         out = self._outputs(planes)
         anchors = _Anchors()
         stats = _Stats()
@@ -425,7 +433,8 @@ class Context:
         """Build from a device-resident text into device-resident planes
         (raw pointers, e.g. from torch tensors).  Returns the stats."""
         desc = _Desc(sa_bits, isa_bits, int(LcpEncoding(lcp)), FLAG_VALIDATE if validate else 0)
-        out = _Outputs(*(out_ptrs.get(k) for k in ("sa_low", "sa_high", "isa_low", "isa_high", "lcp")))
+        out = _Outputs(*(out_ptrs.get(k) for k in ("sa_low", "sa_high", "isa_low", "isa_high", "lcp",
+                                                   "prefix_intervals")))
         anchors = _Anchors()
         stats = _Stats()
         status = self._lib.sufgpu_build(self._h, text_ptr, n, ctypes.byref(desc), ctypes.byref(out),
@@ -564,6 +573,12 @@ def default_context() -> Context:
     if _default_ctx is None:
         _default_ctx = Context(0)
     return _default_ctx
+
+
+def prefix_select_k(suffix_count: int, resident_core_bytes: int) -> int:
+    """FastPrefixIndex::SelectK with its default options: the directory's k
+    (8..10) for an index of this size, 0 for none."""
+    return int(library().sufgpu_prefix_select_k(int(suffix_count), int(resident_core_bytes)))
 
 
 def _rows(n: int, sampling_rate: int) -> int:

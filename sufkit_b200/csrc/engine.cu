@@ -30,6 +30,7 @@
 #include "doubling.cuh"
 #include "lcp.cuh"
 #include "pack.cuh"
+#include "prefixdir.cuh"
 #include "radix.cuh"
 #include "runs.cuh"
 #include "segsort.cuh"
@@ -1312,6 +1313,28 @@ struct TuningScope {
   ~TuningScope() { c.tune = saved; }
 };
 
+// The Fast index's k-mer prefix directory from the final SA (prefixdir.cuh),
+// staged in k1 (free until the outputs are packed) and copied out at once.
+void emit_prefix_directory(Engine& e, const sufgpu_build_desc& d, const sufgpu_outputs& out) {
+  sufgpu_ctx& c = e.c;
+  Layout& L = e.L;
+  const u64 entries = u64(1) << (2 * d.prefix_k);
+  u64* table = L.k1;
+  e.launch("prefix_fill", entries * 8, prefix_fill_kernel, e.grid_stride_blocks(entries, 256),
+           256, 0, table, entries, e.n | (e.n << 32));
+  e.zero(L.scalars + 24, 16);
+  e.launch("prefix_directory", e.n * (4 + d.prefix_k) + entries * 8, prefix_directory_kernel,
+           (e.n + kDirTile - 1) / kDirTile, kDirTile, 0, static_cast<const u8*>(L.text),
+           static_cast<const u32*>(e.sa), e.n, d.prefix_k, table,
+           reinterpret_cast<unsigned long long*>(L.scalars + 24), L.flags);
+  copy_out(c, out.prefix_intervals, table, entries * 8);
+  SG_CUDA(cudaMemcpyAsync(c.host_scalars + 24, L.scalars + 24, 16, cudaMemcpyDeviceToHost,
+                          c.stream));
+  e.sync();
+  e.st.prefix_kmers = c.host_scalars[24];
+  e.st.prefix_entries = c.host_scalars[25];
+}
+
 // Shared build body for one or many instances (already concatenated in
 // L.text).  outs[j] receives instance j's planes.
 void run_build(Engine& e, const sufgpu_build_desc& d, sufgpu_outputs* outs,
@@ -1319,6 +1342,7 @@ void run_build(Engine& e, const sufgpu_build_desc& d, sufgpu_outputs* outs,
   SG_CUDA(cudaEventRecord(e.c.ev[1], e.c.stream));
   e.suffix_sort();
   SG_CUDA(cudaEventRecord(e.c.ev[2], e.c.stream));
+  if (d.prefix_k) emit_prefix_directory(e, d, outs[0]);
   emit_outputs(e, d, outs, anchors, count);
 }
 
@@ -1391,6 +1415,18 @@ const char* sufgpu_last_error(const sufgpu_ctx* ctx) {
 
 uint64_t sufgpu_max_symbols(void) { return 0xffffffffull; }
 
+uint32_t sufgpu_prefix_select_k(uint64_t suffix_count, uint64_t resident_core_bytes) {
+  // FastPrefixIndexOptions defaults: k in [8, 10], 2500 basis points of the
+  // resident core arrays, at least 2^16 suffixes; 32-bit rows below 2^32.
+  if (suffix_count < (u64(1) << 16)) return 0;
+  const u64 budget = (resident_core_bytes / 10000) * 2500 + ((resident_core_bytes % 10000) * 2500) / 10000;
+  const u64 row_bytes = suffix_count <= 0xffffffffull ? 4 : 8;
+  for (u32 k = 10; k >= 8; --k) {
+    if ((u64(1) << (2 * k)) * 2 * row_bytes <= budget) return k;
+  }
+  return 0;
+}
+
 uint64_t sufgpu_device_bytes(uint64_t n, const sufgpu_build_desc*) {
   return plan_layout(nullptr, n, 1).total;
 }
@@ -1418,6 +1454,10 @@ static sufgpu_status check_desc(sufgpu_ctx* ctx, const sufgpu_build_desc* d) {
   if (d->isa_storage_bits && !valid_width(d->isa_storage_bits))
     return fail(ctx, SUFGPU_INVALID_INPUT, "invalid ISA storage width");
   if (d->lcp_encoding > SUFGPU_LCP_BYTE64) return fail(ctx, SUFGPU_INVALID_INPUT, "invalid LCP encoding");
+  if (d->prefix_k > 10) return fail(ctx, SUFGPU_INVALID_INPUT, "prefix directory k must be at most 10");
+  if (d->prefix_k && d->sampling_rate > 1) {
+    return fail(ctx, SUFGPU_INVALID_INPUT, "the prefix directory needs a complete suffix array");
+  }
   return SUFGPU_OK;
 }
 
@@ -1476,6 +1516,13 @@ sufgpu_status sufgpu_build(sufgpu_ctx* ctx, const uint8_t* text, uint64_t n,
   if (n > sufgpu_max_symbols()) return fail(ctx, SUFGPU_INVALID_INPUT, "text exceeds 2^32-1 symbols");
   if (n > 0 && !text) return fail(ctx, SUFGPU_INVALID_INPUT, "text is null");
   if (!out) return fail(ctx, SUFGPU_INVALID_INPUT, "outputs are null");
+  if (desc->prefix_k) {
+    if (!out->prefix_intervals) return fail(ctx, SUFGPU_INVALID_INPUT, "prefix_intervals is null");
+    // The directory is staged in the 8n-byte key buffer.
+    if ((u64(8) << (2 * desc->prefix_k)) > 8 * std::max<u64>(n, 1) + 256) {
+      return fail(ctx, SUFGPU_INVALID_INPUT, "prefix directory larger than the text allows");
+    }
+  }
   const auto t0 = std::chrono::steady_clock::now();
   ctx->launches = 0;
   ctx->pending.clear();
@@ -1551,6 +1598,9 @@ extern "C" sufgpu_status sufgpu_build_batch(sufgpu_ctx* ctx, sufgpu_instance* in
   if (!instances) return fail(ctx, SUFGPU_INVALID_INPUT, "instances are null");
   if (count > kMaxSegmentsPerLaunch) {
     return fail(ctx, SUFGPU_INVALID_INPUT, "too many instances in one batch launch");
+  }
+  if (desc->prefix_k) {
+    return fail(ctx, SUFGPU_INVALID_INPUT, "the prefix directory is built for single references");
   }
   std::vector<u64> begin(count + 1, 0);
   for (u32 j = 0; j < count; ++j) {
@@ -2094,6 +2144,8 @@ sufgpu_status sufgpu_server_submit(sufgpu_server* S, const uint8_t* text, uint64
                                    uint64_t* ticket) {
   if (!S || !desc || !out || !ticket || (n && !text)) return SUFGPU_INVALID_INPUT;
   if (auto s = check_desc(S->ctx, desc)) return s;
+  // Served builds return complete arrays without the prefix directory.
+  if (desc->sampling_rate > 1 || desc->prefix_k) return SUFGPU_INVALID_INPUT;
   if (n == 0 || n > sufgpu_max_symbols()) return SUFGPU_INVALID_INPUT;
   auto r = std::make_shared<ServedRequest>();
   r->text = text;

@@ -113,3 +113,22 @@ def test_sampling_restatement_matches_reference(golden, rate):
         assert (sa_k == r_sa.astype(np.int64)).all()
         assert (isa_k == r_isa.astype(np.int64)).all()
         assert (lcp_k == r_lcp.astype(np.int64)).all()
+
+
+def test_prefix_directory_restatement_matches_reference():
+    """oracle.prefix_directory (from the SA) equals the reference's
+    FastPrefixIndex (built from its own SA/ISA, read back with Lookup)."""
+    if oracle.ref() is None:
+        pytest.skip("reference library not built")
+    texts = [synth.plain_4mbp(scale=0.2).logical_text(),
+             synth.repeat_rich_100mbp(scale=0.003).logical_text()]
+    for t, want_k in zip(texts, (9, 8)):
+        resident = t.size * 12  # SA + ISA + LCP, 32-bit
+        k, table, kmers, entries = oracle.ref_prefix_directory(t, resident)
+        assert k == want_k
+        import sufkit_b200 as sg
+        assert sg.prefix_select_k(t.size, resident) == k
+        sa = oracle.ref_divsufsort64(t)
+        mine = oracle.prefix_directory(t, sa, k)
+        assert (mine == table).all()
+        assert int((mine != (t.size | (t.size << 32))).sum()) == entries
