@@ -54,6 +54,11 @@ typedef enum sufgpu_lcp_encoding {
 
 /* Build flags. */
 #define SUFGPU_FLAG_VALIDATE 1u /* check the SA is a permutation (device) */
+/* CRC-32 (zlib's crc32, the checksum of a .sufidx section) of every output
+ * plane, computed on the device before the plane is copied out, into
+ * stats.plane_crc (single builds).  A section's CRC follows from its header
+ * bytes and these with zlib's crc32_combine. */
+#define SUFGPU_FLAG_PLANE_CRC 2u
 
 /* What to build.  Stored widths follow CoordinateStorageWidth
  * (include/sufkit/types.hpp:100-111): 32 native, 40 split low32+high8,
@@ -125,6 +130,10 @@ typedef struct sufgpu_build_stats {
   uint32_t reserved;
   uint64_t prefix_kmers;      /* rows with a canonical k-mer (FastPrefixIndex::IndexedKmers) */
   uint64_t prefix_entries;    /* k-mers present (FastPrefixIndex::NonemptyEntries) */
+  /* SUFGPU_FLAG_PLANE_CRC: CRC-32 of sa_low, sa_high, isa_low, isa_high, lcp
+   * as written (0 for planes not written). */
+  uint32_t plane_crc[5];
+  uint32_t reserved2;
 } sufgpu_build_stats;
 
 typedef struct sufgpu_ctx sufgpu_ctx;
@@ -139,6 +148,13 @@ SUFGPU_API const char *sufgpu_last_error(const sufgpu_ctx *ctx);
 
 /* Largest text (symbols, sentinel included) one build accepts. */
 SUFGPU_API uint64_t sufgpu_max_symbols(void);
+
+/* zlib's crc32(crc_in, data, bytes) of device memory of the context's device
+ * (the .sufidx section checksum, src/serialization.cpp:47-56, without a trip
+ * through the host): 16 KiB chunks in parallel, folded by polynomial
+ * multiplication.  No counterpart in the reference. */
+SUFGPU_API sufgpu_status sufgpu_crc32_device(sufgpu_ctx *ctx, const void *data, uint64_t bytes,
+                                             uint32_t crc_in, uint32_t *crc_out);
 
 /* k of the Fast index's prefix directory, as FastPrefixIndex::SelectK with
  * its default options (src/fast_prefix_index.cpp:280-301): the largest k in

@@ -57,6 +57,7 @@ class LcpEncoding(enum.IntEnum):
 
 
 FLAG_VALIDATE = 1
+FLAG_PLANE_CRC = 2
 
 
 class _Desc(ctypes.Structure):
@@ -91,10 +92,15 @@ class _Stats(ctypes.Structure):
                 ("anchors", ctypes.c_uint64), ("kernel_launches", ctypes.c_uint32),
                 ("long_runs", ctypes.c_uint32), ("seg_sort_fallbacks", ctypes.c_uint32),
                 ("reserved", ctypes.c_uint32), ("prefix_kmers", ctypes.c_uint64),
-                ("prefix_entries", ctypes.c_uint64)]
+                ("prefix_entries", ctypes.c_uint64), ("plane_crc", ctypes.c_uint32 * 5),
+                ("reserved2", ctypes.c_uint32)]
 
     def as_dict(self) -> dict:
-        return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
+        d = {name: getattr(self, name) for name, _ in self._fields_
+             if name not in ("reserved", "reserved2", "plane_crc")}
+        d["plane_crc"] = dict(zip(("sa_low", "sa_high", "isa_low", "isa_high", "lcp"),
+                                  list(self.plane_crc)))
+        return d
 
 
 class _ServerConfig(ctypes.Structure):
@@ -152,6 +158,8 @@ _SIGNATURES = {
                                             ctypes.POINTER(ctypes.c_uint64)]),
     "sufgpu_set_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int64]),
     "sufgpu_prefix_select_k": (ctypes.c_uint32, [ctypes.c_uint64, ctypes.c_uint64]),
+    "sufgpu_crc32_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                           ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]),
     "sufgpu_set_tuning_class": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_char_p,
                                                ctypes.c_int64]),
     "sufgpu_clear_tuning_classes": (None, [ctypes.c_void_p]),
@@ -350,7 +358,8 @@ class Context:
 
     def build(self, text, sa_bits: int = 32, isa_bits: int = 32,
               lcp: LcpEncoding = LcpEncoding.RAW32, validate: bool = False,
-              sampling_rate: int = 1, prefix_k: int = 0) -> BuildResult:
+              sampling_rate: int = 1, prefix_k: int = 0,
+              plane_crc: bool = False) -> BuildResult:
         """One complete build of ``text`` (the logical text including its
         sentinel).  Returns host planes; see include/sufgpu/sufgpu.h.  With
         sampling_rate K > 1 the planes hold the ceil(n / K) suffixes at
@@ -362,8 +371,8 @@ class Context:
         planes = self._alloc_outputs(_rows(n, sampling_rate), sa_bits, isa_bits, lcp)
         if prefix_k:
             planes["prefix_intervals"] = np.empty(1 << (2 * prefix_k), np.uint64)
-        desc = _Desc(sa_bits, isa_bits, int(lcp), FLAG_VALIDATE if validate else 0,
-                     int(sampling_rate), int(prefix_k))
+        flags = (FLAG_VALIDATE if validate else 0) | (FLAG_PLANE_CRC if plane_crc else 0)
+        desc = _Desc(sa_bits, isa_bits, int(lcp), flags, int(sampling_rate), int(prefix_k))
         out = self._outputs(planes)
         anchors = _Anchors()
         stats = _Stats()
@@ -404,6 +413,15 @@ class Context:
             results.append(BuildResult(anchor_positions=pos, anchor_values=val,
                                        stats=self.last_stats, **planes))
         return results
+
+    def crc32_device(self, ptr: int, nbytes: int, crc_in: int = 0) -> int:
+        """zlib's crc32(crc_in, data, nbytes) of device memory at ptr."""
+        out = ctypes.c_uint32()
+        status = self._lib.sufgpu_crc32_device(self._h, ptr, int(nbytes), int(crc_in),
+                                               ctypes.byref(out))
+        if status != 0:
+            _raise(status, self._error())
+        return int(out.value)
 
     def set_tuning(self, key: str, value: int) -> None:
         status = self._lib.sufgpu_set_tuning(self._h, key.encode(), int(value))

@@ -31,6 +31,7 @@
 #include "lcp.cuh"
 #include "pack.cuh"
 #include "prefixdir.cuh"
+#include "crc32.cuh"
 #include "radix.cuh"
 #include "runs.cuh"
 #include "segsort.cuh"
@@ -328,6 +329,9 @@ struct sufgpu_ctx {
     u32 kernels;
   };
   std::vector<CachedGraph> round_graphs;
+  // Fold buffers of sufgpu_crc32_device (grown on demand).
+  u32* crc_scratch = nullptr;
+  u64 crc_scratch_words = 0;
   // Layouts of recent builds: a layout's rounds are captured from its second
   // build on, so one-off builds never pay for a capture.
   std::vector<std::vector<u64>> seen_layouts;
@@ -354,6 +358,9 @@ struct Engine {
   u64 rank_rows = 0;    // rows a rank may name (n, or the arena capacity)
   // Long-run split (runs.cuh): allowed by suffix_sort, on once runs were
   // found and laid out.  The host vectors back the uploads until the build ends.
+  // Plane checksums (SUFGPU_FLAG_PLANE_CRC, single builds): CRC-32 of each
+  // plane's bytes as copied out, into st.plane_crc.
+  bool want_crc = false;
   bool allow_runs = false;
   bool runs_on = false;
   u32 run_count = 0;
@@ -490,6 +497,60 @@ struct Engine {
     last_tiles = tiles.back();
   }
   u32 last_tiles = 0;
+
+  // ---- CRC-32 (zlib's crc32(crc_in, data, bytes)) of device memory: the
+  // bytes before the first 16-byte boundary on the host (the chunk kernel
+  // loads 16-byte vectors), full 16 KiB chunks on the device (crc32.cuh)
+  // folded to one remainder, the tail on the host.  scratch holds
+  // 2 * ceil(bytes / 16 KiB) words.
+  u32 crc32_device(const void* data, u64 bytes, u32 crc_in, u32* scratch) {
+    static const std::vector<u32> table = [] {
+      std::vector<u32> t(256);
+      for (u32 i = 0; i < 256; ++i) t[i] = crc_table_entry(i);
+      return t;
+    }();
+    const u8* p = static_cast<const u8*>(data);
+    u32 state = crc_in ^ 0xffffffffu;
+    const u64 head = std::min<u64>(bytes, (16 - (reinterpret_cast<uintptr_t>(p) & 15)) & 15);
+    if (head) {
+      u8 host[16];
+      SG_CUDA(cudaMemcpyAsync(host, p, head, cudaMemcpyDefault, c.stream));
+      sync();
+      for (u64 i = 0; i < head; ++i) state = table[(state ^ host[i]) & 0xffu] ^ (state >> 8);
+      p += head;
+      bytes -= head;
+    }
+    const u64 full = bytes / kCrcChunk;
+    if (full) {
+      launch("crc32", full * kCrcChunk, crc_chunks_kernel, std::min<u64>(full, u64(c.sm_count) * 8),
+             kCrcBlock, 0, p, full, scratch);
+      u32* in = scratch;
+      u32* out = scratch + full;
+      u64 count = full, width = kCrcChunk, last = kCrcChunk;
+      while (count > 1) {
+        launch("crc32_fold", count * 4, crc_fold_kernel, grid_stride_blocks((count + 1) / 2, 256),
+               256, 0, static_cast<const u32*>(in), count, width, last,
+               crc_shift_factor(width), out);
+        last = (count & 1) ? last : width + last;
+        width *= 2;
+        count = (count + 1) / 2;
+        std::swap(in, out);
+      }
+      SG_CUDA(cudaMemcpyAsync(c.host_scalars + 30, in, 4, cudaMemcpyDeviceToHost, c.stream));
+      sync();
+      u32 raw = 0;
+      std::memcpy(&raw, c.host_scalars + 30, 4);
+      state = crc_mulmod(state, crc_shift_factor(full * kCrcChunk)) ^ raw;
+    }
+    const u64 tail = bytes - full * kCrcChunk;
+    if (tail) {
+      std::vector<u8> host(tail);
+      SG_CUDA(cudaMemcpyAsync(host.data(), p + full * kCrcChunk, tail, cudaMemcpyDefault, c.stream));
+      sync();
+      for (u8 b : host) state = table[(state ^ b) & 0xffu] ^ (state >> 8);
+    }
+    return state ^ 0xffffffffu;
+  }
 
   // ---- Long runs of one symbol: find them, pair starts with ends and lay out
   // their sub-groups (runs.cuh).  Leaves runs_on false when there are none,
@@ -1091,6 +1152,15 @@ void copy_out(sufgpu_ctx& c, void* dst, const void* src, u64 bytes) {
   SG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, c.stream));
 }
 
+// Plane slots of Engine::plane_crc.
+enum : int { kCrcSaLow = 0, kCrcSaHigh, kCrcIsaLow, kCrcIsaHigh, kCrcLcp };
+
+// copy_out of a whole plane (device source), with its CRC-32 when asked.
+void copy_plane(Engine& e, void* dst, const void* src, u64 bytes, int slot) {
+  copy_out(e.c, dst, src, bytes);
+  if (e.want_crc && dst) e.st.plane_crc[slot] = e.crc32_device(src, bytes, 0, reinterpret_cast<u32*>(e.L.status));
+}
+
 u64 plane_bytes(u32 bits, u64 rows) { return rows * (bits == 64 ? 8 : 4); }
 u64 high_bytes(u32 bits, u64 rows) { return bits == 40 ? rows : bits == 48 ? 2 * rows : 0; }
 
@@ -1146,10 +1216,11 @@ void emit_sampled(Engine& e, const sufgpu_build_desc& d, sufgpu_outputs* outs, u
              static_cast<void*>(low), static_cast<void*>(high));
     for (u32 j = 0; j < count; ++j) {
       const u64 rows = off[j + 1] - off[j];
-      copy_out(c, isa ? outs[j].isa_low : outs[j].sa_low, low + off[j] * w, rows * w);
+      const int slot = isa ? kCrcIsaLow : kCrcSaLow;
+      copy_plane(e, isa ? outs[j].isa_low : outs[j].sa_low, low + off[j] * w, rows * w, slot);
       if (high_bytes(bits, 1)) {
-        copy_out(c, isa ? outs[j].isa_high : outs[j].sa_high, high + high_bytes(bits, off[j]),
-                 high_bytes(bits, rows));
+        copy_plane(e, isa ? outs[j].isa_high : outs[j].sa_high, high + high_bytes(bits, off[j]),
+                   high_bytes(bits, rows), slot + 1);
       }
     }
   };
@@ -1166,7 +1237,7 @@ void emit_sampled(Engine& e, const sufgpu_build_desc& d, sufgpu_outputs* outs, u
     }
     const u64 w = wide ? 8 : 4;
     for (u32 j = 0; j < count; ++j) {
-      copy_out(c, outs[j].lcp, src + off[j] * w, (off[j + 1] - off[j]) * w);
+      copy_plane(e, outs[j].lcp, src + off[j] * w, (off[j + 1] - off[j]) * w, kCrcLcp);
     }
   }
   SG_CUDA(cudaEventRecord(c.ev[5], c.stream));
@@ -1200,10 +1271,11 @@ void emit_outputs(Engine& e, const sufgpu_build_desc& d, sufgpu_outputs* outs,
       void* dst_low = isa ? outs[j].isa_low : outs[j].sa_low;
       void* dst_high = isa ? outs[j].isa_high : outs[j].sa_high;
       const u64 w = bits == 64 ? 8 : 4;
-      if (direct) copy_out(c, dst_low, values + b, rows * 4);
-      else copy_out(c, dst_low, low + b * w, rows * w);
+      const int slot = isa ? kCrcIsaLow : kCrcSaLow;
+      if (direct) copy_plane(e, dst_low, values + b, rows * 4, slot);
+      else copy_plane(e, dst_low, low + b * w, rows * w, slot);
       if (!direct && high_bytes(bits, 1)) {
-        copy_out(c, dst_high, high + b * high_bytes(bits, 1), high_bytes(bits, rows));
+        copy_plane(e, dst_high, high + b * high_bytes(bits, 1), high_bytes(bits, rows), slot + 1);
       }
     }
   };
@@ -1231,7 +1303,7 @@ void emit_outputs(Engine& e, const sufgpu_build_desc& d, sufgpu_outputs* outs,
       const u64 w = wide ? 8 : 4;
       for (u32 j = 0; j < count; ++j) {
         const u64 b = e.begin[j], rows = e.begin[j + 1] - e.begin[j];
-        copy_out(c, outs[j].lcp, src + b * w, rows * w);
+        copy_plane(e, outs[j].lcp, src + b * w, rows * w, kCrcLcp);
       }
     } else {
       const bool wide = d.lcp_encoding == SUFGPU_LCP_BYTE64;
@@ -1240,7 +1312,7 @@ void emit_outputs(Engine& e, const sufgpu_build_desc& d, sufgpu_outputs* outs,
                static_cast<const u32*>(ph.lcp), n, primary);
       for (u32 j = 0; j < count; ++j) {
         const u64 b = e.begin[j], rows = e.begin[j + 1] - e.begin[j];
-        copy_out(c, outs[j].lcp, primary + b, rows);
+        copy_plane(e, outs[j].lcp, primary + b, rows, kCrcLcp);
       }
       // Anchors into x/y (8n bytes): a filter of the sorted long rows.
       const u64 w = wide ? 8 : 4;
@@ -1399,6 +1471,7 @@ void sufgpu_destroy(sufgpu_ctx* ctx) {
     if (ev) cudaEventDestroy(ev);
   }
   ctx->drop_round_graphs();
+  if (ctx->crc_scratch) cudaFree(ctx->crc_scratch);
   if (ctx->host_scalars) cudaFreeHost(ctx->host_scalars);
   if (ctx->host_small) cudaFreeHost(ctx->host_small);
   if (ctx->arena.base) {
@@ -1414,6 +1487,29 @@ const char* sufgpu_last_error(const sufgpu_ctx* ctx) {
 }
 
 uint64_t sufgpu_max_symbols(void) { return 0xffffffffull; }
+
+sufgpu_status sufgpu_crc32_device(sufgpu_ctx* ctx, const void* data, uint64_t bytes,
+                                  uint32_t crc_in, uint32_t* crc_out) {
+  if (!ctx || !crc_out || (bytes && !data)) return SUFGPU_INVALID_INPUT;
+  try {
+    SG_CUDA(cudaSetDevice(ctx->device));
+    const u64 words = 2 * (bytes / kCrcChunk + 1);
+    if (ctx->crc_scratch_words < words) {
+      if (ctx->crc_scratch) cudaFree(ctx->crc_scratch);
+      ctx->crc_scratch = nullptr;
+      ctx->crc_scratch_words = 0;
+      SG_CUDA(cudaMalloc(&ctx->crc_scratch, words * 4));
+      ctx->crc_scratch_words = words;
+    }
+    Engine e(*ctx);
+    *crc_out = e.crc32_device(data, bytes, crc_in, ctx->crc_scratch);
+    return SUFGPU_OK;
+  } catch (const CudaError& err) {
+    cudaGetLastError();
+    return fail(ctx, SUFGPU_BUILD_FAILURE,
+                std::string("CUDA error in ") + err.what + ": " + cudaGetErrorString(err.code));
+  }
+}
 
 uint32_t sufgpu_prefix_select_k(uint64_t suffix_count, uint64_t resident_core_bytes) {
   // FastPrefixIndexOptions defaults: k in [8, 10], 2500 basis points of the
@@ -1547,6 +1643,7 @@ sufgpu_status sufgpu_build(sufgpu_ctx* ctx, const uint8_t* text, uint64_t n,
     e.zero(e.L.flags, sizeof(DeviceFlags));
     SG_CUDA(cudaMemcpyAsync(e.L.text, text, n, cudaMemcpyDefault, ctx->stream));
     e.zero(e.L.text + n, kTextPad);
+    e.want_crc = (desc->flags & SUFGPU_FLAG_PLANE_CRC) != 0;
     sufgpu_outputs o = *out;
     run_build(e, *desc, &o, anchors, 1);
     e.st.kernel_launches = ctx->launches;
@@ -1601,6 +1698,9 @@ extern "C" sufgpu_status sufgpu_build_batch(sufgpu_ctx* ctx, sufgpu_instance* in
   }
   if (desc->prefix_k) {
     return fail(ctx, SUFGPU_INVALID_INPUT, "the prefix directory is built for single references");
+  }
+  if (desc->flags & SUFGPU_FLAG_PLANE_CRC) {
+    return fail(ctx, SUFGPU_INVALID_INPUT, "plane checksums are kept for single builds");
   }
   std::vector<u64> begin(count + 1, 0);
   for (u32 j = 0; j < count; ++j) {
