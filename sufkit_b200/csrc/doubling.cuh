@@ -254,6 +254,16 @@ seed_rank_kernel(const u64* __restrict__ keys, u32* __restrict__ sa,
       act += active_row[i];
     }
   }
+  // Positions of this thread's rows, loaded before the scans so that their
+  // latency overlaps the look-back (packed keys carry them in the low bits).
+  const u64 local_mask = packed_shift ? (1ull << packed_shift) - 1 : 0;
+  u32 pos[kScanItems];
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const u64 r = row0 + i;
+    pos[i] = 0;
+    if (r < n) pos[i] = packed_shift ? static_cast<u32>(keys[r] & local_mask) : sa[r];
+  }
   u64 agg_max, agg_sum;
   const u64 excl_max = block_exclusive_scan<kScanBlock>(head_max, MaxOp{}, warp_smem, &agg_max);
   const u64 excl_sum = block_exclusive_scan<kScanBlock>(act, SumOp{}, warp_smem, &agg_sum);
@@ -268,7 +278,6 @@ seed_rank_kernel(const u64* __restrict__ keys, u32* __restrict__ sa,
   __syncthreads();
   u64 running_max = tile_prefix[0] > excl_max ? tile_prefix[0] : excl_max;
   u64 out = tile_prefix[1] + excl_sum;
-  const u64 local_mask = packed_shift ? (1ull << packed_shift) - 1 : 0;
 #pragma unroll
   for (int i = 0; i < kScanItems; ++i) {
     const u64 r = row0 + i;
@@ -277,10 +286,10 @@ seed_rank_kernel(const u64* __restrict__ keys, u32* __restrict__ sa,
       u32 p;
       if (packed_shift) {
         cur.locate(segs.begin, segs.count, r);
-        p = static_cast<u32>(cur.lo + (keys[r] & local_mask));
+        p = static_cast<u32>(cur.lo + pos[i]);
         sa[r] = p;
       } else {
-        p = sa[r];
+        p = pos[i];
       }
       if (p >= n) {
         flag_error(flags, kErrBounds);
@@ -497,6 +506,22 @@ round_rank_kernel(const u64* __restrict__ ckey, const u32* __restrict__ cval,
       if (!(head[i] && head[i + 1])) ++keep;
     }
   }
+  // Values and group tables of this thread's rows, loaded before the scans
+  // so that their latency overlaps the look-back.
+  u32 val[kScanItems], g_head[kScanItems], g_first[kScanItems];
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const u64 a = a0 + i;
+    const u64 dense = k[i + 1] >> second_bits;
+    val[i] = 0;
+    g_head[i] = 0;
+    g_first[i] = 0;
+    if (a < count && dense < group_cap) {
+      val[i] = cval[a];
+      g_head[i] = ghead[dense];
+      g_first[i] = gstart[dense];
+    }
+  }
   u64 agg_max, agg_sum;
   const u64 excl_max = block_exclusive_scan<kScanBlock>(head_max, MaxOp{}, warp_smem, &agg_max);
   const u64 excl_sum = block_exclusive_scan<kScanBlock>(keep, SumOp{}, warp_smem, &agg_sum);
@@ -521,9 +546,9 @@ round_rank_kernel(const u64* __restrict__ ckey, const u32* __restrict__ cval,
         flag_error(flags, kErrBounds);
         continue;
       }
-      const u32 group_head = ghead[dense];
-      const u32 group_first = gstart[dense];
-      const u32 p = cval[a];
+      const u32 group_head = g_head[i];
+      const u32 group_first = g_first[i];
+      const u32 p = val[i];
       const u64 row = group_head + (a - group_first);
       if (row >= rows || p >= rows || a < group_first) {
         flag_error(flags, kErrBounds);
