@@ -203,7 +203,7 @@ seed_rank_kernel(const u64* __restrict__ keys, u32* __restrict__ sa,
                  u64* __restrict__ pairs, u32* __restrict__ lcp,
                  u32* __restrict__ active, u64* status_max, u64* status_sum,
                  u32* tile_counter, u64* active_count, DeviceFlags* flags,
-                 u32 run_keys = 0) {
+                 u32 run_keys = 0, u32 local_pairs = 0) {
   __shared__ u64 warp_smem[kScanBlock / 32];
   __shared__ u64 tile_prefix[2];
   __shared__ u32 tile_slot;
@@ -295,7 +295,14 @@ seed_rank_kernel(const u64* __restrict__ keys, u32* __restrict__ sa,
         flag_error(flags, kErrBounds);
         continue;
       }
-      pairs[r] = (static_cast<u64>(p) << 32) | static_cast<u32>(running_max);
+      // With local_pairs the pair carries the instance-local position (the
+      // batched rank write groups by windows of each instance).
+      u64 pair_pos = p;
+      if (local_pairs) {
+        cur.locate(segs.begin, segs.count, r);
+        pair_pos = p - cur.lo;
+      }
+      pairs[r] = (pair_pos << 32) | static_cast<u32>(running_max);
       if (active_row[i]) active[out++] = p;
     }
   }
@@ -373,6 +380,43 @@ struct RoundState {
 
 __device__ __forceinline__ bool round_skipped(const RoundState& rs) {
   return rs.abort && *rs.abort;
+}
+
+// The same window write per instance: pairs carry instance-local positions
+// and are grouped by 2048-position window inside each instance's rows, so
+// instance j's window w is rows begin[j] + [w * 2048, min((w + 1) * 2048, n_j)).
+// wbegin[j] = windows of the instances before j (count + 1 entries).
+static __global__ void __launch_bounds__(256)
+segment_window_scatter_kernel(const u64* __restrict__ pairs, Segments segs,
+                              const u64* __restrict__ wbegin, u32* __restrict__ rank,
+                              DeviceFlags* flags) {
+  __shared__ u32 window[kWindow];
+  u32 lo = 0, hi = segs.count;  // instance j with wbegin[j] <= blockIdx.x < wbegin[j + 1]
+  while (hi - lo > 1) {
+    const u32 mid = (lo + hi) >> 1;
+    if (wbegin[mid] <= blockIdx.x) lo = mid;
+    else hi = mid;
+  }
+  const u64 w = blockIdx.x - wbegin[lo];
+  const u64 base = segs.begin[lo];
+  const u64 len = segs.begin[lo + 1] - base;
+  const u64 first = w * kWindow;
+  if (first >= len) {
+    flag_error(flags, kErrBounds);
+    return;
+  }
+  const u32 count = static_cast<u32>(len - first < kWindow ? len - first : kWindow);
+  for (u32 i = threadIdx.x; i < count; i += 256) {
+    const u64 v = pairs[base + first + i];
+    const u64 local = v >> 32;
+    if ((local >> kWindowBits) != w || (local & (kWindow - 1)) >= count) {
+      flag_error(flags, kErrBounds);  // not a permutation
+      continue;
+    }
+    window[local & (kWindow - 1)] = static_cast<u32>(v);
+  }
+  __syncthreads();
+  for (u32 i = threadIdx.x; i < count; i += 256) rank[base + first + i] = window[i];
 }
 
 // Round step 1: composite keys for the active list.  counters: *group_count

@@ -774,12 +774,37 @@ struct Engine {
     launch("seed_rank", n * 24, seed_rank_kernel, scan_tiles, kScanBlock, 0,
            static_cast<const u64*>(keys), sa, n, segments(), packed_shift, bits, symbols,
            pairs, L.lcp, L.x, status_max, status_sum, L.counters, L.scalars + 0, L.flags,
-           runs_on ? 1u : 0u);
+           runs_on ? 1u : 0u, segs > 1 ? 1u : 0u);
     // rank[SA[r]] = head: group the pairs by 2048-position window (keys-only
     // passes over the position's high bits), then one coalesced window write.
+    // A batch groups instance-local positions inside each instance (a pass
+    // per 8 bits of the longest instance above 11, not of the whole batch).
     const u32 pos_bits = std::max<u32>(1, bits_for(n - 1));
     u64* grouped = pairs;
-    if (pos_bits > kWindowBits) {
+    if (segs > 1) {
+      u64 longest = 1;
+      std::vector<u64> wbegin(segs + 1, 0);
+      for (u32 j = 0; j < segs; ++j) {
+        const u64 len = begin[j + 1] - begin[j];
+        longest = std::max(longest, len);
+        wbegin[j + 1] = wbegin[j] + (len + kWindow - 1) / kWindow;
+      }
+      const u32 local_bits = std::max<u32>(1, bits_for(longest - 1));
+      if (local_bits > kWindowBits) {
+        u64* other_keys = pairs == L.k0 ? L.k1 : L.k0;
+        const bool sw = radix_sort("rank_group", pairs, nullptr, other_keys, nullptr, L.seg_begin,
+                                   L.seg_tiles, segs, seed_tiles, n, 32 + kWindowBits,
+                                   32 + local_bits, false);
+        grouped = sw ? other_keys : pairs;
+      }
+      sync();
+      std::memcpy(c.host_small, wbegin.data(), (segs + 1) * 8);
+      SG_CUDA(cudaMemcpyAsync(L.digit_start, c.host_small, (segs + 1) * 8, cudaMemcpyHostToDevice,
+                              c.stream));
+      launch("window_scatter", n * 12, segment_window_scatter_kernel, wbegin[segs], 256, 0,
+             static_cast<const u64*>(grouped), segments(), static_cast<const u64*>(L.digit_start),
+             L.rank, L.flags);
+    } else if (pos_bits > kWindowBits) {
       const u64 b2[2] = {0, n};
       const u32 t = static_cast<u32>((n + c.tune.sort_tile - 1) / c.tune.sort_tile);
       const u32 t2[2] = {0, t};
@@ -793,8 +818,10 @@ struct Engine {
                                  L.sort_tiles, 1, t, n, 32 + kWindowBits, 32 + pos_bits, false);
       grouped = sw ? other_keys : pairs;
     }
-    launch("window_scatter", n * 12, window_scatter_kernel, (n + kWindow - 1) / kWindow, 256, 0,
-           static_cast<const u64*>(grouped), n, L.rank, L.flags);
+    if (segs == 1) {
+      launch("window_scatter", n * 12, window_scatter_kernel, (n + kWindow - 1) / kWindow, 256, 0,
+             static_cast<const u64*>(grouped), n, L.rank, L.flags);
+    }
     u64 active = read_scalar(0);
     if (runs_on) {
       // Members of long runs: sub-group rows and ranks, and the rows in
