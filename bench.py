@@ -331,7 +331,19 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    texts, desc = workload(args.workload, args.scale, args.count)
+    sharded = args.workload == "batched" and world > 1 and args.impl == "ours"
+    all_symbols = None
+    if sharded:
+        # N GPUs build a collection of N x count references, each its
+        # bin-packed share (no collective on the data path).
+        from sufkit_b200 import shard
+        _, texts = shard.collection_share(args.count * world, world, rank, args.scale)
+        desc = (f"batched uneven collection sharded over {world} GPUs: {args.count * world} "
+                "bacterial-like references (log-normal sizes, median 4 Mbp, clipped 0.5-12 Mbp, "
+                "GC 30-70%, 1-8 contigs), each GPU its bin-packed share of about "
+                f"{args.count}; SA + raw LCP32 per reference, 32-bit")
+    else:
+        texts, desc = workload(args.workload, args.scale, args.count)
     if args.scale != 1.0:
         desc += f" (scaled x{args.scale})"
 
@@ -361,6 +373,8 @@ def main():
 
     # Device-resident inputs and outputs.
     n_total = sum(int(t.size) for t in texts)
+    if sharded:
+        all_symbols = int(shard.sum_over_ranks(n_total, dist, dev))
     d_texts = [torch.from_numpy(t).to(dev) for t in texts]
     lcp_dtype = torch.uint8 if lcp_enc == sg.LcpEncoding.BYTE32 else torch.int32
     d_out = [{"sa_low": torch.empty(t.size, dtype=torch.int32, device=dev),
@@ -452,12 +466,12 @@ def main():
                   "batched_over_one_at_a_time": (sec / (device_seconds / args.steps)),
                   "batches": len(batches), "references": len(texts)}
 
-    step_seconds = device_seconds / args.steps
-    if dist is not None:
-        t = torch.tensor([step_seconds], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        step_seconds = float(t.item())
-    value = world * n_total / step_seconds / 1e9
+    from sufkit_b200 import shard
+    step_seconds = shard.max_over_ranks(device_seconds / args.steps, dist, dev)
+    # Replicas: every rank builds the whole workload; sharded: the ranks
+    # together build the collection once.
+    job_symbols = all_symbols if sharded else world * n_total
+    value = job_symbols / step_seconds / 1e9
 
     # End to end through the C ABI with pinned host buffers.
     e2e = None
@@ -488,12 +502,8 @@ def main():
         t0 = time.perf_counter()
         for _ in range(args.steps):
             e2e_step(ctx, pinned_text, host_out, isa_bits, lcp_enc, sa_bits)
-        e2e_sec = (time.perf_counter() - t0) / args.steps
-        if dist is not None:
-            t = torch.tensor([e2e_sec], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_sec = float(t.item())
-        e2e = {"value": world * n_total / e2e_sec / 1e9, "unit": "Gsym/s",
+        e2e_sec = shard.max_over_ranks((time.perf_counter() - t0) / args.steps, dist, dev)
+        e2e = {"value": job_symbols / e2e_sec / 1e9, "unit": "Gsym/s",
                "h2d_bytes_per_step": n_total, "d2h_bytes_per_step": d2h,
                "ms_per_step": e2e_sec * 1e3}
 
@@ -542,9 +552,10 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_seconds * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "u32", "data": "synthetic",
-            "config": {"workload": desc, "symbols": n_total,
+            "config": {"workload": desc, "symbols": n_total, "job_symbols": job_symbols,
                        "l2": "flushed between steps (256 MiB device write)",
-                       "parallelism": f"{world} independent replica(s)",
+                       "parallelism": (f"{world} GPUs, bin-packed shares" if sharded
+                                       else f"{world} independent replica(s)"),
                        "timing": "device time per build (library CUDA events), "
                                  "max over ranks", "wall_s": wall,
                        "build_roofline": whole, "batched": single, "kernels": kernels},

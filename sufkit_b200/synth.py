@@ -207,6 +207,25 @@ def uneven_collection(count: int = 1024, scale: float = 1.0,
     return refs
 
 
+def uneven_sizes(count: int, scale: float = 1.0, seed: Optional[int] = None) -> list[int]:
+    """Lengths of a bacterial collection of `count` references (log-normal,
+    median 4 Mbp, clipped to 0.5-12 Mbp), without generating the sequences."""
+    rng = np.random.default_rng(BASE_SEED + 13 if seed is None else seed)
+    sizes = np.clip(rng.lognormal(np.log(4e6), 0.5, size=count), 0.5e6, 12e6) * scale
+    return [max(64, int(x)) for x in sizes]
+
+
+def uneven_reference(index: int, total: int, seed: Optional[int] = None) -> Reference:
+    """Reference `index` of such a collection with its own random stream, so
+    that any subset (one GPU's share) is generated without the rest: GC
+    U(30%,70%), 1-8 contigs."""
+    rng = np.random.default_rng([BASE_SEED + 13 if seed is None else seed, index])
+    gc = rng.uniform(0.30, 0.70)
+    k = int(rng.integers(1, 9))
+    lengths = _scaled_lengths(rng.uniform(0.2, 1.0, size=k), total)
+    return Reference(_split(_bases(rng, total, gc), lengths))
+
+
 def strain_collection(copies: int = 50, genome_bp: int = 2_000_000,
                       rng: Optional[np.random.Generator] = None) -> Reference:
     """50 copies of one random genome at 0.1% SNP + 0.01% indel divergence."""
