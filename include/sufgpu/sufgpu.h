@@ -127,13 +127,13 @@ typedef struct sufgpu_build_stats {
   uint32_t kernel_launches;   /* kernels launched by this call */
   uint32_t long_runs;         /* single-symbol runs split directly after the seed */
   uint32_t seg_sort_fallbacks;/* rounds whose groups did not fit the shared-memory sort */
-  uint32_t reserved;
+  uint32_t seed_rare_rows;    /* two-bit seed: rows placed from the rare list */
   uint64_t prefix_kmers;      /* rows with a canonical k-mer (FastPrefixIndex::IndexedKmers) */
   uint64_t prefix_entries;    /* k-mers present (FastPrefixIndex::NonemptyEntries) */
   /* SUFGPU_FLAG_PLANE_CRC: CRC-32 of sa_low, sa_high, isa_low, isa_high, lcp
    * as written (0 for planes not written). */
   uint32_t plane_crc[5];
-  uint32_t reserved2;
+  uint32_t seed_code_bits;    /* bits per symbol of the seed sort key (2: two-bit seed) */
 } sufgpu_build_stats;
 
 typedef struct sufgpu_ctx sufgpu_ctx;
@@ -235,7 +235,12 @@ SUFGPU_API sufgpu_status sufgpu_profile_entry(const sufgpu_ctx *ctx, uint32_t in
  *   "graph_rounds"  1 = a layout built before runs its rounds as a cached
  *                   CUDA graph of two rounds (one host synchronization per
  *                   pair), 0 = the host drives every round.  Builds with the
- *                   per-kernel profile on are always host-driven.
+ *                   per-kernel profile on are always host-driven;
+ *   "two_bit_seed"  1 = a single text of four consecutive byte values (A, C,
+ *                   G, T) and few others sorts 2-bit seed keys, the windows
+ *                   that hold another symbol placed exactly from a side
+ *                   list; 0 = keys of the text's own code width always;
+ *   "two_bit_min"   smallest text (symbols) that uses the two-bit seed.
  * Results are identical for every setting; only speed changes. */
 SUFGPU_API sufgpu_status sufgpu_set_tuning(sufgpu_ctx *ctx, const char *key, int64_t value);
 

@@ -91,13 +91,13 @@ class _Stats(ctypes.Structure):
                 ("irreducible_long", ctypes.c_uint64),
                 ("anchors", ctypes.c_uint64), ("kernel_launches", ctypes.c_uint32),
                 ("long_runs", ctypes.c_uint32), ("seg_sort_fallbacks", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32), ("prefix_kmers", ctypes.c_uint64),
+                ("seed_rare_rows", ctypes.c_uint32), ("prefix_kmers", ctypes.c_uint64),
                 ("prefix_entries", ctypes.c_uint64), ("plane_crc", ctypes.c_uint32 * 5),
-                ("reserved2", ctypes.c_uint32)]
+                ("seed_code_bits", ctypes.c_uint32)]
 
     def as_dict(self) -> dict:
         d = {name: getattr(self, name) for name, _ in self._fields_
-             if name not in ("reserved", "reserved2", "plane_crc")}
+             if name != "plane_crc"}
         d["plane_crc"] = dict(zip(("sa_low", "sa_high", "isa_low", "isa_high", "lcp"),
                                   list(self.plane_crc)))
         return d

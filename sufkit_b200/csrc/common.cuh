@@ -139,6 +139,19 @@ __device__ __forceinline__ u64 warp_lookback(u64* status, u32 tile,
   return exclusive;
 }
 
+// Warp-aggregated append of one item per participating lane (all 32 lanes
+// call it): the lane's slot in the list whose length *counter holds.
+__device__ __forceinline__ u64 warp_append(u64* counter, bool take) {
+  const u32 mask = __ballot_sync(0xffffffffu, take);
+  if (!mask) return 0;
+  const u32 lane = threadIdx.x & 31;
+  const u32 leader = __ffs(mask) - 1;
+  u64 base = 0;
+  if (lane == leader) base = atomicAdd(reinterpret_cast<unsigned long long*>(counter), __popc(mask));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  return base + __popc(mask & ((1u << lane) - 1));
+}
+
 // Number of bits needed to represent values 0..v.
 __host__ __device__ __forceinline__ u32 bits_for(u64 v) {
   u32 b = 0;

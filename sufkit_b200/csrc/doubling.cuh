@@ -101,14 +101,77 @@ struct SeedSmem {
   __align__(16) u8 window[kSeedTile + kSeedHalo];
 };
 
+// Two-bit seed for texts of four consecutive regular symbols (A, C, G, T in
+// the logical text) and few others.  A window's key is the 2-bit codes of its
+// regular symbols followed by a 2-bit tag t:
+//   t = 1  every symbol regular: the codes of the whole window;
+//   t = 0  its first irregular symbol (at offset j) is below the regular ones
+//          or past the end: the codes of offsets [0, j), then all A;
+//   t = 2  that symbol is above them: the codes of [0, j), then all T;
+//   t = 3  every symbol is the largest symbol `hi` (inside a run of N).
+// The map is monotone in the windows' order, one-to-one on the t = 1 and
+// t = 3 windows, and strict between a t = 1 / t = 3 window and any other, so
+// after the sort every group of t = 1 or t = 3 keys is exact and only rows of
+// the same t = 0 / t = 2 key ("rare rows") may hold different windows in the
+// wrong order.  Their exact keys (the code-table key) go to a side list that
+// is sorted on its own; seed ranks place them from it.
+struct TwoBitSeed {
+  u32 lo = 0;         // code of the first regular symbol (regular: lo..lo+3)
+  u32 hi = 0;         // code of the largest symbol when above the regular ones
+  u64 all_hi = 0;     // exact key of a window of s x hi
+  u64* rare_key = nullptr;  // exact keys of rare rows (unordered)
+  u32* rare_pos = nullptr;
+  u64 rare_cap = 0;
+  u64* rare_count = nullptr;  // may exceed rare_cap: the host then falls back
+};
+
+// Two-bit key from the window's exact key, its regular codes k2 (2 bits per
+// symbol, 0 for irregular ones) and its irregular mask (bit s-1-k set when
+// offset k is irregular).
+__host__ __device__ __forceinline__ u64 two_bit_key(u64 exact, u64 k2, u32 irregular, u32 s,
+                                                    u32 bits, const TwoBitSeed& tb) {
+  if (irregular == 0) return (k2 << 2) | 1;
+#ifdef __CUDA_ARCH__
+  const u32 top = 31 - __clz(irregular);
+#else
+  u32 top = 31;
+  while (!((irregular >> top) & 1u)) --top;
+#endif
+  const u32 j = s - 1 - top;  // first irregular offset
+  const u32 cj = static_cast<u32>(exact >> (bits * (s - 1 - j))) & ((1u << bits) - 1);
+  const u32 tail = 2 * (s - j);
+  const u64 head = (k2 >> tail) << tail;
+  if (cj < tb.lo) return head << 2;
+  const u64 fill = (1ull << tail) - 1;
+  if (j == 0 && tb.hi && exact == tb.all_hi) return ((head | fill) << 2) | 3;
+  return ((head | fill) << 2) | 2;
+}
+
+// The same from the exact key alone (s symbols of `bits`).
+__host__ __device__ __forceinline__ u64 two_bit_of_exact(u64 exact, u32 s, u32 bits,
+                                                         const TwoBitSeed& tb) {
+  u64 k2 = 0;
+  u32 irregular = 0;
+  for (u32 k = 0; k < s; ++k) {
+    const u32 c = static_cast<u32>(exact >> (bits * (s - 1 - k))) & ((1u << bits) - 1);
+    const bool reg = c >= tb.lo && c < tb.lo + 4;
+    k2 = (k2 << 2) | (reg ? c - tb.lo : 0u);
+    irregular = (irregular << 1) | (reg ? 0u : 1u);
+  }
+  return two_bit_key(exact, k2, irregular, s, bits, tb);
+}
+
 // packed_shift > 0 selects the packed seed: key = (prefix << packed_shift) |
 // instance-local index (no value array); histograms then cover the passes
 // over bits [packed_shift, packed_shift + 8*passes).
+// kTwoBit: sort keys are two-bit keys (one instance); rare rows also append
+// (exact key, position) to tb's list.
+template <bool kTwoBit>
 static __global__ void __launch_bounds__(kSeedBlock)
 seed_keys_kernel(const u8* __restrict__ text, u64 n, Segments segs,
                  const u16* __restrict__ code_table, u32 bits, u32 symbols,
                  u32 passes, u32* __restrict__ hist_out, u32 packed_shift,
-                 u64* __restrict__ keys, u32* __restrict__ vals) {
+                 u64* __restrict__ keys, u32* __restrict__ vals, TwoBitSeed tb) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SeedSmem& sm = *reinterpret_cast<SeedSmem*>(smem_raw);
   sm.code[threadIdx.x] = code_table[threadIdx.x];
@@ -124,14 +187,26 @@ seed_keys_kernel(const u8* __restrict__ text, u64 n, Segments segs,
   __syncthreads();
   const u32 block_seg = segs.count == 1 ? 0 : find_segment(segs.begin, segs.count, tile_first);
   const u64 mask = symbols * bits >= 64 ? ~0ull : ((1ull << (symbols * bits)) - 1);
+  const u64 mask2 = 2 * symbols >= 64 ? ~0ull : ((1ull << (2 * symbols)) - 1);
+  const u32 smask = symbols >= 32 ? ~0u : ((1u << symbols) - 1);
   const u32 local0 = threadIdx.x * kSeedRun;
   const u32 lane = threadIdx.x & 31;
   u64 pos = tile_first + local0;
   u32 seg = segs.count == 1 ? 0 : (pos < n ? find_segment(segs.begin, segs.count, pos) : block_seg);
   u64 end = pos < n ? segs.begin[seg + 1] : n;
   u64 seg_lo = pos < n ? segs.begin[seg] : 0;
-  u64 key = 0;
+  u64 key = 0, k2 = 0;
+  u32 irregular = 0;
   bool fresh = true;
+  // Pushes the code of one more symbol into the window state.
+  auto push = [&](u32 c) {
+    key = ((key << bits) | c) & mask;
+    if (kTwoBit) {
+      const bool reg = c >= tb.lo && c < tb.lo + 4;
+      k2 = ((k2 << 2) | (reg ? c - tb.lo : 0u)) & mask2;
+      irregular = ((irregular << 1) | (reg ? 0u : 1u)) & smask;
+    }
+  };
   for (int r = 0; r < kSeedRun; ++r, ++pos) {
     const bool valid = pos < n;
     if (valid && pos >= end) {  // crossed into the next instance
@@ -141,26 +216,37 @@ seed_keys_kernel(const u8* __restrict__ text, u64 n, Segments segs,
       fresh = true;
     }
     const u32 local = local0 + r;
+    u64 sort_key = 0;
+    bool rare = false;
     if (valid) {
       if (fresh) {
-        key = 0;
-        for (u32 t = 0; t < symbols; ++t) {
-          const u32 c = pos + t < end ? sm.code[sm.window[local + t]] : 0u;
-          key = (key << bits) | c;
-        }
+        key = k2 = 0;
+        irregular = 0;
+        for (u32 t = 0; t < symbols; ++t) push(pos + t < end ? sm.code[sm.window[local + t]] : 0u);
         fresh = false;
       } else {
         const u64 q = pos + symbols - 1;
-        const u32 c = q < end ? sm.code[sm.window[local + symbols - 1]] : 0u;
-        key = ((key << bits) | c) & mask;
+        push(q < end ? sm.code[sm.window[local + symbols - 1]] : 0u);
       }
-      sm.keys[local] = packed_shift ? (key << packed_shift) | (pos - seg_lo) : key;
+      sort_key = key;
+      if (kTwoBit) {
+        sort_key = two_bit_key(key, k2, irregular, symbols, bits, tb);
+        rare = (sort_key & 1) == 0;
+      }
+      sm.keys[local] = packed_shift ? (sort_key << packed_shift) | (pos - seg_lo) : sort_key;
+    }
+    if (kTwoBit) {
+      const u64 slot = warp_append(tb.rare_count, rare);
+      if (rare && slot < tb.rare_cap) {
+        tb.rare_key[slot] = key;
+        tb.rare_pos[slot] = static_cast<u32>(pos);
+      }
     }
     // Histogram of every pass; a warp whose lanes agree adds once.
     const bool mine = valid && seg == block_seg;
     const bool all_mine = __all_sync(0xffffffffu, mine);
     for (u32 p = 0; p < passes; ++p) {
-      const u32 digit = static_cast<u32>((key >> (p * 8)) & 0xff);
+      const u32 digit = static_cast<u32>((sort_key >> (p * 8)) & 0xff);
       const u32 d0 = __shfl_sync(0xffffffffu, digit, 0);
       if (all_mine && __all_sync(0xffffffffu, digit == d0)) {
         if (lane == 0) atomicAdd(&sm.hist[p][d0], 32u);
@@ -195,8 +281,40 @@ seed_keys_kernel(const u8* __restrict__ text, u64 n, Segments segs,
 // resolved from the text later (their LCP is at least the seed length).
 constexpr u32 kLcpUnknown = 0xffffffffu;
 
+// Rare rows of a two-bit seed (one instance), sorted by their exact keys:
+// positions and, in the same order (so ascending too), their two-bit keys.
+struct RareRows {
+  const u64* key = nullptr;
+  const u32* pos = nullptr;
+  const u64* k2 = nullptr;
+  u64 count = 0;
+  const u8* text = nullptr;
+};
+
+// First index in v[lo, hi) with v[i] >= x (hi if none).
+__device__ __forceinline__ u64 lower_bound_u64(const u64* v, u64 lo, u64 hi, u64 x) {
+  while (lo < hi) {
+    const u64 mid = (lo + hi) >> 1;
+    if (v[mid] < x) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Common prefix of the s-symbol windows at p != q of a text of n symbols.
+__device__ __forceinline__ u32 window_lcp(const u8* text, u64 n, u64 p, u64 q, u32 s) {
+  u32 l = 0;
+  while (l < s && p + l < n && q + l < n && text[p + l] == text[q + l]) ++l;
+  return l;
+}
+
 // Ranks leave as (position << 32 | head row) words in row order (pairs), so
 // the write is coalesced; the window scatter below turns them into rank[].
+// kTwoBit: keys are two-bit keys (one instance).  Groups of t = 1 / t = 3
+// keys are exact and handled here; rows of t = 0 / t = 2 keys (rare rows) get
+// placeholder pairs and SA entries, no LCP (nor the row after them), and stay
+// off the active list: rare_place_kernel and rare_active_kernel finish them.
+template <bool kTwoBit>
 static __global__ void __launch_bounds__(kScanBlock)
 seed_rank_kernel(const u64* __restrict__ keys, u32* __restrict__ sa,
                  u64 n, Segments segs, u32 packed_shift, u32 bits, u32 symbols,
@@ -219,7 +337,7 @@ seed_rank_kernel(const u64* __restrict__ keys, u32* __restrict__ sa,
   }
   SegCursor cur;
   bool head[kScanItems + 1];
-  const u32 unused_top = 64 - bits * symbols;
+  const u32 unused_top = kTwoBit ? 64 - (2 * symbols + 2) : 64 - bits * symbols;
 #pragma unroll
   for (int i = 0; i < kScanItems + 1; ++i) {
     const u64 r = row0 + i;
@@ -231,15 +349,25 @@ seed_rank_kernel(const u64* __restrict__ keys, u32* __restrict__ sa,
     head[i] = start || k[i + 1] != k[i];
     if (i < kScanItems && r < n) {
       u32 v = kLcpUnknown;
-      if (start) v = 0;
-      else if (head[i]) v = (static_cast<u32>(__clzll(static_cast<long long>(k[i + 1] ^ k[i]))) - unused_top) / bits;
-      lcp[r] = v;
+      bool write = true;
+      const u32 x = static_cast<u32>(__clzll(static_cast<long long>(k[i + 1] ^ k[i])));
+      if (start) {
+        v = 0;
+      } else if (kTwoBit) {
+        const u32 t = static_cast<u32>(k[i + 1] & 3), tp = static_cast<u32>(k[i] & 3);
+        if (!(t & 1) || (head[i] && !(tp & 1))) write = false;  // a rare row involved
+        else if (head[i]) v = t != tp ? 0 : (x - unused_top) / 2;
+      } else if (head[i]) {
+        v = (x - unused_top) / bits;
+      }
+      if (write) lcp[r] = v;
     }
   }
   // With run_keys set, rows whose seed key is one symbol repeated s times
   // (members of long runs) stay off the active list: the run split places
   // them (runs.cuh).
-  const u64 run_low = symbols > 1 ? (1ull << (bits * (symbols - 1))) - 1 : 0;
+  const u32 sym_bits = kTwoBit ? 2 : bits;
+  const u64 run_low = symbols > 1 ? (1ull << (sym_bits * (symbols - 1))) - 1 : 0;
   bool active_row[kScanItems];
   u64 head_max = 0;  // inclusive running max within the thread
   u32 act = 0;
@@ -249,8 +377,10 @@ seed_rank_kernel(const u64* __restrict__ keys, u32* __restrict__ sa,
     active_row[i] = false;
     if (r < n) {
       if (head[i]) head_max = r;
-      const bool run_member = run_keys && (k[i + 1] >> bits) == (k[i + 1] & run_low);
-      active_row[i] = !(head[i] && head[i + 1]) && !run_member;
+      const u64 prefix = kTwoBit ? k[i + 1] >> 2 : k[i + 1];
+      const bool rare_row = kTwoBit && !(k[i + 1] & 1);
+      const bool run_member = run_keys && !rare_row && (prefix >> sym_bits) == (prefix & run_low);
+      active_row[i] = !(head[i] && head[i + 1]) && !run_member && !rare_row;
       act += active_row[i];
     }
   }
@@ -291,6 +421,7 @@ seed_rank_kernel(const u64* __restrict__ keys, u32* __restrict__ sa,
       } else {
         p = pos[i];
       }
+      const u64 head_row = running_max;
       if (p >= n) {
         flag_error(flags, kErrBounds);
         continue;
@@ -302,12 +433,120 @@ seed_rank_kernel(const u64* __restrict__ keys, u32* __restrict__ sa,
         cur.locate(segs.begin, segs.count, r);
         pair_pos = p - cur.lo;
       }
-      pairs[r] = (pair_pos << 32) | static_cast<u32>(running_max);
+      pairs[r] = (pair_pos << 32) | static_cast<u32>(head_row);
       if (active_row[i]) active[out++] = p;
     }
   }
   const u64 tiles = (n + kScanTile - 1) / kScanTile;
   if (tile == tiles - 1 && threadIdx.x == 0) *active_count = tile_prefix[1] + agg_sum;
+}
+
+// Rare rows of a two-bit seed: entry idx of the sorted list is row g + (idx -
+// i0) of the rows sharing its two-bit key k (g = first row of k in the sorted
+// keys, i0 = first entry of k).  Writes its SA entry, its pair (position,
+// exact head row), its LCP and, for the last entry of k, the LCP of the row
+// after it.  keys: the sorted seed keys (two-bit key << packed_shift, with the
+// instance-local index below when packed).
+static __global__ void __launch_bounds__(256)
+rare_place_kernel(const u64* __restrict__ keys, u64 n, u32 packed_shift, RareRows rare,
+                  u32 bits, u32 symbols, u32* __restrict__ sa, u64* __restrict__ pairs,
+                  u32* __restrict__ lcp, DeviceFlags* flags) {
+  const u64 local_mask = packed_shift ? (1ull << packed_shift) - 1 : 0;
+  const u32 unused = 64 - bits * symbols;
+  auto row_pos = [&](u64 r) -> u32 {  // a non-rare row's position
+    return packed_shift ? static_cast<u32>(keys[r] & local_mask) : sa[r];
+  };
+  auto rare_row = [&](u64 r) { return ((keys[r] >> packed_shift) & 1) == 0; };
+  for (u64 idx = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; idx < rare.count;
+       idx += static_cast<u64>(gridDim.x) * blockDim.x) {
+    const u64 k = rare.k2[idx];
+    const u64 i0 = lower_bound_u64(rare.k2, 0, idx, k);
+    const u64 g = lower_bound_u64(keys, 0, n, k << packed_shift);
+    const u64 row = g + (idx - i0);
+    if (row >= n || (keys[row] >> packed_shift) != k) {
+      flag_error(flags, kErrBounds);
+      continue;
+    }
+    const u32 p = rare.pos[idx];
+    const u64 ek = rare.key[idx];
+    const u64 e0 = lower_bound_u64(rare.key, i0, idx, ek);
+    if (p >= n) {
+      flag_error(flags, kErrBounds);
+      continue;
+    }
+    sa[row] = p;
+    pairs[row] = (static_cast<u64>(p) << 32) | static_cast<u32>(g + (e0 - i0));
+    u32 v;
+    if (row == 0) {
+      v = 0;
+    } else if (e0 < idx) {
+      v = kLcpUnknown;  // the same window as the row before
+    } else if (idx > i0 || rare_row(row - 1)) {  // the row before is entry idx - 1
+      if (idx == 0) {
+        flag_error(flags, kErrBounds);
+        continue;
+      }
+      const u32 x = static_cast<u32>(__clzll(static_cast<long long>(ek ^ rare.key[idx - 1])));
+      v = (x - unused) / bits;
+    } else {
+      v = window_lcp(rare.text, n, p, row_pos(row - 1), symbols);
+    }
+    lcp[row] = v;
+    const bool last = idx + 1 == rare.count || rare.k2[idx + 1] != k;
+    if (last && row + 1 < n && !rare_row(row + 1)) {
+      lcp[row + 1] = window_lcp(rare.text, n, row_pos(row + 1), p, symbols);
+    }
+  }
+}
+
+// Two-bit keys of the sorted rare rows.
+static __global__ void __launch_bounds__(256)
+rare_two_bit_kernel(const u64* __restrict__ key, u64 count, u32 symbols, u32 bits,
+                    TwoBitSeed tb, u64* __restrict__ k2) {
+  for (u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
+       i += static_cast<u64>(gridDim.x) * blockDim.x) {
+    k2[i] = two_bit_of_exact(key[i], symbols, bits, tb);
+  }
+}
+
+// Rare rows whose exact window is shared (groups of two or more, contiguous in
+// the sorted list) join the active list after the *base rows seed_rank put
+// there; *total receives their number.
+static __global__ void __launch_bounds__(kScanBlock)
+rare_active_kernel(const u64* __restrict__ key, const u32* __restrict__ pos, u64 count,
+                   u32* __restrict__ active, const u64* base, u64* total, u64* status,
+                   u32* tile_counter, DeviceFlags* flags) {
+  __shared__ u64 warp_smem[kScanBlock / 32];
+  __shared__ u64 tile_prefix;
+  __shared__ u32 tile_slot;
+  const u32 tile = claim_tile(tile_counter, &tile_slot);
+  const u64 e0 = static_cast<u64>(tile) * kScanTile + threadIdx.x * kScanItems;
+  bool take[kScanItems];
+  u32 act = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const u64 e = e0 + i;
+    take[i] = false;
+    if (e < count) {
+      const u64 v = key[e];
+      take[i] = (e > 0 && key[e - 1] == v) || (e + 1 < count && key[e + 1] == v);
+      act += take[i];
+    }
+  }
+  u64 agg;
+  const u64 excl = block_exclusive_scan<kScanBlock>(act, SumOp{}, warp_smem, &agg);
+  if ((threadIdx.x >> 5) == 0) {
+    const u64 p = warp_lookback(status, tile, agg, SumOp{}, flags, 7);
+    if ((threadIdx.x & 31) == 0) tile_prefix = p;
+  }
+  __syncthreads();
+  u64 out = *base + tile_prefix + excl;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    if (take[i]) active[out++] = pos[e0 + i];
+  }
+  const u64 tiles = (count + kScanTile - 1) / kScanTile;
+  if (tile == tiles - 1 && threadIdx.x == 0) *total = tile_prefix + agg;
 }
 
 // rank[pos] = head for (pos << 32 | head) pairs grouped by 2048-position

@@ -229,6 +229,10 @@ struct Tuning {
   u32 sort_block = 256;
   // Keys per onesweep tile (2048 or 4096).
   u32 sort_tile = 4096;
+  // Two-bit seed keys for single DNA-like texts of at least two_bit_min
+  // symbols (rare symbols placed from a side list).
+  bool two_bit_seed = true;
+  u64 two_bit_min = u64(1) << 22;
 };
 
 // Overrides for builds whose longest instance has at most max_symbols symbols.
@@ -259,6 +263,11 @@ std::string apply_tuning(Tuning& t, const std::string& k, int64_t value) {
     t.graph_rounds = value != 0;
   } else if (k == "run_split") {
     t.run_split = value != 0;
+  } else if (k == "two_bit_seed") {
+    t.two_bit_seed = value != 0;
+  } else if (k == "two_bit_min") {
+    if (value < 0) return "two_bit_min must be >= 0";
+    t.two_bit_min = static_cast<u64>(value);
   } else if (k == "sort_block") {
     if (value != 256 && value != 512) return "sort_block must be 256 or 512";
     t.sort_block = static_cast<u32>(value);
@@ -362,6 +371,7 @@ struct Engine {
   // plane's bytes as copied out, into st.plane_crc.
   bool want_crc = false;
   bool allow_runs = false;
+  bool allow_two_bit = false;  // the served engine's shared arena keeps the code-table seed
   bool runs_on = false;
   u32 run_count = 0;
   u64 run_members = 0;
@@ -554,8 +564,9 @@ struct Engine {
 
   // ---- Long runs of one symbol: find them, pair starts with ends and lay out
   // their sub-groups (runs.cuh).  Leaves runs_on false when there are none,
-  // too many, or the seed is too short for the split to pay.
-  void plan_runs(u32 s) {
+  // too many, or the seed is too short for the split to pay.  With `keep`,
+  // runs of the other byte values are left to the rounds.
+  void plan_runs(u32 s, const bool* keep = nullptr) {
     runs_on = false;
     run_index = RunIndex{};
     if (!allow_runs || !c.tune.run_split || s < 8 || n < 2 * u64(s)) return;
@@ -566,7 +577,7 @@ struct Engine {
     SG_CUDA(cudaMemcpyAsync(c.host_scalars + 8, L.scalars + 8, 16, cudaMemcpyDeviceToHost,
                             c.stream));
     sync();
-    const u64 count = c.host_scalars[8];
+    u64 count = c.host_scalars[8];
     if (count != c.host_scalars[9]) {
       throw BuildError{SUFGPU_BUILD_FAILURE, "long-run starts and ends do not pair"};
     }
@@ -579,6 +590,19 @@ struct Engine {
     sync();
     std::sort(starts.begin(), starts.end());
     std::sort(ends.begin(), ends.end());
+    if (keep) {  // starts and ends pair by rank (runs do not overlap)
+      u64 kept = 0;
+      for (u64 i = 0; i < count; ++i) {
+        if (!keep[starts[i] & 0xff]) continue;
+        starts[kept] = starts[i];
+        ends[kept] = ends[i];
+        ++kept;
+      }
+      count = kept;
+      starts.resize(count);
+      ends.resize(count);
+      if (count == 0) return;
+    }
     // Runs in position order; key (instance, symbol, class) names the class.
     std::vector<u64> key(count);
     std::vector<u32> len(count);
@@ -691,18 +715,16 @@ struct Engine {
     u32 sigma = 0;
     for (int b = 0; b < 256; ++b) code[b] = counts[b] ? static_cast<u16>(++sigma) : 0;
     const u32 bits = std::max<u32>(1, bits_for(sigma));
-    u32 symbols = 64 / bits;
     u64 longest = 1;
     for (u32 j = 0; j < segs; ++j) longest = std::max<u64>(longest, begin[j + 1] - begin[j]);
-    if (c.tune.seed_symbols) {
-      symbols = std::min(symbols, c.tune.seed_symbols);
-    } else {
-      // Enough symbols that two seed keys of one instance rarely collide by
-      // chance, log2(longest) / H + 2.5 with H the text's entropy in bits per
-      // symbol, plus one per doubling beyond 2^27 symbols (larger genomes
-      // hold more repeat copies), rounded up to whole 8-bit radix passes.
-      // Longer seeds cost a pass per 8 bits; shorter ones leave more rows to
-      // the rounds.
+    // Seed length: enough symbols that two seed keys of one instance rarely
+    // collide by chance, log2(longest) / H + 2.5 with H the text's entropy in
+    // bits per symbol, plus one per doubling beyond 2^27 symbols (larger
+    // genomes hold more repeat copies), rounded up to whole 8-bit radix
+    // passes of the sort key.  Longer seeds cost a pass per 8 bits; shorter
+    // ones leave more rows to the rounds.  0 = no rule (near-constant text).
+    u32 need = 0;
+    {
       double entropy = 0;
       for (int b = 0; b < 256; ++b) {
         if (!counts[b]) continue;
@@ -711,58 +733,159 @@ struct Engine {
       }
       if (entropy > 0.5) {
         const double lg = std::log2(static_cast<double>(longest));
-        const double want = lg / entropy + 2.5 + std::max(0.0, lg - 27.0);
-        const u32 need = static_cast<u32>(std::ceil(want));
-        const u32 passes = (need * bits + kRadixBits - 1) / kRadixBits;
-        symbols = std::min(symbols, std::max<u32>(1, passes * kRadixBits / bits));
+        need = static_cast<u32>(std::ceil(lg / entropy + 2.5 + std::max(0.0, lg - 27.0)));
       }
     }
-    // Packed seed: when every instance fits 2^packed_max_bits symbols, its
-    // local index rides in the low key bits and the sort moves keys only.
+    // Two-bit seed: one instance whose text is four consecutive byte values
+    // (A, C, G, T) but for a few others (sentinel, separators, N), which the
+    // rare list places exactly.  The exact keys of rare rows hold s symbols
+    // of `bits`, so s <= 64 / bits.
+    TwoBitSeed tb{};
+    bool two_bit = false;
+    bool keep_runs[256] = {};
+    if (allow_two_bit && segs == 1 && c.tune.two_bit_seed && n >= c.tune.two_bit_min && sigma >= 4 && bits <= 4) {
+      int lo_byte = -1;
+      u64 best = 0;
+      for (int b = 0; b + 3 < 256; ++b) {
+        if (!counts[b] || !counts[b + 1] || !counts[b + 2] || !counts[b + 3]) continue;
+        const u64 c4 = u64(counts[b]) + counts[b + 1] + counts[b + 2] + counts[b + 3];
+        if (c4 > best) {
+          best = c4;
+          lo_byte = b;
+        }
+      }
+      int top_byte = 255;
+      while (top_byte > 0 && !counts[top_byte]) --top_byte;
+      if (lo_byte >= 0) {
+        const bool has_hi = top_byte > lo_byte + 3;
+        const u64 other = n - best - (has_hi ? counts[top_byte] : 0);
+        if (other * 64 <= n) {
+          two_bit = true;
+          tb.lo = code[lo_byte];
+          tb.hi = has_hi ? code[top_byte] : 0;
+          for (int b = lo_byte; b < lo_byte + 4; ++b) keep_runs[b] = true;
+          if (has_hi) keep_runs[top_byte] = true;
+        }
+      }
+    }
     const u32 index_bits = std::max<u32>(1, bits_for(longest - 1));
-    u32 packed_shift = 0;
-    if (c.tune.packed_max_bits && index_bits <= c.tune.packed_max_bits) {
-      u32 packed_symbols = (64 - index_bits) / bits;
-      if (c.tune.seed_symbols) packed_symbols = std::min(packed_symbols, c.tune.seed_symbols);
-      if (packed_symbols >= std::min<u32>(symbols, 12)) {
-        packed_shift = index_bits;
-        symbols = packed_symbols;
-      }
-    }
-    st.seed_symbols = symbols;
     upload(L.code, code, sizeof(code));
-
-    // Seed keys and the segmented seed sort.
     upload_segments(begin);
     const u32 seed_tiles = last_tiles;
-    plan_runs(symbols);
-    const u32 seed_bits = bits * symbols;
-    const u32 seed_passes = (seed_bits + kRadixBits - 1) / kRadixBits;
-    zero(L.hist, u64(segs) * seed_passes * kRadixDigits * 4);
-    launch("seed_keys", packed_shift ? n * 9 : n * 13, seed_keys_kernel,
-           (n + kSeedTile - 1) / kSeedTile, kSeedBlock, sizeof(SeedSmem), L.text, n, segments(),
-           static_cast<const u16*>(L.code), bits, symbols, seed_passes, L.hist, packed_shift,
-           L.k0, L.v0);
-    u64* keys = L.k0;
-    if (packed_shift) {
-      const bool swapped = radix_sort("seed_onesweep", L.k0, nullptr, L.k1, nullptr, L.seg_begin,
-                                      L.seg_tiles, segs, seed_tiles, n, packed_shift,
-                                      packed_shift + seed_bits, true, true);
-      keys = swapped ? L.k1 : L.k0;
-      sa = L.sa;
-      spare = L.v0;
-    } else {
-      const bool swapped = radix_sort("seed_onesweep", L.k0, L.v0, L.k1, L.sa, L.seg_begin,
-                                      L.seg_tiles, segs, seed_tiles, n, 0, seed_bits, true, true);
-      if (swapped) {
-        keys = L.k1;
+    u32 symbols = 0, packed_shift = 0, seed_bits = 0;
+    u64* keys = nullptr;
+    u64 rare_count = 0;
+    // Rare list in rank (free until the window scatter): exact keys, their
+    // sort's second buffer, two-bit keys, positions and their second buffer.
+    const u64 rare_cap = n / 16;  // 32 bytes each: half of rank's 4n
+    u64* rare_key = reinterpret_cast<u64*>(L.rank);
+    u64* rare_key_alt = rare_key + rare_cap;
+    u64* rare_k2 = rare_key_alt + rare_cap;
+    u32* rare_pos = reinterpret_cast<u32*>(rare_k2 + rare_cap);
+    u32* rare_pos_alt = rare_pos + rare_cap;
+    for (int attempt = 0;; ++attempt) {
+      if (attempt > 0) two_bit = false;  // too many rare rows: the code-table seed
+      // Symbols per key: sym_bits each (+ 2 tag bits for the two-bit key).
+      const u32 sym_bits = two_bit ? 2 : bits;
+      const u32 tag = two_bit ? 2 : 0;
+      const u32 cap_symbols = two_bit ? std::min<u32>(64 / bits, 31) : 64 / bits;
+      symbols = (64 - tag) / sym_bits;
+      if (c.tune.seed_symbols) {
+        symbols = std::min(symbols, c.tune.seed_symbols);
+      } else if (need) {
+        const u32 passes = (need * sym_bits + tag + kRadixBits - 1) / kRadixBits;
+        symbols = std::min(symbols, std::max<u32>(1, (passes * kRadixBits - tag) / sym_bits));
+      }
+      symbols = std::min(symbols, cap_symbols);
+      // Packed seed: when every instance fits 2^packed_max_bits symbols, its
+      // local index rides in the low key bits and the sort moves keys only.
+      packed_shift = 0;
+      if (c.tune.packed_max_bits && index_bits <= c.tune.packed_max_bits) {
+        u32 packed_symbols = std::min((64 - index_bits - tag) / sym_bits, cap_symbols);
+        if (c.tune.seed_symbols) packed_symbols = std::min(packed_symbols, c.tune.seed_symbols);
+        if (packed_symbols >= std::min<u32>(symbols, 12)) {
+          packed_shift = index_bits;
+          symbols = packed_symbols;
+        }
+      }
+      st.seed_symbols = symbols;
+      st.seed_code_bits = sym_bits;
+      plan_runs(symbols, two_bit ? keep_runs : nullptr);
+
+      // Seed keys and the segmented seed sort.
+      seed_bits = sym_bits * symbols + tag;
+      const u32 seed_passes = (seed_bits + kRadixBits - 1) / kRadixBits;
+      zero(L.hist, u64(segs) * seed_passes * kRadixDigits * 4);
+      if (two_bit) {
+        tb.all_hi = 0;
+        for (u32 k = 0; k < symbols; ++k) tb.all_hi = (tb.all_hi << bits) | tb.hi;
+        tb.rare_key = rare_key;
+        tb.rare_pos = rare_pos;
+        tb.rare_cap = rare_cap;
+        tb.rare_count = L.scalars + 44;
+        zero(L.scalars + 44, 8);
+        launch("seed_keys", packed_shift ? n * 9 : n * 13, seed_keys_kernel<true>,
+               (n + kSeedTile - 1) / kSeedTile, kSeedBlock, sizeof(SeedSmem), L.text, n,
+               segments(), static_cast<const u16*>(L.code), bits, symbols, seed_passes, L.hist,
+               packed_shift, L.k0, L.v0, tb);
+        // Read back with the sort's pass check below (one synchronisation).
+        SG_CUDA(cudaMemcpyAsync(c.host_scalars + 44, L.scalars + 44, 8, cudaMemcpyDeviceToHost,
+                                c.stream));
+      } else {
+        launch("seed_keys", packed_shift ? n * 9 : n * 13, seed_keys_kernel<false>,
+               (n + kSeedTile - 1) / kSeedTile, kSeedBlock, sizeof(SeedSmem), L.text, n,
+               segments(), static_cast<const u16*>(L.code), bits, symbols, seed_passes, L.hist,
+               packed_shift, L.k0, L.v0, TwoBitSeed{});
+      }
+      keys = L.k0;
+      if (packed_shift) {
+        const bool swapped = radix_sort("seed_onesweep", L.k0, nullptr, L.k1, nullptr, L.seg_begin,
+                                        L.seg_tiles, segs, seed_tiles, n, packed_shift,
+                                        packed_shift + seed_bits, true, true);
+        keys = swapped ? L.k1 : L.k0;
         sa = L.sa;
         spare = L.v0;
       } else {
-        keys = L.k0;
-        sa = L.v0;
-        spare = L.sa;
+        const bool swapped = radix_sort("seed_onesweep", L.k0, L.v0, L.k1, L.sa, L.seg_begin,
+                                        L.seg_tiles, segs, seed_tiles, n, 0, seed_bits, true, true);
+        if (swapped) {
+          keys = L.k1;
+          sa = L.sa;
+          spare = L.v0;
+        } else {
+          keys = L.k0;
+          sa = L.v0;
+          spare = L.sa;
+        }
       }
+      if (!two_bit) break;
+      rare_count = c.host_scalars[44];
+      if (rare_count <= rare_cap) break;
+    }
+    st.seed_rare_rows = static_cast<u32>(std::min<u64>(rare_count, 0xffffffffu));
+    RareRows rare{};
+    if (two_bit && rare_count > 0) {
+      // The rare rows in exact order, and their two-bit keys.
+      const u32 t = static_cast<u32>((rare_count + c.tune.sort_tile - 1) / c.tune.sort_tile);
+      const u64 b2[2] = {0, rare_count};
+      const u32 t2[2] = {0, t};
+      // A staging slot no other copy of this build uses: no synchronisation.
+      std::memcpy(c.host_small + 16384, b2, 16);
+      std::memcpy(c.host_small + 16384 + 16, t2, 8);
+      SG_CUDA(cudaMemcpyAsync(L.sort_begin, c.host_small + 16384, 16, cudaMemcpyHostToDevice, c.stream));
+      SG_CUDA(cudaMemcpyAsync(L.sort_tiles, c.host_small + 16384 + 16, 8, cudaMemcpyHostToDevice,
+                              c.stream));
+      const bool sw = radix_sort("rare_sort", rare_key, rare_pos, rare_key_alt, rare_pos_alt,
+                                 L.sort_begin, L.sort_tiles, 1, t, rare_count, 0, bits * symbols,
+                                 false);
+      rare.key = sw ? rare_key_alt : rare_key;
+      rare.pos = sw ? rare_pos_alt : rare_pos;
+      rare.k2 = rare_k2;
+      rare.count = rare_count;
+      rare.text = L.text;
+      launch("rare_two_bit", rare_count * 16, rare_two_bit_kernel,
+             grid_stride_blocks(rare_count, 256), 256, 0, rare.key, rare_count, symbols, bits, tb,
+             rare_k2);
     }
     // Seed ranks and the initial active list (in x).
     const u64 scan_tiles = (n + kScanTile - 1) / kScanTile;
@@ -771,10 +894,25 @@ struct Engine {
     u64* status_max = L.status;
     u64* status_sum = L.status + scan_tiles + 1;
     u64* pairs = keys == L.k0 ? L.k1 : L.k0;
-    launch("seed_rank", n * 24, seed_rank_kernel, scan_tiles, kScanBlock, 0,
-           static_cast<const u64*>(keys), sa, n, segments(), packed_shift, bits, symbols,
-           pairs, L.lcp, L.x, status_max, status_sum, L.counters, L.scalars + 0, L.flags,
-           runs_on ? 1u : 0u, segs > 1 ? 1u : 0u);
+    launch("seed_rank", n * 24, two_bit ? seed_rank_kernel<true> : seed_rank_kernel<false>,
+           scan_tiles, kScanBlock, 0, static_cast<const u64*>(keys), sa, n, segments(),
+           packed_shift, bits, symbols, pairs, L.lcp, L.x, status_max, status_sum, L.counters,
+           L.scalars + 0, L.flags, runs_on ? 1u : 0u, segs > 1 ? 1u : 0u);
+    if (rare.count > 0) {
+      launch("rare_place", rare.count * 32, rare_place_kernel, grid_stride_blocks(rare.count, 256),
+             256, 0, static_cast<const u64*>(keys), n, packed_shift, rare, bits, symbols, sa,
+             pairs, L.lcp, L.flags);
+      // Rare rows in shared windows join the active list (count in [45]).
+      const u64 rare_tiles = (rare.count + kScanTile - 1) / kScanTile;
+      zero(L.status, (rare_tiles + 1) * 8);
+      zero(L.counters + 2, 4);
+      zero(L.scalars + 45, 8);
+      launch("rare_active", rare.count * 16, rare_active_kernel, rare_tiles, kScanBlock, 0,
+             rare.key, rare.pos, rare.count, L.x, static_cast<const u64*>(L.scalars + 0),
+             L.scalars + 45, L.status, L.counters + 2, L.flags);
+      SG_CUDA(cudaMemcpyAsync(c.host_scalars + 45, L.scalars + 45, 8, cudaMemcpyDeviceToHost,
+                              c.stream));
+    }
     // rank[SA[r]] = head: group the pairs by 2048-position window (keys-only
     // passes over the position's high bits), then one coalesced window write.
     // A batch groups instance-local positions inside each instance (a pass
@@ -823,6 +961,7 @@ struct Engine {
              static_cast<const u64*>(grouped), n, L.rank, L.flags);
     }
     u64 active = read_scalar(0);
+    if (rare.count > 0) active += c.host_scalars[45];
     if (runs_on) {
       // Members of long runs: sub-group rows and ranks, and the rows in
       // sub-groups of two or more appended to the active list.
@@ -1085,6 +1224,7 @@ struct Engine {
   // ---- The doubling sort: leaves SA in `sa` and ISA (global rows) in rank.
   void suffix_sort() {
     allow_runs = true;
+    allow_two_bit = true;
     u64 active = seed_phase();
     // Rounds.  act and other alternate between x and the spare SA-sized
     // buffer; y holds the per-group tables.

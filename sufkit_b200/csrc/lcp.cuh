@@ -47,18 +47,6 @@ struct LongRow {
   u32 done;  // bytes known equal
 };
 
-// Warp-aggregated append of one item per participating lane.
-__device__ __forceinline__ u64 warp_append(u64* counter, bool take) {
-  const u32 mask = __ballot_sync(0xffffffffu, take);
-  if (!mask) return 0;
-  const u32 lane = threadIdx.x & 31;
-  const u32 leader = __ffs(mask) - 1;
-  u64 base = 0;
-  if (lane == leader) base = atomicAdd(reinterpret_cast<unsigned long long*>(counter), __popc(mask));
-  base = __shfl_sync(0xffffffffu, base, leader);
-  return base + __popc(mask & ((1u << lane) - 1));
-}
-
 // Row pass.  lcp receives final values for short rows; long rows go to the
 // irreducible queue or the pending (reducible) list.
 // With known_prefix > 0, rows whose lcp[] is already set (seed-group heads,
