@@ -52,6 +52,10 @@ def parse_args():
                     help="shrink the workload (profiling captures only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-workers", type=int, default=2,
+                    help="collections: contexts building sub-batches side by side (e2e)")
+    ap.add_argument("--e2e-batch-symbols", type=float, default=3e8,
+                    help="collections: symbols per sub-batch (e2e)")
     ap.add_argument("--tune", action="append", default=[],
                     help="library tuning knob key=value (sufgpu_set_tuning)")
     return ap.parse_args()
@@ -495,17 +499,23 @@ def main():
                 planes[key] = arr.ctypes.data
                 d2h += arr.nbytes
             host_out.append(planes)
+        def step():
+            return e2e_step(ctx, pinned_text, host_out, isa_bits, lcp_enc, sa_bits,
+                            args.e2e_batch_symbols, args.e2e_workers)
         for _ in range(2):
-            e2e_step(ctx, pinned_text, host_out, isa_bits, lcp_enc, sa_bits)
+            step()
         if dist is not None:
             dist.barrier()
         t0 = time.perf_counter()
         for _ in range(args.steps):
-            e2e_step(ctx, pinned_text, host_out, isa_bits, lcp_enc, sa_bits)
+            step()
         e2e_sec = shard.max_over_ranks((time.perf_counter() - t0) / args.steps, dist, dev)
         e2e = {"value": job_symbols / e2e_sec / 1e9, "unit": "Gsym/s",
                "h2d_bytes_per_step": n_total, "d2h_bytes_per_step": d2h,
                "ms_per_step": e2e_sec * 1e3}
+        if len(texts) > 1:
+            e2e["collection"] = {"workers": args.e2e_workers,
+                                 "batch_symbols": args.e2e_batch_symbols}
 
     # Roofline of the dominant kernel and of the whole build.
     peak, peak_kind = peaks()
@@ -567,14 +577,18 @@ def main():
         dist.destroy_process_group()
 
 
-def e2e_step(ctx, pinned_text, host_out, isa_bits, lcp_enc, sa_bits=32):
+def e2e_step(ctx, pinned_text, host_out, isa_bits, lcp_enc, sa_bits=32, batch_symbols=3e8,
+             workers=2):
+    """One build through the public API from pinned host buffers: a single
+    reference, or a collection in sub-batches on `workers` contexts
+    (sufgpu_build_collection), whose host copies overlap each other's kernels."""
     if len(pinned_text) == 1:
         t = pinned_text[0]
         return ctx.build_device(t.ctypes.data, int(t.size), host_out[0], sa_bits=sa_bits,
                                 isa_bits=isa_bits, lcp=lcp_enc)
-    for lo in range(0, len(pinned_text), 64):
-        ctx.build_batch_device([(t.ctypes.data, int(t.size)) for t in pinned_text[lo:lo + 64]],
-                               host_out[lo:lo + 64], sa_bits=32, isa_bits=isa_bits, lcp=lcp_enc)
+    return ctx.build_collection_device([(t.ctypes.data, int(t.size)) for t in pinned_text],
+                                       host_out, sa_bits=32, isa_bits=isa_bits, lcp=lcp_enc,
+                                       batch_symbols=int(batch_symbols), workers=workers)
 
 
 if __name__ == "__main__":

@@ -207,6 +207,21 @@ SUFGPU_API sufgpu_status sufgpu_build_batch(sufgpu_ctx *ctx, sufgpu_instance *in
                                  uint32_t count, const sufgpu_build_desc *desc,
                                  sufgpu_build_stats *stats);
 
+/* A collection larger than one launch (no counterpart in the reference, which
+ * builds one reference per call): the instances are split in order into
+ * sub-batches of at most batch_symbols symbols (0 = 2^30; a larger instance
+ * alone) and 8192 instances, and `workers` contexts on this context's device
+ * (this one plus up to 7 helpers it creates and keeps) build them side by side
+ * from host threads, so one sub-batch's host copies overlap another's kernels.
+ * Each sub-batch is one sufgpu_build_batch; every instance's planes equal a
+ * single build of it.  Byte-coded anchors stay valid until the next
+ * collection build or sufgpu_destroy.  stats: phase seconds, device_seconds
+ * and counters summed over the sub-batches, total_seconds the whole call. */
+SUFGPU_API sufgpu_status sufgpu_build_collection(sufgpu_ctx *ctx, sufgpu_instance *instances,
+                                                 uint64_t count, const sufgpu_build_desc *desc,
+                                                 uint64_t batch_symbols, uint32_t workers,
+                                                 sufgpu_build_stats *stats);
+
 /* Per-kernel profile: when enabled, every launch is bracketed by CUDA events
  * on the context stream and accumulated per kernel name with its algorithmic
  * bytes (the minimum it must read and write).  Enabling resets the totals. */

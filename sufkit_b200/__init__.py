@@ -149,6 +149,10 @@ _SIGNATURES = {
     "sufgpu_build_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(_Instance),
                                           ctypes.c_uint32, ctypes.POINTER(_Desc),
                                           ctypes.POINTER(_Stats)]),
+    "sufgpu_build_collection": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(_Instance),
+                                               ctypes.c_uint64, ctypes.POINTER(_Desc),
+                                               ctypes.c_uint64, ctypes.c_uint32,
+                                               ctypes.POINTER(_Stats)]),
     "sufgpu_set_profiling": (None, [ctypes.c_void_p, ctypes.c_int]),
     "sufgpu_profile_count": (ctypes.c_uint32, [ctypes.c_void_p]),
     "sufgpu_profile_entry": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32,
@@ -413,6 +417,60 @@ class Context:
             results.append(BuildResult(anchor_positions=pos, anchor_values=val,
                                        stats=self.last_stats, **planes))
         return results
+
+    def build_collection(self, texts: Sequence, sa_bits: int = 32, isa_bits: int = 0,
+                         lcp: LcpEncoding = LcpEncoding.RAW32, validate: bool = False,
+                         sampling_rate: int = 1, batch_symbols: int = 0,
+                         workers: int = 2) -> list[BuildResult]:
+        """Builds a collection in sub-batches of at most ``batch_symbols``
+        symbols on ``workers`` contexts side by side (sufgpu_build_collection);
+        each result equals a single build of that text."""
+        ts = [_as_text(t) for t in texts]
+        lcp = LcpEncoding(lcp)
+        all_planes = [self._alloc_outputs(_rows(int(t.size), sampling_rate), sa_bits, isa_bits,
+                                          lcp) for t in ts]
+        arr = (_Instance * max(1, len(ts)))()
+        for j, (t, planes) in enumerate(zip(ts, all_planes)):
+            arr[j].text = _ptr(t)
+            arr[j].n = int(t.size)
+            arr[j].out = self._outputs(planes)
+        desc = _Desc(sa_bits, isa_bits, int(lcp), FLAG_VALIDATE if validate else 0,
+                     int(sampling_rate))
+        stats = _Stats()
+        status = self._lib.sufgpu_build_collection(self._h, arr, len(ts), ctypes.byref(desc),
+                                                   int(batch_symbols), int(workers),
+                                                   ctypes.byref(stats))
+        if status != 0:
+            _raise(status, self._error())
+        self.last_stats = stats.as_dict()
+        results = []
+        for j, planes in enumerate(all_planes):
+            pos, val = self._anchors(arr[j].anchors, lcp)
+            results.append(BuildResult(anchor_positions=pos, anchor_values=val,
+                                       stats=self.last_stats, **planes))
+        return results
+
+    def build_collection_device(self, texts: Sequence[tuple[int, int]], outs: Sequence[dict],
+                                sa_bits: int = 32, isa_bits: int = 0,
+                                lcp: LcpEncoding = LcpEncoding.RAW32, batch_symbols: int = 0,
+                                workers: int = 2) -> dict:
+        """sufgpu_build_collection from (pointer, length) texts into raw
+        output pointers (host or device)."""
+        arr = (_Instance * max(1, len(texts)))()
+        for j, ((ptr, n), o) in enumerate(zip(texts, outs)):
+            arr[j].text = ptr
+            arr[j].n = n
+            arr[j].out = _Outputs(*(o.get(k) for k in ("sa_low", "sa_high", "isa_low",
+                                                       "isa_high", "lcp")))
+        desc = _Desc(sa_bits, isa_bits, int(LcpEncoding(lcp)), 0)
+        stats = _Stats()
+        status = self._lib.sufgpu_build_collection(self._h, arr, len(texts), ctypes.byref(desc),
+                                                   int(batch_symbols), int(workers),
+                                                   ctypes.byref(stats))
+        if status != 0:
+            _raise(status, self._error())
+        self.last_stats = stats.as_dict()
+        return self.last_stats
 
     def crc32_device(self, ptr: int, nbytes: int, crc_in: int = 0) -> int:
         """zlib's crc32(crc_in, data, nbytes) of device memory at ptr."""

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <chrono>
 #include <condition_variable>
@@ -344,6 +345,11 @@ struct sufgpu_ctx {
   // Layouts of recent builds: a layout's rounds are captured from its second
   // build on, so one-off builds never pay for a capture.
   std::vector<std::vector<u64>> seen_layouts;
+  // sufgpu_build_collection: helper contexts on the same device (one host
+  // thread each) and the anchors of its sub-batches (valid until the next
+  // collection build on this context).
+  std::vector<sufgpu_ctx*> helpers;
+  std::vector<std::vector<u8>> collection_anchors;
   void drop_round_graphs() {
     for (auto& g : round_graphs) cudaGraphExecDestroy(g.exec);
     round_graphs.clear();
@@ -1632,6 +1638,8 @@ sufgpu_status sufgpu_create(sufgpu_ctx** out, int device) {
 
 void sufgpu_destroy(sufgpu_ctx* ctx) {
   if (!ctx) return;
+  for (sufgpu_ctx* h : ctx->helpers) sufgpu_destroy(h);
+  ctx->helpers.clear();
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (auto& ev : ctx->ev) {
@@ -1918,6 +1926,130 @@ extern "C" sufgpu_status sufgpu_build_batch(sufgpu_ctx* ctx, sufgpu_instance* in
   } catch (const std::exception& err) {
     return fail(ctx, SUFGPU_BUILD_FAILURE, err.what());
   }
+}
+
+extern "C" sufgpu_status sufgpu_build_collection(sufgpu_ctx* ctx, sufgpu_instance* instances,
+                                                 uint64_t count, const sufgpu_build_desc* desc,
+                                                 uint64_t batch_symbols, uint32_t workers,
+                                                 sufgpu_build_stats* stats) {
+  if (!ctx) return SUFGPU_INVALID_INPUT;
+  if (auto s = check_desc(ctx, desc)) return s;
+  if (count > 0 && !instances) return fail(ctx, SUFGPU_INVALID_INPUT, "instances are null");
+  if (desc->prefix_k || (desc->flags & SUFGPU_FLAG_PLANE_CRC)) {
+    return fail(ctx, SUFGPU_INVALID_INPUT, "prefix directories and plane checksums are kept for single builds");
+  }
+  if (workers == 0 || workers > 8) return fail(ctx, SUFGPU_INVALID_INPUT, "workers must be 1..8");
+  if (batch_symbols == 0) batch_symbols = u64(1) << 30;
+  // Sub-batches in order: at most batch_symbols symbols (a larger instance
+  // alone) and kMaxSegmentsPerLaunch instances each.
+  std::vector<std::pair<u64, u32>> parts;  // (first instance, count)
+  for (u64 j = 0; j < count;) {
+    u64 syms = 0;
+    u32 m = 0;
+    while (j + m < count && m < kMaxSegmentsPerLaunch &&
+           (m == 0 || syms + instances[j + m].n <= batch_symbols)) {
+      syms += instances[j + m].n;
+      ++m;
+    }
+    parts.emplace_back(j, m);
+    j += m;
+  }
+  if (ctx->profiling) workers = 1;  // the per-kernel profile is kept per context
+  workers = static_cast<u32>(std::min<u64>(workers, std::max<size_t>(parts.size(), 1)));
+  const auto t0 = std::chrono::steady_clock::now();
+  while (ctx->helpers.size() + 1 < workers) {
+    sufgpu_ctx* h = nullptr;
+    if (sufgpu_status st = sufgpu_create(&h, ctx->device)) {
+      return fail(ctx, st, "cannot create a helper context: " + g_create_error);
+    }
+    ctx->helpers.push_back(h);
+  }
+  std::vector<sufgpu_ctx*> pool{ctx};
+  for (u32 w = 1; w < workers; ++w) {
+    sufgpu_ctx* h = ctx->helpers[w - 1];
+    h->tune = ctx->tune;
+    h->tuning_classes = ctx->tuning_classes;
+    pool.push_back(h);
+  }
+  const bool byte_coded =
+      desc->lcp_encoding == SUFGPU_LCP_BYTE32 || desc->lcp_encoding == SUFGPU_LCP_BYTE64;
+  ctx->collection_anchors.assign(byte_coded ? 2 * parts.size() : 0, {});
+  std::vector<sufgpu_build_stats> part_stats(parts.size());
+  std::atomic<size_t> next{0};
+  std::atomic<bool> failed{false};
+  std::mutex error_mu;
+  sufgpu_status first_status = SUFGPU_OK;
+  std::string first_error;
+  auto work = [&](sufgpu_ctx* w) {
+    while (!failed.load()) {
+      const size_t i = next.fetch_add(1);
+      if (i >= parts.size()) return;
+      sufgpu_instance* inst = instances + parts[i].first;
+      const sufgpu_status st = sufgpu_build_batch(w, inst, parts[i].second, desc, &part_stats[i]);
+      if (st != SUFGPU_OK) {
+        std::lock_guard<std::mutex> lock(error_mu);
+        if (first_status == SUFGPU_OK) {
+          first_status = st;
+          first_error = w->last_error;
+        }
+        failed = true;
+        return;
+      }
+      if (byte_coded) {  // keep this sub-batch's anchors past the worker's next build
+        const u64 w_bytes = desc->lcp_encoding == SUFGPU_LCP_BYTE64 ? 8 : 4;
+        u64 total = 0;
+        for (u32 j = 0; j < parts[i].second; ++j) total += inst[j].anchors.count;
+        std::vector<u8>& pos = ctx->collection_anchors[2 * i];
+        std::vector<u8>& val = ctx->collection_anchors[2 * i + 1];
+        pos.resize(std::max<u64>(total * w_bytes, 8));
+        val.resize(std::max<u64>(total * w_bytes, 8));
+        u64 at = 0;
+        for (u32 j = 0; j < parts[i].second; ++j) {
+          sufgpu_anchors& a = inst[j].anchors;
+          const u64 bytes = a.count * w_bytes;
+          if (bytes) {
+            std::memcpy(pos.data() + at, a.positions, bytes);
+            std::memcpy(val.data() + at, a.values, bytes);
+          }
+          a.positions = pos.data() + at;
+          a.values = val.data() + at;
+          at += bytes;
+        }
+      }
+    }
+  };
+  std::vector<std::thread> threads;
+  for (u32 w = 1; w < workers; ++w) threads.emplace_back(work, pool[w]);
+  work(pool[0]);
+  for (auto& t : threads) t.join();
+  if (first_status != SUFGPU_OK) return fail(ctx, first_status, first_error);
+  if (stats) {
+    sufgpu_build_stats sum{};
+    for (const auto& p : part_stats) {
+      sum.h2d_seconds += p.h2d_seconds;
+      sum.sa_seconds += p.sa_seconds;
+      sum.isa_seconds += p.isa_seconds;
+      sum.lcp_seconds += p.lcp_seconds;
+      sum.storage_seconds += p.storage_seconds;
+      sum.d2h_seconds += p.d2h_seconds;
+      sum.device_seconds += p.device_seconds;
+      sum.symbols += p.symbols;
+      sum.rounds = std::max(sum.rounds, p.rounds);
+      sum.seed_symbols = std::max(sum.seed_symbols, p.seed_symbols);
+      sum.active_rows += p.active_rows;
+      sum.active_first += p.active_first;
+      sum.irreducible_long += p.irreducible_long;
+      sum.anchors += p.anchors;
+      sum.kernel_launches += p.kernel_launches;
+      sum.long_runs += p.long_runs;
+      sum.seg_sort_fallbacks += p.seg_sort_fallbacks;
+      sum.seed_code_bits = std::max(sum.seed_code_bits, p.seed_code_bits);
+    }
+    sum.total_seconds =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    *stats = sum;
+  }
+  return SUFGPU_OK;
 }
 
 extern "C" void sufgpu_set_profiling(sufgpu_ctx* ctx, int enable) {

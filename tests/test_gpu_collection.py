@@ -1,0 +1,57 @@
+"""GPU: collections built in sub-batches on several contexts side by side
+(sufgpu_build_collection).  Every instance equals a single build of it."""
+import numpy as np
+import pytest
+
+import sufkit_b200 as sg
+from sufkit_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def texts(count, seed):
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(rng.integers(2_000, 60_000))
+        body = rng.integers(2, 6, size=n).astype(np.uint8)
+        if i % 3 == 0:
+            body[n // 3:n // 3 + 500] = 6
+        out.append(np.concatenate([body, np.array([1], np.uint8), body[: n // 4],
+                                   np.zeros(1, np.uint8)]))
+    return out
+
+
+@pytest.mark.parametrize("workers,batch_symbols", [(1, 200_000), (2, 150_000), (3, 1), (2, 0)])
+def test_collection_equals_single_builds(ctx, workers, batch_symbols):
+    ts = texts(23, workers * 10 + 1)
+    got = ctx.build_collection(ts, sa_bits=32, isa_bits=32, lcp=sg.LcpEncoding.RAW32,
+                               validate=True, batch_symbols=batch_symbols, workers=workers)
+    assert ctx.last_stats["symbols"] == sum(t.size for t in ts)
+    for t, r in zip(ts, got):
+        one = ctx.build(t, sa_bits=32, isa_bits=32, lcp=sg.LcpEncoding.RAW32)
+        assert (r.sa_low == one.sa_low).all()
+        assert (r.isa_low == one.isa_low).all()
+        assert (r.lcp == one.lcp).all()
+
+
+def test_collection_byte_coded_anchors_survive(ctx):
+    """Anchors of every sub-batch stay readable after the later sub-batches."""
+    ts = [synth.uneven_reference(i, 40_000 + 5_000 * i).logical_text() for i in range(9)]
+    for t in ts[::3]:
+        t[1000:1300] = 2  # long LCPs: anchors
+    got = ctx.build_collection(ts, sa_bits=40, lcp=sg.LcpEncoding.BYTE32, batch_symbols=100_000,
+                               workers=2)
+    for t, r in zip(ts, got):
+        one = ctx.build(t, sa_bits=40, isa_bits=0, lcp=sg.LcpEncoding.BYTE32)
+        assert (r.sa == one.sa).all() and (r.lcp == one.lcp).all()
+        assert (r.anchor_positions == one.anchor_positions).all()
+        assert (r.anchor_values == one.anchor_values).all()
+
+
+def test_collection_rejects_bad_arguments(ctx):
+    with pytest.raises(sg.SufkitError):
+        ctx.build_collection(texts(2, 5), workers=0)
+    with pytest.raises(sg.SufkitError):
+        ctx.build_collection(texts(2, 5), workers=9)
+    assert ctx.build_collection([], workers=2) == []
