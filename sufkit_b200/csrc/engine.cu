@@ -378,6 +378,26 @@ struct Engine {
   bool want_crc = false;
   bool allow_runs = false;
   bool allow_two_bit = false;  // the served engine's shared arena keeps the code-table seed
+  // Collection workers share one gate: a build holds it from its first kernel
+  // to its last, so that one worker's output copies run while another
+  // computes instead of all workers computing, then copying, in step.
+  std::mutex* gate = nullptr;
+  bool gate_held = false;
+  void gate_enter() {
+    if (!gate) return;
+    gate->lock();
+    gate_held = true;
+  }
+  void gate_leave() {  // after the build's last kernel is enqueued
+    if (!gate_held) return;
+    SG_CUDA(cudaEventRecord(c.ev[6], c.stream));
+    SG_CUDA(cudaEventSynchronize(c.ev[6]));
+    gate_held = false;
+    gate->unlock();
+  }
+  ~Engine() {
+    if (gate_held) gate->unlock();
+  }
   bool runs_on = false;
   u32 run_count = 0;
   u64 run_members = 0;
@@ -1430,6 +1450,45 @@ void emit_outputs(Engine& e, const sufgpu_build_desc& d, sufgpu_outputs* outs,
   // ISA: rank holds global rows.  Stage packed planes in k0/k1 when the
   // layout differs from the device one, then copy each instance's rows.
   const bool want_isa = d.isa_storage_bits != 0;
+  // A gated build (collection worker) without ISA, with a 32-bit SA and raw or
+  // no LCP computes every plane first (the packed SA staged in rank, free
+  // once validated) and leaves the gate before its copies.
+  const bool raw_lcp = d.lcp_encoding == SUFGPU_LCP_RAW32 || d.lcp_encoding == SUFGPU_LCP_RAW64;
+  if (e.gate && !want_isa && d.sa_storage_bits == 32 &&
+      (raw_lcp || d.lcp_encoding == SUFGPU_LCP_NONE) && !e.want_crc) {
+    SG_CUDA(cudaEventRecord(c.ev[3], c.stream));
+    if (d.flags & SUFGPU_FLAG_VALIDATE) {
+      e.launch("validate", n * 8, validate_kernel, e.grid_stride_blocks(n, 256), 256, 0, e.sa,
+               L.rank, n, e.segments(), L.flags);
+    }
+    const bool direct = count == 1;
+    const u32* sa_plane = e.sa;
+    if (!direct) {
+      e.launch("pack", n * 8, pack_kernel, e.grid_stride_blocks(n, 256), 256, 0, e.sa, n,
+               e.segments(), 32u, static_cast<void*>(L.rank), static_cast<void*>(nullptr));
+      sa_plane = L.rank;
+    }
+    SG_CUDA(cudaEventRecord(c.ev[4], c.stream));
+    const u8* lcp_src = nullptr;
+    const u64 lw = d.lcp_encoding == SUFGPU_LCP_RAW64 ? 8 : 4;
+    if (raw_lcp) {
+      const Engine::LcpPhase ph = e.lcp_phase();
+      lcp_src = reinterpret_cast<const u8*>(ph.lcp);
+      if (lw == 8) {
+        e.launch("lcp_widen", n * 12, widen_kernel<u64>, e.grid_stride_blocks(n, 256), 256, 0,
+                 static_cast<const u32*>(ph.lcp), n, L.k0);
+        lcp_src = reinterpret_cast<const u8*>(L.k0);
+      }
+    }
+    e.gate_leave();
+    for (u32 j = 0; j < count; ++j) {
+      const u64 b = e.begin[j], rows = e.begin[j + 1] - e.begin[j];
+      copy_out(c, outs[j].sa_low, sa_plane + b, rows * 4);
+      if (lcp_src) copy_out(c, outs[j].lcp, lcp_src + b * lw, rows * lw);
+    }
+    SG_CUDA(cudaEventRecord(c.ev[5], c.stream));
+    return;
+  }
   auto emit = [&](const u32* values, u32 bits, bool isa) {
     const bool direct = bits == 32 && count == 1;
     u8* low = reinterpret_cast<u8*>(L.k0);
@@ -1734,8 +1793,13 @@ static sufgpu_status check_desc(sufgpu_ctx* ctx, const sufgpu_build_desc* d) {
 
 static sufgpu_status finish(sufgpu_ctx* ctx, Engine& e, sufgpu_build_stats* stats,
                             std::chrono::steady_clock::time_point t0) {
+  // The build's stream is non-blocking: wait for it before reading its error
+  // flags and events (a legacy-stream copy would not), and so that every
+  // output copy has landed when the call returns.
+  SG_CUDA(cudaStreamSynchronize(ctx->stream));
   DeviceFlags flags{};
-  SG_CUDA(cudaMemcpy(&flags, e.L.flags, sizeof(flags), cudaMemcpyDeviceToHost));
+  SG_CUDA(cudaMemcpyAsync(&flags, e.L.flags, sizeof(flags), cudaMemcpyDeviceToHost, ctx->stream));
+  SG_CUDA(cudaStreamSynchronize(ctx->stream));
   if (flags.error) {
     char buf[160];
     std::snprintf(buf, sizeof(buf), "device check failed (flags 0x%x, site %u)", flags.error,
@@ -1858,9 +1922,20 @@ int sufgpu_divsufsort(sufgpu_ctx* ctx, const uint8_t* T, int32_t* SA, int32_t n)
 
 }  // extern "C"
 
+// sufgpu_build_batch; a collection worker passes the workers' shared gate.
+static sufgpu_status build_batch(sufgpu_ctx* ctx, sufgpu_instance* instances, uint32_t count,
+                                 const sufgpu_build_desc* desc, sufgpu_build_stats* stats,
+                                 std::mutex* gate);
+
 extern "C" sufgpu_status sufgpu_build_batch(sufgpu_ctx* ctx, sufgpu_instance* instances,
                                             uint32_t count, const sufgpu_build_desc* desc,
                                             sufgpu_build_stats* stats) {
+  return build_batch(ctx, instances, count, desc, stats, nullptr);
+}
+
+static sufgpu_status build_batch(sufgpu_ctx* ctx, sufgpu_instance* instances, uint32_t count,
+                                 const sufgpu_build_desc* desc, sufgpu_build_stats* stats,
+                                 std::mutex* gate) {
   if (!ctx) return SUFGPU_INVALID_INPUT;
   if (auto s = check_desc(ctx, desc)) return s;
   if (count == 0) {
@@ -1913,6 +1988,8 @@ extern "C" sufgpu_status sufgpu_build_batch(sufgpu_ctx* ctx, sufgpu_instance* in
     std::vector<sufgpu_outputs> outs(count);
     std::vector<sufgpu_anchors> anchors(count);
     for (u32 j = 0; j < count; ++j) outs[j] = instances[j].out;
+    e.gate = gate;
+    e.gate_enter();  // the text copies above run while another worker computes
     run_build(e, *desc, outs.data(), anchors.data(), count);
     for (u32 j = 0; j < count; ++j) instances[j].anchors = anchors[j];
     e.st.kernel_launches = ctx->launches;
@@ -1977,7 +2054,7 @@ extern "C" sufgpu_status sufgpu_build_collection(sufgpu_ctx* ctx, sufgpu_instanc
   std::vector<sufgpu_build_stats> part_stats(parts.size());
   std::atomic<size_t> next{0};
   std::atomic<bool> failed{false};
-  std::mutex error_mu;
+  std::mutex error_mu, gate;
   sufgpu_status first_status = SUFGPU_OK;
   std::string first_error;
   auto work = [&](sufgpu_ctx* w) {
@@ -1985,7 +2062,8 @@ extern "C" sufgpu_status sufgpu_build_collection(sufgpu_ctx* ctx, sufgpu_instanc
       const size_t i = next.fetch_add(1);
       if (i >= parts.size()) return;
       sufgpu_instance* inst = instances + parts[i].first;
-      const sufgpu_status st = sufgpu_build_batch(w, inst, parts[i].second, desc, &part_stats[i]);
+      const sufgpu_status st = build_batch(w, inst, parts[i].second, desc, &part_stats[i],
+                                           workers > 1 ? &gate : nullptr);
       if (st != SUFGPU_OK) {
         std::lock_guard<std::mutex> lock(error_mu);
         if (first_status == SUFGPU_OK) {
@@ -2423,8 +2501,10 @@ void server_loop(sufgpu_server* S) {
         }
       }
       if (!finished.empty()) finalize_batch(S, finished, other);
-      DeviceFlags flags{};
-      SG_CUDA(cudaMemcpy(&flags, S->L.flags, sizeof(flags), cudaMemcpyDeviceToHost));
+      DeviceFlags flags{};  // read on the engine's (non-blocking) stream
+      SG_CUDA(cudaMemcpyAsync(&flags, S->L.flags, sizeof(flags), cudaMemcpyDeviceToHost,
+                              S->ctx->stream));
+      SG_CUDA(cudaStreamSynchronize(S->ctx->stream));
       if (flags.error) throw BuildError{SUFGPU_BUILD_FAILURE, "device check failed in the served engine"};
     } catch (const CudaError& err) {
       cudaGetLastError();

@@ -35,6 +35,21 @@ def test_collection_equals_single_builds(ctx, workers, batch_symbols):
         assert (r.lcp == one.lcp).all()
 
 
+@pytest.mark.parametrize("lcp", [sg.LcpEncoding.RAW32, sg.LcpEncoding.RAW64, sg.LcpEncoding.NONE])
+@pytest.mark.parametrize("workers", [2, 3])
+def test_collection_sa_and_lcp_only(ctx, lcp, workers):
+    """Without ISA a worker computes all planes first and copies after it
+    leaves the shared gate (the packed SA staged in the rank buffer)."""
+    ts = texts(31, 7 + workers)
+    got = ctx.build_collection(ts, sa_bits=32, isa_bits=0, lcp=lcp, validate=True,
+                               batch_symbols=120_000, workers=workers)
+    for t, r in zip(ts, got):
+        one = ctx.build(t, sa_bits=32, isa_bits=0, lcp=lcp)
+        assert (r.sa_low == one.sa_low).all()
+        if lcp != sg.LcpEncoding.NONE:
+            assert (r.lcp == one.lcp).all()
+
+
 def test_collection_byte_coded_anchors_survive(ctx):
     """Anchors of every sub-batch stay readable after the later sub-batches."""
     ts = [synth.uneven_reference(i, 40_000 + 5_000 * i).logical_text() for i in range(9)]
