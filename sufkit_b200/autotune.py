@@ -1,5 +1,5 @@
 """Autotuner for the build knobs (seed length, radix tile and block shape,
-ballot-ranking threshold, packed-seed threshold).
+ballot-ranking threshold, packed-seed threshold, two-bit seed).
 
     python -m sufkit_b200.autotune [--out sufkit_b200/tuning.json] [--quick]
 
@@ -31,9 +31,10 @@ CANDIDATES = {
     "sort_block": [256, 512],
     "ballot_min_elems": [1 << 23, 0, 1 << 62],
     "packed_max_bits": [24, 0],
+    "two_bit_seed": [1, 0],
 }
 DEFAULTS = {"seed_symbols": 0, "sort_tile": 4096, "sort_block": 256,
-            "ballot_min_elems": 1 << 23, "packed_max_bits": 24}
+            "ballot_min_elems": 1 << 23, "packed_max_bits": 24, "two_bit_seed": 1}
 
 
 def workloads(quick: bool):

@@ -21,6 +21,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <system_error>
 #include <thread>
 #include <unordered_map>
 #include <utility>
@@ -888,7 +889,7 @@ struct Engine {
       rare_count = c.host_scalars[44];
       if (rare_count <= rare_cap) break;
     }
-    st.seed_rare_rows = static_cast<u32>(std::min<u64>(rare_count, 0xffffffffu));
+    st.seed_rare_rows = two_bit ? static_cast<u32>(std::min<u64>(rare_count, 0xffffffffu)) : 0;
     RareRows rare{};
     if (two_bit && rare_count > 0) {
       // The rare rows in exact order, and their two-bit keys.
@@ -1354,7 +1355,6 @@ void copy_plane(Engine& e, void* dst, const void* src, u64 bytes, int slot) {
   if (e.want_crc && dst) e.st.plane_crc[slot] = e.crc32_device(src, bytes, 0, reinterpret_cast<u32*>(e.L.status));
 }
 
-u64 plane_bytes(u32 bits, u64 rows) { return rows * (bits == 64 ? 8 : 4); }
 u64 high_bytes(u32 bits, u64 rows) { return bits == 40 ? rows : bits == 48 ? 2 * rows : 0; }
 
 // Everything after the sort: ISA and SA packing, validation, LCP (raw or
@@ -2057,7 +2057,15 @@ extern "C" sufgpu_status sufgpu_build_collection(sufgpu_ctx* ctx, sufgpu_instanc
   std::mutex error_mu, gate;
   sufgpu_status first_status = SUFGPU_OK;
   std::string first_error;
-  auto work = [&](sufgpu_ctx* w) {
+  auto record_failure = [&](sufgpu_status st, const std::string& message) {
+    std::lock_guard<std::mutex> lock(error_mu);
+    if (first_status == SUFGPU_OK) {
+      first_status = st;
+      first_error = message;
+    }
+    failed = true;
+  };
+  auto build_parts = [&](sufgpu_ctx* w) {
     while (!failed.load()) {
       const size_t i = next.fetch_add(1);
       if (i >= parts.size()) return;
@@ -2065,12 +2073,7 @@ extern "C" sufgpu_status sufgpu_build_collection(sufgpu_ctx* ctx, sufgpu_instanc
       const sufgpu_status st = build_batch(w, inst, parts[i].second, desc, &part_stats[i],
                                            workers > 1 ? &gate : nullptr);
       if (st != SUFGPU_OK) {
-        std::lock_guard<std::mutex> lock(error_mu);
-        if (first_status == SUFGPU_OK) {
-          first_status = st;
-          first_error = w->last_error;
-        }
-        failed = true;
+        record_failure(st, w->last_error);
         return;
       }
       if (byte_coded) {  // keep this sub-batch's anchors past the worker's next build
@@ -2096,8 +2099,19 @@ extern "C" sufgpu_status sufgpu_build_collection(sufgpu_ctx* ctx, sufgpu_instanc
       }
     }
   };
+  auto work = [&](sufgpu_ctx* w) {
+    try {
+      build_parts(w);
+    } catch (const std::exception& err) {  // host allocation in the anchor copies
+      record_failure(SUFGPU_BUILD_FAILURE, err.what());
+    }
+  };
   std::vector<std::thread> threads;
-  for (u32 w = 1; w < workers; ++w) threads.emplace_back(work, pool[w]);
+  try {
+    for (u32 w = 1; w < workers; ++w) threads.emplace_back(work, pool[w]);
+  } catch (const std::system_error&) {
+    // No more host threads: the workers started so far take every sub-batch.
+  }
   work(pool[0]);
   for (auto& t : threads) t.join();
   if (first_status != SUFGPU_OK) return fail(ctx, first_status, first_error);
