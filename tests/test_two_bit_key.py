@@ -52,8 +52,10 @@ def rare(k):
 
 
 @pytest.mark.parametrize("s", [1, 2, 3, 4])
-@pytest.mark.parametrize("alphabet,hi", [(range(8), HI), (range(7), 0)])
+@pytest.mark.parametrize("alphabet,hi", [(range(8), HI), (range(7), 0), (range(9), 8)])
 def test_order_properties(s, alphabet, hi):
+    """range(9): two symbols above T (N and one more); only windows of the
+    largest one get t = 3."""
     ws = sorted(windows(s, alphabet))
     keys = [two_bit_key(w, hi) for w in ws]
     assert all(a <= b for a, b in zip(keys, keys[1:])), "not monotone"
@@ -68,3 +70,44 @@ def test_rare_windows_are_the_ones_with_other_symbols():
         regular = all(LO <= c < LO + 4 for c in w)
         all_n = all(c == HI for c in w)
         assert rare(two_bit_key(w)) == (not regular and not all_n)
+
+
+def place(text, s):
+    """The seed phase on a small text, as the kernels do it: sort by two-bit
+    key (ties by position), then place the rare rows from the list sorted by
+    exact key: entry idx of key k goes to row g + (idx - i0), g the first row
+    of k, i0 its first entry.  Returns the positions in row order."""
+    import bisect
+    n = len(text)
+    codes = list(text) + [0] * s  # text given as codes 1..7, 0 past the end
+    windows = [tuple(codes[p:p + s]) for p in range(n)]
+    keys = [two_bit_key(w) for w in windows]
+    rows = sorted(range(n), key=lambda p: (keys[p], p))
+    sorted_keys = [keys[p] for p in rows]
+    rare_list = sorted((p for p in range(n) if rare(keys[p])), key=lambda p: exact_key(windows[p]))
+    rare_keys = [keys[p] for p in rare_list]
+    for idx, p in enumerate(rare_list):
+        k = rare_keys[idx]
+        i0 = bisect.bisect_left(rare_keys, k)
+        g = bisect.bisect_left(sorted_keys, k)
+        rows[g + idx - i0] = p
+    return rows, windows
+
+
+@pytest.mark.parametrize("seed", range(40))
+def test_placement_orders_rows_by_exact_window(seed):
+    import random
+    rng = random.Random(seed)
+    n = rng.randint(5, 200)
+    body = [rng.randint(LO, LO + 3) for _ in range(n)]
+    for _ in range(rng.randint(0, 5)):  # N runs
+        at, length = rng.randrange(n), rng.randint(1, 10)
+        body[at:at + length] = [HI] * len(body[at:at + length])
+    for _ in range(rng.randint(0, 3)):  # separators
+        body[rng.randrange(n)] = 2
+    text = body + ([1] if rng.random() < 0.7 else [])  # the sentinel, mostly
+    s = rng.randint(1, 7)
+    rows, windows = place(text, s)
+    assert sorted(rows) == list(range(len(text)))
+    order = [exact_key(windows[p]) for p in rows]
+    assert order == sorted(order)
