@@ -75,7 +75,7 @@ def peaks():
 def workload(name: str, scale: float = 1.0, count: int = 256):
     from sufkit_b200 import synth
     if name == "plain4m":
-        ref = synth.plain_4mbp()
+        ref = synth.plain_4mbp(scale)
         desc = ("plain 4 Mbp build: 4 contigs (1.5/1.2/0.8/0.5 Mbp), uniform ACGT, "
                 "0.1% N runs; Fast profile SA+ISA+raw LCP32, 32-bit storage")
         return [ref.logical_text()], desc
