@@ -514,8 +514,16 @@ def main():
                "h2d_bytes_per_step": n_total, "d2h_bytes_per_step": d2h,
                "ms_per_step": e2e_sec * 1e3}
         if len(texts) > 1:
-            e2e["collection"] = {"workers": args.e2e_workers,
-                                 "batch_symbols": args.e2e_batch_symbols}
+            # Where the last step's sub-batches spent their time (host clock):
+            # waiting for the compute gate, holding it, and copying after it.
+            trace = ctx.collection_trace()
+            e2e["collection"] = {
+                "workers": args.e2e_workers, "batch_symbols": args.e2e_batch_symbols,
+                "sub_batches": len(trace),
+                "gate_wait_s": sum(t["gate_in"] - t["start"] for t in trace),
+                "gate_held_s": sum(t["gate_out"] - t["gate_in"] for t in trace),
+                "after_gate_s": sum(t["end"] - t["gate_out"] for t in trace),
+                "span_s": max((t["end"] for t in trace), default=0.0)}
 
     # Roofline of the dominant kernel and of the whole build.
     peak, peak_kind = peaks()

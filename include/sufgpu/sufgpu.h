@@ -222,6 +222,15 @@ SUFGPU_API sufgpu_status sufgpu_build_collection(sufgpu_ctx *ctx, sufgpu_instanc
                                                  uint64_t batch_symbols, uint32_t workers,
                                                  sufgpu_build_stats *stats);
 
+/* Trace of the last sufgpu_build_collection on this context, one entry per
+ * sub-batch in order: the worker that built it and the host clock (seconds
+ * since the call began) when it started, took the workers' compute gate, left
+ * it, and finished (copies included).  With one worker the gate times are the
+ * start and the end. */
+SUFGPU_API uint64_t sufgpu_collection_parts(const sufgpu_ctx *ctx);
+SUFGPU_API sufgpu_status sufgpu_collection_trace(const sufgpu_ctx *ctx, uint64_t index,
+                                                 uint32_t *worker, double times[4]);
+
 /* Per-kernel profile: when enabled, every launch is bracketed by CUDA events
  * on the context stream and accumulated per kernel name with its algorithmic
  * bytes (the minimum it must read and write).  Enabling resets the totals. */

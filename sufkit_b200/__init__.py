@@ -153,6 +153,10 @@ _SIGNATURES = {
                                                ctypes.c_uint64, ctypes.POINTER(_Desc),
                                                ctypes.c_uint64, ctypes.c_uint32,
                                                ctypes.POINTER(_Stats)]),
+    "sufgpu_collection_parts": (ctypes.c_uint64, [ctypes.c_void_p]),
+    "sufgpu_collection_trace": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64,
+                                               ctypes.POINTER(ctypes.c_uint32),
+                                               ctypes.POINTER(ctypes.c_double)]),
     "sufgpu_set_profiling": (None, [ctypes.c_void_p, ctypes.c_int]),
     "sufgpu_profile_count": (ctypes.c_uint32, [ctypes.c_void_p]),
     "sufgpu_profile_entry": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32,
@@ -471,6 +475,20 @@ class Context:
             _raise(status, self._error())
         self.last_stats = stats.as_dict()
         return self.last_stats
+
+    def collection_trace(self) -> list[dict]:
+        """Per sub-batch of the last collection build: its worker and the host
+        seconds (since the call began) at which it started, took the compute
+        gate, left it, and finished."""
+        out = []
+        worker = ctypes.c_uint32()
+        times = (ctypes.c_double * 4)()
+        for i in range(int(self._lib.sufgpu_collection_parts(self._h))):
+            if self._lib.sufgpu_collection_trace(self._h, i, ctypes.byref(worker), times) != 0:
+                break
+            out.append({"worker": int(worker.value), "start": times[0], "gate_in": times[1],
+                        "gate_out": times[2], "end": times[3]})
+        return out
 
     def crc32_device(self, ptr: int, nbytes: int, crc_in: int = 0) -> int:
         """zlib's crc32(crc_in, data, nbytes) of device memory at ptr."""

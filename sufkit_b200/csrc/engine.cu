@@ -351,6 +351,13 @@ struct sufgpu_ctx {
   // collection build on this context).
   std::vector<sufgpu_ctx*> helpers;
   std::vector<std::vector<u8>> collection_anchors;
+  // Per sub-batch of the last collection build: worker, and seconds since
+  // the call began at which it started, took the gate, left it and ended.
+  struct PartTrace {
+    u32 worker;
+    double start, gate_in, gate_out, end;
+  };
+  std::vector<PartTrace> collection_trace;
   void drop_round_graphs() {
     for (auto& g : round_graphs) cudaGraphExecDestroy(g.exec);
     round_graphs.clear();
@@ -384,16 +391,20 @@ struct Engine {
   // computes instead of all workers computing, then copying, in step.
   std::mutex* gate = nullptr;
   bool gate_held = false;
+  // Host clock readings of the gate (steady_clock), for the collection trace.
+  std::chrono::steady_clock::time_point gate_in{}, gate_out{};
   void gate_enter() {
     if (!gate) return;
     gate->lock();
     gate_held = true;
+    gate_in = std::chrono::steady_clock::now();
   }
   void gate_leave() {  // after the build's last kernel is enqueued
     if (!gate_held) return;
     SG_CUDA(cudaEventRecord(c.ev[6], c.stream));
     SG_CUDA(cudaEventSynchronize(c.ev[6]));
     gate_held = false;
+    gate_out = std::chrono::steady_clock::now();
     gate->unlock();
   }
   ~Engine() {
@@ -1922,10 +1933,14 @@ int sufgpu_divsufsort(sufgpu_ctx* ctx, const uint8_t* T, int32_t* SA, int32_t n)
 
 }  // extern "C"
 
-// sufgpu_build_batch; a collection worker passes the workers' shared gate.
+// sufgpu_build_batch; a collection worker passes the workers' shared gate and
+// receives the host clock readings of its gate (unchanged without one).
+struct GateTimes {
+  std::chrono::steady_clock::time_point in{}, out{};
+};
 static sufgpu_status build_batch(sufgpu_ctx* ctx, sufgpu_instance* instances, uint32_t count,
                                  const sufgpu_build_desc* desc, sufgpu_build_stats* stats,
-                                 std::mutex* gate);
+                                 std::mutex* gate, GateTimes* times = nullptr);
 
 extern "C" sufgpu_status sufgpu_build_batch(sufgpu_ctx* ctx, sufgpu_instance* instances,
                                             uint32_t count, const sufgpu_build_desc* desc,
@@ -1935,7 +1950,7 @@ extern "C" sufgpu_status sufgpu_build_batch(sufgpu_ctx* ctx, sufgpu_instance* in
 
 static sufgpu_status build_batch(sufgpu_ctx* ctx, sufgpu_instance* instances, uint32_t count,
                                  const sufgpu_build_desc* desc, sufgpu_build_stats* stats,
-                                 std::mutex* gate) {
+                                 std::mutex* gate, GateTimes* times) {
   if (!ctx) return SUFGPU_INVALID_INPUT;
   if (auto s = check_desc(ctx, desc)) return s;
   if (count == 0) {
@@ -1993,7 +2008,14 @@ static sufgpu_status build_batch(sufgpu_ctx* ctx, sufgpu_instance* instances, ui
     run_build(e, *desc, outs.data(), anchors.data(), count);
     for (u32 j = 0; j < count; ++j) instances[j].anchors = anchors[j];
     e.st.kernel_launches = ctx->launches;
-    return finish(ctx, e, stats, t0);
+    const sufgpu_status st = finish(ctx, e, stats, t0);
+    if (e.gate_held) {  // a build without the compute-first path leaves here
+      e.gate_held = false;
+      e.gate_out = std::chrono::steady_clock::now();
+      gate->unlock();
+    }
+    if (times && gate) *times = GateTimes{e.gate_in, e.gate_out};
+    return st;
   } catch (const CudaError& err) {
     cudaGetLastError();
     return fail(ctx, SUFGPU_BUILD_FAILURE,
@@ -2065,13 +2087,23 @@ extern "C" sufgpu_status sufgpu_build_collection(sufgpu_ctx* ctx, sufgpu_instanc
     }
     failed = true;
   };
-  auto build_parts = [&](sufgpu_ctx* w) {
+  ctx->collection_trace.assign(parts.size(), sufgpu_ctx::PartTrace{});
+  auto since = [&](std::chrono::steady_clock::time_point t) {
+    return std::chrono::duration<double>(t - t0).count();
+  };
+  auto build_parts = [&](sufgpu_ctx* w, u32 worker) {
     while (!failed.load()) {
       const size_t i = next.fetch_add(1);
       if (i >= parts.size()) return;
       sufgpu_instance* inst = instances + parts[i].first;
+      const auto started = std::chrono::steady_clock::now();
+      GateTimes gt{started, started};
       const sufgpu_status st = build_batch(w, inst, parts[i].second, desc, &part_stats[i],
-                                           workers > 1 ? &gate : nullptr);
+                                           workers > 1 ? &gate : nullptr, &gt);
+      const auto ended = std::chrono::steady_clock::now();
+      if (workers == 1) gt.out = ended;
+      ctx->collection_trace[i] =
+          sufgpu_ctx::PartTrace{worker, since(started), since(gt.in), since(gt.out), since(ended)};
       if (st != SUFGPU_OK) {
         record_failure(st, w->last_error);
         return;
@@ -2099,20 +2131,20 @@ extern "C" sufgpu_status sufgpu_build_collection(sufgpu_ctx* ctx, sufgpu_instanc
       }
     }
   };
-  auto work = [&](sufgpu_ctx* w) {
+  auto work = [&](sufgpu_ctx* w, u32 worker) {
     try {
-      build_parts(w);
+      build_parts(w, worker);
     } catch (const std::exception& err) {  // host allocation in the anchor copies
       record_failure(SUFGPU_BUILD_FAILURE, err.what());
     }
   };
   std::vector<std::thread> threads;
   try {
-    for (u32 w = 1; w < workers; ++w) threads.emplace_back(work, pool[w]);
+    for (u32 w = 1; w < workers; ++w) threads.emplace_back(work, pool[w], w);
   } catch (const std::system_error&) {
     // No more host threads: the workers started so far take every sub-batch.
   }
-  work(pool[0]);
+  work(pool[0], 0u);
   for (auto& t : threads) t.join();
   if (first_status != SUFGPU_OK) return fail(ctx, first_status, first_error);
   if (stats) {
@@ -2141,6 +2173,22 @@ extern "C" sufgpu_status sufgpu_build_collection(sufgpu_ctx* ctx, sufgpu_instanc
         std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     *stats = sum;
   }
+  return SUFGPU_OK;
+}
+
+extern "C" uint64_t sufgpu_collection_parts(const sufgpu_ctx* ctx) {
+  return ctx ? ctx->collection_trace.size() : 0;
+}
+
+extern "C" sufgpu_status sufgpu_collection_trace(const sufgpu_ctx* ctx, uint64_t index,
+                                                 uint32_t* worker, double* times) {
+  if (!ctx || index >= ctx->collection_trace.size() || !times) return SUFGPU_INVALID_INPUT;
+  const auto& t = ctx->collection_trace[index];
+  if (worker) *worker = t.worker;
+  times[0] = t.start;
+  times[1] = t.gate_in;
+  times[2] = t.gate_out;
+  times[3] = t.end;
   return SUFGPU_OK;
 }
 

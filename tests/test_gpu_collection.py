@@ -50,6 +50,20 @@ def test_collection_sa_and_lcp_only(ctx, lcp, workers):
             assert (r.lcp == one.lcp).all()
 
 
+def test_collection_trace(ctx):
+    ts = texts(12, 99)
+    ctx.build_collection(ts, isa_bits=0, batch_symbols=100_000, workers=2)
+    trace = ctx.collection_trace()
+    assert len(trace) >= 2
+    for t in trace:
+        assert t["worker"] in (0, 1)
+        assert 0 <= t["start"] <= t["gate_in"] <= t["gate_out"] <= t["end"]
+    # The gate admits one build at a time.
+    held = sorted((t["gate_in"], t["gate_out"]) for t in trace)
+    for (a0, a1), (b0, b1) in zip(held, held[1:]):
+        assert a1 <= b0
+
+
 def test_collection_byte_coded_anchors_survive(ctx):
     """Anchors of every sub-batch stay readable after the later sub-batches."""
     ts = [synth.uneven_reference(i, 40_000 + 5_000 * i).logical_text() for i in range(9)]
