@@ -1,9 +1,10 @@
 // Prefix-doubling suffix sort kernels.
 //
 // Seed: every position gets a 64-bit key packing its first s symbols (symbols
-// remapped to 1..sigma, 0 = past the end of the instance), and (key, position)
-// pairs are radix sorted.  Groups of equal keys then get their head row as
-// rank; rows in groups of two or more go to the active list.
+// remapped to 1..sigma, 0 = past the end of the instance; or, for a DNA text,
+// 2 bits per A/C/G/T plus a tag, see TwoBitSeed), and (key, position) pairs
+// are radix sorted.  Groups of equal keys then get their head row as rank;
+// rows in groups of two or more go to the active list.
 //
 // Round (prefix length h -> 2h): each active position p gets the composite key
 // (dense group id, rank[p+h] + 1 or 0 past the end); a radix sort of the
