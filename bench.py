@@ -2,10 +2,15 @@
 """SA+ISA+LCP build throughput on B200 (Gsym/s), one JSON line.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload plain100m|plain4m|batched]
+                    [--workload plain3g|plain100m|plain4m|batched|served]
+
+The default workload is the human-scale plain build: 3.1 Gbp, 25 contigs,
+Low-memory profile (64-bit construction, split40 SA storage, byte-coded LCP,
+no resident ISA).  The batched-over-one-at-a-time ratio of the uneven
+collection is a second invocation: ``--workload batched --count 1024``.
 
 A step is one complete build of the workload: seed sort, doubling rounds,
-ISA, PHI LCP and packing.  ``value`` uses a device-resident text and device
+ISA, LCP and packing.  ``value`` uses a device-resident text and device
 output planes and the device time of each build (CUDA events recorded by the
 library on its own stream, first to last); L2 is flushed (256 MiB write)
 between steps.  ``e2e`` is the same build through the C ABI with pinned host
@@ -40,7 +45,7 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="plain100m",
+    ap.add_argument("--workload", default="plain3g",
                     choices=["plain100m", "plain4m", "plain3g", "batched", "served"])
     ap.add_argument("--count", type=int, default=256,
                     help="references in the batched workload (1,024 in the full collection)")
@@ -157,35 +162,74 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-# Algorithmic-byte model of one build (per-unit figures in DESIGN.md)
+# Algorithmic-byte model of one build
 # ---------------------------------------------------------------------------
-def build_bytes(text: np.ndarray, sa: np.ndarray, isa: np.ndarray, lcp: np.ndarray,
-                w_sa: int = 4, w_isa: int = 4, w_lcp: int = 4, seed: int = 21) -> int:
-    n = int(text.size)
+def model_bytes(n: int, a_k: list[int], lcp_nonzero: int, w_sa: int, w_isa: int,
+                lcp_kind: str, w_lcp: int = 4, anchors: int = 0, w_anchor: int = 4) -> int:
+    """Algorithmic bytes B of one build of n symbols:
+
+        B = n(1 + 2(8+W) + W)            seed: text read, one (key, idx) sort pass, rank write
+          + sum_k 8 W A_k                doubling rounds over still-unsorted suffixes
+          + n(W + w_isa)                 ISA emit
+          + 6nW + 2C                     PHI scatter, PLCP read/write, LCP gather; C compares
+          + n(W + w_sa)                  SA pack to the stored width
+          + n w_lcp | n + 2 w_anchor #anchors   raw or byte-coded LCP
+
+    with W = 4 if n-1 fits 32 bits else 8, A_k = #{suffixes i : m(i) >= 21 *
+    2^(k-1)}, m(i) = max(LCP[ISA[i]], LCP[ISA[i]+1]) (LCP[n] = 0) and C =
+    sum_p (PLCP[p] - max(PLCP[p-1] - 1, 0) + 1).  The last sum telescopes: for a
+    sentinel-terminated text (PLCP of the last position is 0) C = n + #{rows r
+    : LCP[r] >= 1}.  A_k and C depend only on the text."""
     W = 4 if n - 1 <= 0xFFFFFFFF else 8
-    lcp64 = lcp.astype(np.int64)
-    nxt = np.append(lcp64[1:], 0)
-    row = isa.astype(np.int64)
-    m = np.maximum(lcp64[row], nxt[row])
-    rounds_bytes = 0
-    k = 1
-    while True:
-        a_k = int(np.count_nonzero(m >= seed * (1 << (k - 1))))
-        if a_k == 0:
-            break
-        rounds_bytes += 8 * W * a_k
-        k += 1
-    plcp = np.empty(n, np.int64)
-    plcp[sa.astype(np.int64)] = lcp64
-    prev = np.concatenate([[0], np.maximum(plcp[:-1] - 1, 0)])
-    compares = int(np.sum(plcp - prev + 1))
     b = n * (1 + 2 * (8 + W) + W)
-    b += rounds_bytes
+    b += sum(8 * W * a for a in a_k)
     b += n * (W + w_isa)
-    b += n * 6 * W + 2 * compares
+    b += n * 6 * W + 2 * (n + lcp_nonzero)
     b += n * (W + w_sa)
-    b += n * w_lcp
+    b += n * w_lcp if lcp_kind == "raw" else n + 2 * w_anchor * anchors
     return int(b)
+
+
+def text_statistics(lcp: np.ndarray, seed: int = 21) -> tuple[list[int], int]:
+    """A_k (k = 1..R) and #{r : LCP[r] >= 1} from a row-order LCP (host)."""
+    l = np.asarray(lcp).astype(np.int64)
+    m = np.maximum(l, np.append(l[1:], 0))
+    a_k, k = [], 1
+    while True:
+        a = int(np.count_nonzero(m >= seed * (1 << (k - 1))))
+        if a == 0:
+            break
+        a_k.append(a)
+        k += 1
+    return a_k, int(np.count_nonzero(l >= 1))
+
+
+def text_statistics_device(d_lcp, torch, seed: int = 21, chunk: int = 1 << 28):
+    """text_statistics over a device-resident uint32 LCP plane (an int32
+    tensor holding the bits), in chunks, with the counts reduced on the
+    device: a multi-Gsym build needs no host copy of its LCP."""
+    n = int(d_lcp.numel())
+    counts = {}
+    nonzero = 0
+    for s in range(0, n, chunk):
+        e = min(n, s + chunk)
+        cur = d_lcp[s:e].to(torch.int64) & 0xFFFFFFFF
+        nxt = torch.zeros_like(cur)
+        nxt[: e - s - 1] = cur[1:]
+        if e < n:
+            nxt[e - s - 1] = int(d_lcp[e].item()) & 0xFFFFFFFF
+        m = torch.maximum(cur, nxt)
+        nonzero += int((cur >= 1).sum().item())
+        k = 1
+        while True:
+            a = int((m >= seed * (1 << (k - 1))).sum().item())
+            if a == 0:
+                break
+            counts[k] = counts.get(k, 0) + a
+            k += 1
+        del cur, nxt, m
+    a_k = [counts[k] for k in sorted(counts)]
+    return a_k, nonzero
 
 
 def load_traffic(kernel: str):
@@ -202,6 +246,30 @@ def load_traffic(kernel: str):
 # ---------------------------------------------------------------------------
 # Reference arm and CPU baseline (the reference's own CPU build path)
 # ---------------------------------------------------------------------------
+def host_info() -> dict:
+    """CPU model, logical CPUs, host RAM and the compiler that built the
+    reference's CPU code (recorded beside every CPU timing)."""
+    info = {"cpu": None, "nproc": os.cpu_count(), "ram_gb": None, "compiler": None}
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                info["cpu"] = line.split(":", 1)[1].strip()
+                break
+        for line in Path("/proc/meminfo").read_text().splitlines():
+            if line.startswith("MemTotal"):
+                info["ram_gb"] = round(int(line.split()[1]) / 1048576, 1)
+                break
+    except OSError:
+        pass
+    try:
+        out = subprocess.run([os.environ.get("CXX", "g++"), "--version"], capture_output=True,
+                             text=True, timeout=10).stdout
+        info["compiler"] = (out.splitlines() or [None])[0]
+    except (OSError, subprocess.TimeoutExpired):
+        pass
+    return info
+
+
 def cpu_reference_step(text: np.ndarray, threads: int) -> float:
     import oracle
     t0 = time.perf_counter()
@@ -238,7 +306,8 @@ def run_reference(args, texts, desc):
                          "kind": "reference",
                          "sample": f"first {sample.size} symbols of the workload text; "
                                    "libdivsufsort64 + ISA + Kasai LCP through "
-                                   "detail::BuildDivsufsort64 (threads=%d)" % threads},
+                                   "detail::BuildDivsufsort64 (threads=%d)" % threads,
+                         "host": host_info()},
         "e2e": {"value": value, "unit": "Gsym/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -438,6 +507,7 @@ def main():
     clocks.start()
     device_seconds = 0.0
     launches = 0
+    last_anchors = None
     wall0 = time.perf_counter()
     for k in range(args.steps):
         flush.fill_(k & 0xff)
@@ -445,6 +515,7 @@ def main():
         st = device_step()
         device_seconds += st["device_seconds"]
         launches += st["kernel_launches"]
+        last_anchors = st.get("anchors")
     torch.cuda.synchronize()
     wall = time.perf_counter() - wall0
     clock_info = clocks.stop()
@@ -541,16 +612,43 @@ def main():
                        "GBps": (k["bytes"] / k["seconds"] / 1e9) if k["seconds"] else None}
                       for k in profile), key=lambda k: -k["ms_per_step"])
 
+    # Whole-build roofline: the algorithmic bytes of every build in a step
+    # (A_k and C from each text's exact row LCP, reduced on the device) over
+    # the step's device time.  A byte-coded build has no raw LCP plane, so one
+    # extra build of the same text with raw LCP32 supplies it (the values
+    # depend only on the text); the timed buffers are freed first.
     whole = None
-    if rank == 0 and len(texts) == 1 and isa_bits and lcp_enc == sg.LcpEncoding.RAW32:
-        # Algorithmic bytes of the whole build from this build's own exact
-        # outputs (A_k, C depend only on the text).
-        sa = d_out[0]["sa_low"].cpu().numpy().view(np.uint32)
-        isa = d_out[0]["isa_low"].cpu().numpy().view(np.uint32)
-        lcp = d_out[0]["lcp"].cpu().numpy().view(np.uint32)
-        b = build_bytes(texts[0], sa, isa, lcp)
-        whole = {"algorithmic_bytes": b, "achieved_GBps": b / step_seconds / 1e9,
-                 "frac": b / step_seconds / 1e9 / peak}
+    w_sa = {32: 4, 40: 5, 48: 6, 64: 8}[sa_bits]
+    kind = "raw" if lcp_enc == sg.LcpEncoding.RAW32 else "byte"
+    anchors_total = int(last_anchors) if last_anchors is not None else 0
+    total_bytes = 0
+    if kind == "raw":
+        for j, t in enumerate(texts):
+            a_k, nz = text_statistics_device(d_out[j]["lcp"], torch)
+            total_bytes += model_bytes(int(t.size), a_k, nz, w_sa, isa_bits // 8, "raw")
+    else:
+        n0 = int(texts[0].size)
+        d_out.clear()
+        flush = None
+        torch.cuda.empty_cache()
+        d_sa = torch.empty(n0, dtype=torch.int32, device=dev)
+        d_lcp = torch.empty(n0, dtype=torch.int32, device=dev)
+        ctx.build_device(d_texts[0].data_ptr(), n0, {"sa_low": d_sa.data_ptr(),
+                                                     "lcp": d_lcp.data_ptr()},
+                         sa_bits=32, isa_bits=0, lcp=sg.LcpEncoding.RAW32)
+        del d_sa
+        ctx.close()  # the build arena is not needed any more
+        torch.cuda.empty_cache()
+        a_k, nz = text_statistics_device(d_lcp, torch)
+        del d_lcp
+        total_bytes = model_bytes(n0, a_k, nz, w_sa, isa_bits // 8, "byte",
+                                  anchors=anchors_total)
+    whole = {"algorithmic_bytes": total_bytes,
+             "achieved_GBps": total_bytes / step_seconds / 1e9,
+             "peak_GBps": peak, "frac": total_bytes / step_seconds / 1e9 / peak,
+             "peak_source": peak_kind,
+             "A_k": a_k if len(texts) == 1 else None,
+             "anchors": anchors_total if kind == "byte" else None}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -562,7 +660,8 @@ def main():
                    "kind": "reference",
                    "sample": f"first {sample.size} symbols of the workload text, "
                              "libdivsufsort64 + Kasai LCP via detail::BuildDivsufsort64, "
-                             "1 thread (divsufsort is serial)"}
+                             "1 thread (divsufsort is serial)",
+                   "host": host_info()}
 
     if rank == 0:
         line = {

@@ -349,16 +349,17 @@ SUFGPU_API void sufgpu_host_free(void *ptr);
  * device, so a foreign cudaMalloc fails or fragments it), callbacks that run
  * while an allocation lock is held, and loops that cannot block on an
  * allocation.  Its scratch is one fixed array compiled into the library
- * (about 11.6 MB, held on every GPU that loads the library until exit); it
- * calls no cudaMalloc, cudaFree or allocating library routine.  n above
- * SUFGPU_NOALLOC_MAX_SYMBOLS returns SUFGPU_INVALID_INPUT.  All calls share
- * the array (each clears what must start at zero), so calls that overlap on
- * the GPU race and must be serialized by the caller.  The first call on a
- * device resolves the array's address and a kernel attribute with that
- * device current; make it before any stream capture.  stream is a
- * cudaStream_t (NULL = default stream); the call returns after the result is
- * complete.  No counterpart in the reference: sufkit computes LCP on the host
- * with its own allocations (src/divsufsort_backend.cpp:121-150). */
+ * (11.4 MiB, held on every GPU that loads the library until exit); it calls
+ * no cudaMalloc, cudaFree or allocating library routine.  n above
+ * SUFGPU_NOALLOC_MAX_SYMBOLS returns SUFGPU_INVALID_INPUT.  sa must be a
+ * permutation of [0, n); an entry outside that range is detected on the
+ * device and returns SUFGPU_BUILD_FAILURE.  All calls share the array (each
+ * clears what must start at zero), so calls that overlap on the GPU race and
+ * must be serialized by the caller.  The first call on a device does that
+ * device's set-up (resolves the array's address and a kernel attribute with
+ * the device current); make it before any stream capture begins.  stream is
+ * a cudaStream_t (NULL = default stream); the call returns after the result
+ * is complete.  This entry point has no counterpart in the reference. */
 SUFGPU_API sufgpu_status sufgpu_lcp_noalloc(const uint8_t *text, const uint32_t *sa,
                                             uint64_t n, uint32_t *lcp, void *stream);
 

@@ -3,6 +3,11 @@
 * ``port()``  -> liboracle.so, our C restatement (oracle/sa_oracle.c).
 * ``ref()``   -> _ref/libsufref.so, the reference's own sources compiled by
   oracle/Makefile (None when it has not been built).
+* ``sufkit_index(...)`` / ``sufkit_load(...)`` run sufkit's public
+  SuffixArray::Build + Save and Load in a child process, through libsufref.so
+  or through _ref/libsufref_cuda.so (the same sources with the constructor
+  translation unit replaced by the sufgpu drop-in), so that both builds of
+  one FASTA can be compared as saved files.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
 package, and only as the checker or the timed CPU baseline.
@@ -19,18 +24,22 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 PORT_PATH = HERE / "liboracle.so"
 REF_PATH = HERE / "_ref" / "libsufref.so"
+REF_CUDA_PATH = HERE / "_ref" / "libsufref_cuda.so"
 
 P = ctypes.c_void_p
 U64 = ctypes.c_uint64
 
 
-def build(reference: Optional[str] = None) -> None:
+def build(reference: Optional[str] = None, cuda_seam: bool = False) -> None:
     """Compiles liboracle.so, and _ref/libsufref.so when the reference tree is
-    available (make -C oracle)."""
+    available (make -C oracle); with cuda_seam also _ref/libsufref_cuda.so
+    (needs sufkit_b200/libsufgpu.so)."""
     cmd = ["make", "-C", str(HERE), "-j8", "-s"]
     if reference:
         cmd.append(f"REF={reference}")
     subprocess.run(cmd, check=True)
+    if cuda_seam and REF_PATH.exists():
+        subprocess.run(cmd + ["cuda_seam"], check=True)
 
 
 _port = None
@@ -343,3 +352,66 @@ def ref_encode_fasta(path) -> tuple[np.ndarray, int]:
     if rc < 0:
         raise ValueError(lib.sufref_last_error().decode())
     return out, fp.value
+
+
+# --------------------------------------------------------------------------
+# sufkit's public build/save/load, in a child process (two libraries export
+# the same sufkit symbols, so each run gets a process of its own)
+# --------------------------------------------------------------------------
+_CHILD = r"""
+import ctypes, json, sys
+args = json.loads(sys.argv[1])
+lib = ctypes.CDLL(args["lib"])
+lib.sufref_last_error.restype = ctypes.c_char_p
+out = {}
+if args["op"] == "build":
+    f = lib.sufref_suffix_array_build
+    f.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                  ctypes.c_uint32, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_void_p]
+    stats = (ctypes.c_double * 12)()
+    info = (ctypes.c_uint64 * 6)()
+    rc = f(args["fasta"].encode(), args["profile"], args["width"], args["storage"],
+           args["acceleration"], args["threads"], args["save"].encode(), stats, info)
+    out = {"rc": rc, "stats": list(stats), "info": list(info)}
+else:
+    f = lib.sufref_load_query
+    f.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_void_p,
+                  ctypes.c_uint64, ctypes.c_void_p]
+    occ = ctypes.c_uint64()
+    rows = (ctypes.c_uint64 * args["rows"])()
+    info = (ctypes.c_uint64 * 3)()
+    rc = f(args["path"].encode(), args["pattern"].encode(), ctypes.byref(occ), rows,
+           args["rows"], info)
+    out = {"rc": rc, "count": occ.value, "rows": list(rows), "info": list(info)}
+if out["rc"] != 0:
+    out["error"] = lib.sufref_last_error().decode()
+print(json.dumps(out))
+"""
+
+
+def _child(args: dict) -> dict:
+    import json
+    import sys
+    proc = subprocess.run([sys.executable, "-c", _CHILD, json.dumps(args)], capture_output=True,
+                          text=True, timeout=3600)
+    if proc.returncode != 0:
+        raise RuntimeError(f"child failed ({proc.returncode}): {proc.stderr[-2000:]}")
+    return json.loads(proc.stdout.strip().splitlines()[-1])
+
+
+def sufkit_index(fasta, save_path, profile: int = 0, coordinate_width: int = 64,
+                 storage_width: int = 0, acceleration: int = -1, threads: int = 1,
+                 cuda: bool = False) -> dict:
+    """SuffixArray::Build of a FASTA with sufkit's own code, then Save.
+    profile 0 = Fast, 1 = Low-memory; cuda selects libsufref_cuda.so."""
+    lib = REF_CUDA_PATH if cuda else REF_PATH
+    return _child({"op": "build", "lib": str(lib), "fasta": str(fasta), "profile": profile,
+                   "width": coordinate_width, "storage": storage_width,
+                   "acceleration": acceleration, "threads": threads, "save": str(save_path)})
+
+
+def sufkit_load(path, pattern: str, rows: int) -> dict:
+    """SuffixArray::Load (full validation) with the reference's own library,
+    then Count(pattern) and SuffixAt(0..rows)."""
+    return _child({"op": "load", "lib": str(REF_PATH), "path": str(path), "pattern": pattern,
+                   "rows": rows})

@@ -463,4 +463,28 @@ int sufref_suffix_array_rows(const char* fasta_path, int profile,
   }
 }
 
+// SuffixArray::Load of a saved .sufidx (src/suffix_array.cpp, which fully
+// validates containers, CRCs and semantics), then Count(pattern) and
+// SuffixAt(row) for rows [0, count).  info[0..2] = text_symbols,
+// stored_coordinate_width, lcp_encoding of the loaded index.
+int sufref_load_query(const char* path, const char* pattern, uint64_t* occurrences,
+                      uint64_t* rows_out, uint64_t count, uint64_t* info) {
+  try {
+    auto index = sufkit::SuffixArray::Load(path);
+    const auto index_info = index.GetInfo();
+    if (info != nullptr) {
+      info[0] = index_info.text_symbols;
+      info[1] = index_info.stored_coordinate_width;
+      info[2] = static_cast<uint64_t>(index_info.lcp_encoding);
+    }
+    if (occurrences != nullptr && pattern != nullptr) *occurrences = index.Count(pattern);
+    for (uint64_t row = 0; row < count && row < index_info.text_symbols; ++row) {
+      rows_out[row] = index.SuffixAt(row);
+    }
+    return 0;
+  } catch (const std::exception& error) {
+    return Fail(error);
+  }
+}
+
 }  // extern "C"

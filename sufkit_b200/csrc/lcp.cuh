@@ -68,7 +68,15 @@ lcp_rows_kernel(const u8* __restrict__ text, const u32* __restrict__ sa, u64 n,
       b = sa[r];
       cur.locate(segs.begin, segs.count, r);
       const u64 seg_first = cur.lo;
-      if (r == seg_first) {
+      // A caller-supplied SA (sufgpu_lcp_noalloc) may hold entries outside
+      // the row's instance: flag them and skip the row instead of reading
+      // text past the instance end.
+      const bool b_bad = b < seg_first || b >= cur.hi;
+      const bool a_bad = r != seg_first && (sa[r - 1] < seg_first || sa[r - 1] >= cur.hi);
+      if (b_bad || a_bad) {
+        flag_error(flags, kErrBounds);
+        lcp[r] = 0;
+      } else if (r == seg_first) {
         lcp[r] = 0;
       } else {
         a = sa[r - 1];

@@ -14,15 +14,20 @@
 //
 // Limits and sharing:
 //   * n <= SUFGPU_NOALLOC_MAX_SYMBOLS (2^18); larger inputs are rejected.
-//   * The scratch array (about 11.6 MB) exists on every GPU that loads the
-//     library, from load until process exit.
+//   * The scratch array (kScratchBytes = 11,952,896 bytes, 11.4 MiB; a
+//     static_assert below keeps it under 12 MiB) exists on every GPU that
+//     loads the library, from load until process exit.
+//   * sa must be a permutation of [0, n).  An entry outside [0, n) is
+//     flagged by the row kernel, which skips that row's text compare, and
+//     the call returns SUFGPU_BUILD_FAILURE.
 //   * All calls share it and it keeps the previous call's contents; each call
 //     clears what must start at zero.  Calls that overlap on the GPU (two
 //     streams, two host threads) race on it and must be serialized by the
 //     caller.
-//   * The first call on a device resolves the array's device address (with
-//     that device current) and sets a kernel attribute; make that first call
-//     before any stream capture.
+//   * The first call on a device does the one-time set-up for that device:
+//     with the device current it resolves the array's device address
+//     (cudaGetSymbolAddress) and sets a kernel attribute.  Make that first
+//     call on each device before any stream capture begins.
 
 #include <cuda_runtime.h>
 
@@ -60,6 +65,7 @@ constexpr u64 kOffSmall = kOffDigits + align256(kMaxPasses * kRadixDigits * 8);
 // counters[64] (u32), scalars[16] (u64), flags.
 constexpr u64 kSmallBytes = 16 + 16 + 8 + 256 + 128 + sizeof(DeviceFlags);
 constexpr u64 kScratchBytes = kOffSmall + align256(kSmallBytes);
+static_assert(kScratchBytes <= (u64(12) << 20), "the documented scratch bound is 12 MiB");
 
 static __device__ __align__(256) unsigned char g_lcp_scratch[kScratchBytes];
 

@@ -62,9 +62,10 @@ def _n_runs(rng, genome: np.ndarray, total: int, lo: int, hi: int, log: bool) ->
 
 
 def _interspersed(rng, genome: np.ndarray, fraction: float, families: int, gc: float,
-                  lo: int = 300, hi: int = 6000, div=(0.05, 0.15)) -> None:
-    lengths = np.exp(rng.uniform(np.log(lo), np.log(hi), size=families)).astype(np.int64)
-    consensus = [_bases(rng, int(L), gc) for L in lengths]
+                  lo: int = 300, hi: int = 6000, div=(0.05, 0.15), consensus=None) -> None:
+    if consensus is None:
+        lengths = np.exp(rng.uniform(np.log(lo), np.log(hi), size=families)).astype(np.int64)
+        consensus = [_bases(rng, int(L), gc) for L in lengths]
     target = int(fraction * genome.size)
     placed = 0
     while placed < target:
@@ -174,20 +175,57 @@ def repeat_rich_100mbp(scale: float = 1.0, seed: Optional[int] = None) -> Refere
     return Reference(_split(genome, lengths))
 
 
-def human_scale_3gbp(scale: float = 1.0, seed: Optional[int] = None) -> Reference:
+def _human_contig(task) -> np.ndarray:
+    """One contig of the human-scale reference from its own random stream:
+    bases at GC 41%, interspersed copies of the shared repeat families up to
+    50% of the contig, segmental duplications (10-200 kbp at 1-3% divergence)
+    up to 1%, and the contig's share of the N runs (log-uniform lengths)."""
+    seed, index, length, consensus, n_budget, lo, hi = task
+    rng = np.random.default_rng([seed, index])
+    genome = np.empty(length, np.uint8)
+    step = 1 << 25  # bounded temporaries for 250 Mbp contigs
+    for s in range(0, length, step):
+        genome[s:s + step] = _bases(rng, min(step, length - s), 0.41)
+    _interspersed(rng, genome, 0.50, len(consensus), 0.41, consensus=consensus)
+    _segdups(rng, genome, 0.01, 0.41)
+    _n_runs(rng, genome, n_budget, lo, hi, log=True)
+    return genome
+
+
+def human_scale_3gbp(scale: float = 1.0, seed: Optional[int] = None,
+                     workers: Optional[int] = None) -> Reference:
     """Workload 3: 25 contigs (50-250 Mbp scaled to 3.1 Gbp), GC 41%; 50%
-    interspersed repeats as in workload 2, 1% segmental duplications (10-200
-    kbp at 1-3% divergence), 150 Mbp of N in runs of 10 kbp-3 Mbp (scaled)."""
-    rng = np.random.default_rng(BASE_SEED + 2 if seed is None else seed)
+    interspersed repeats from 500 families as in workload 2, 1% segmental
+    duplications (10-200 kbp at 1-3% divergence), 150 Mbp of N in runs of
+    10 kbp-3 Mbp (scaled), spread over the contigs by length.
+
+    Each contig comes from its own random stream (seed, contig index), so the
+    contigs are generated in parallel (spawned worker processes, safe after
+    CUDA initialisation) for large scales; the result does not depend on the
+    number of workers."""
+    base = BASE_SEED + 2 if seed is None else seed
+    rng = np.random.default_rng(base)
     total = max(10_000, int(3.1e9 * scale))
     lengths = _scaled_lengths(rng.uniform(50e6, 250e6, size=25), total)
-    genome = _bases(rng, total, 0.41)
-    _interspersed(rng, genome, 0.50, 500, 0.41)
-    _segdups(rng, genome, 0.01, 0.41)
+    fam_len = np.exp(rng.uniform(np.log(300), np.log(6000), size=500)).astype(np.int64)
+    consensus = [_bases(rng, int(L), 0.41) for L in fam_len]
     n_total = int(150e6 * scale)
     hi = max(20, int(3e6 * min(1.0, scale * 10)))
-    _n_runs(rng, genome, n_total, min(10_000, hi // 2), hi, log=True)
-    return Reference(_split(genome, lengths))
+    lo = min(10_000, hi // 2)
+    n_share = _scaled_lengths(lengths.astype(np.float64), n_total) if n_total >= 25 else \
+        np.zeros(25, np.int64)
+    tasks = [(base, i, int(lengths[i]), consensus, int(n_share[i]), lo, hi) for i in range(25)]
+    if workers is None:
+        import os
+        workers = min(25, os.cpu_count() or 1) if total >= 64_000_000 else 1
+    if workers > 1:
+        import multiprocessing as mp
+        from concurrent.futures import ProcessPoolExecutor
+        with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+            contigs = list(ex.map(_human_contig, tasks))
+    else:
+        contigs = [_human_contig(t) for t in tasks]
+    return Reference(contigs)
 
 
 def uneven_collection(count: int = 1024, scale: float = 1.0,

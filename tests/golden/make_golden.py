@@ -1,7 +1,7 @@
 """Regenerates tests/golden/*.npz from the reference's own compiled code.
 
-Run in a container that has the sufkit sources at REF (default
-/root/reference):  make -C oracle ref && python tests/golden/make_golden.py
+Run where the sufkit sources are at $SUFKIT_REFERENCE (default: the build
+container's checkout):  make -C oracle ref && python tests/golden/make_golden.py
 
 Inputs are the reference's own test texts, rebuilt from the generators its C++
 tests use (paths inside the sufkit project):

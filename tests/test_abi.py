@@ -106,3 +106,22 @@ def test_context_without_gpu_fails_loudly():
     with pytest.raises(sg.SufkitError) as err:
         sg.Context(0)
     assert err.value.code == sg.ErrorCode.BUILD_FAILURE
+
+
+def test_sufkit_dropin_library_fails_loudly_without_a_device(tmp_path):
+    """sufkit's own Build through the drop-in constructor raises
+    sufkit::Error(kBuildFailure) when no CUDA device is usable: there is no
+    CPU fallback behind it."""
+    import oracle
+    import torch
+    from sufkit_b200 import synth
+    if not oracle.REF_CUDA_PATH.exists():
+        pytest.skip("libsufref_cuda.so was not built")
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    fasta = tmp_path / "a.fa"
+    synth.plain_4mbp(scale=0.01).write_fasta(fasta)
+    out = oracle.sufkit_index(fasta, tmp_path / "g.sufidx", 0, 32, 32, cuda=True)
+    assert out["rc"] == 6  # 1 + ErrorCode::kBuildFailure
+    assert "CUDA" in out["error"]
+    assert not (tmp_path / "g.sufidx").exists()

@@ -5,13 +5,16 @@ under another framework's allocator, inside allocation-locked callbacks, or in
 loops that must not block on an allocation): all of its scratch is one fixed
 array inside the library.  These tests call it through the C ABI on
 device-resident inputs and compare it with the LCP that the regular entry
-point (sufgpu_build) produces, on consecutive calls, so stale scratch contents
-from the previous call cannot leak into the next result.  The file is named
-to be collected last.
+point (sufgpu_build) produces and with the oracle's Kasai LCP (the
+reference's divsufsort64 build when it was compiled, else the C
+restatement), on consecutive calls, so stale scratch contents from the
+previous call cannot leak into the next result.  The file is named to be
+collected last.
 """
 import numpy as np
 import pytest
 
+import oracle
 import sufkit_b200 as sg
 from sufkit_b200 import synth
 
@@ -41,6 +44,12 @@ def _noalloc(lib, torch, text, sa):
     return status, d_lcp.cpu().numpy().view(np.uint32)
 
 
+def _oracle_lcp(text):
+    if oracle.ref() is not None:
+        return oracle.ref_adapter(text, 64)[2]
+    return oracle.full_build(text)[2]
+
+
 def test_noalloc_lcp_matches_build_on_consecutive_calls():
     torch = pytest.importorskip("torch")
     lib = sg.library()
@@ -51,6 +60,24 @@ def test_noalloc_lcp_matches_build_on_consecutive_calls():
             status, lcp = _noalloc(lib, torch, text, built.sa_low)
             assert status == 0
             assert (lcp == built.lcp).all()
+            assert (lcp.astype(np.uint64) == _oracle_lcp(text).astype(np.uint64)).all()
+
+
+def test_noalloc_flags_suffix_array_entries_out_of_range():
+    """An SA entry >= n is caught by the row kernel's range check (the row's
+    text compare is skipped, so nothing is read past the text) and the call
+    reports a build failure; the next call with a valid SA is exact again."""
+    torch = pytest.importorskip("torch")
+    lib = sg.library()
+    text = synth.random_text(np.random.default_rng(7), 5000, 4)
+    sa = oracle.suffix_array(text).astype(np.uint32)
+    bad = sa.copy()
+    bad[1234] = text.size + 100_000
+    status, _ = _noalloc(lib, torch, text, bad)
+    assert status == sg.ErrorCode.BUILD_FAILURE + 1
+    status, lcp = _noalloc(lib, torch, text, sa)
+    assert status == 0
+    assert (lcp.astype(np.uint64) == _oracle_lcp(text).astype(np.uint64)).all()
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch():
