@@ -303,6 +303,14 @@ typedef struct sufgpu_request_info {
   uint32_t rounds;        /* doubling rounds the reference took */
   uint32_t seed_symbols;
   sufgpu_anchors anchors; /* byte-coded encodings; valid until release */
+  /* Continuous batching: the server's iteration count (shared doubling
+   * rounds completed) when the request was admitted and when it finished,
+   * and how many requests were already in flight, mid-rounds, when it was
+   * merged into the running batch. */
+  uint64_t admit_iteration;
+  uint64_t finish_iteration;
+  uint32_t inflight_at_admit;
+  uint32_t reserved;
 } sufgpu_request_info;
 
 typedef struct sufgpu_server_stats {

@@ -415,3 +415,28 @@ def sufkit_load(path, pattern: str, rows: int) -> dict:
     then Count(pattern) and SuffixAt(0..rows)."""
     return _child({"op": "load", "lib": str(REF_PATH), "path": str(path), "pattern": pattern,
                    "rows": rows})
+
+
+# --------------------------------------------------------------------------
+# Digests for full-size collection checks (run in spawned worker processes)
+# --------------------------------------------------------------------------
+def digest_planes(sa: np.ndarray, lcp: np.ndarray) -> tuple[str, str]:
+    """blake2b of the SA and LCP rows as little-endian uint32 words (equal
+    digests <=> equal rows, word for word)."""
+    import hashlib
+    sa32 = np.ascontiguousarray(np.asarray(sa).astype(np.uint32))
+    lcp32 = np.ascontiguousarray(np.asarray(lcp).astype(np.uint32))
+    return (hashlib.blake2b(sa32.tobytes(), digest_size=20).hexdigest(),
+            hashlib.blake2b(lcp32.tobytes(), digest_size=20).hexdigest())
+
+
+def uneven_reference_digests(task) -> tuple[int, int, str, str]:
+    """Reference `index` of the bacterial collection (its own random stream,
+    sufkit_b200.synth.uneven_reference), built by the reference's
+    divsufsort64 + Kasai: (index, n, SA digest, LCP digest)."""
+    from sufkit_b200 import synth
+    index, total = task
+    text = synth.uneven_reference(index, total).logical_text()
+    sa, _, lcp, _ = ref_adapter(text, 64)
+    d_sa, d_lcp = digest_planes(sa, lcp)
+    return index, int(text.size), d_sa, d_lcp

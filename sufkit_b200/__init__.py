@@ -111,7 +111,9 @@ class _ServerConfig(ctypes.Structure):
 class _RequestInfo(ctypes.Structure):
     _fields_ = [("queue_seconds", ctypes.c_double), ("latency_seconds", ctypes.c_double),
                 ("rounds", ctypes.c_uint32), ("seed_symbols", ctypes.c_uint32),
-                ("anchors", _Anchors)]
+                ("anchors", _Anchors), ("admit_iteration", ctypes.c_uint64),
+                ("finish_iteration", ctypes.c_uint64), ("inflight_at_admit", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
 
 
 class _ServerStats(ctypes.Structure):
@@ -536,6 +538,8 @@ class Context:
         if status != 0:
             _raise(status, self._error())
         self.last_stats = stats.as_dict()
+        # Byte-coded builds: the overflow anchors (host copies), else (None, None).
+        self.last_anchors = self._anchors(anchors, LcpEncoding(lcp))
         return self.last_stats
 
     def build_batch_device(self, texts: Sequence[tuple[int, int]], outs: Sequence[dict],
@@ -620,7 +624,10 @@ class Server:
         pos, val = Context._anchors(info.anchors, lcp)
         self._lib.sufgpu_server_release(self._h, ticket)
         stats = {"queue_seconds": info.queue_seconds, "latency_seconds": info.latency_seconds,
-                 "rounds": info.rounds, "seed_symbols": info.seed_symbols}
+                 "rounds": info.rounds, "seed_symbols": info.seed_symbols,
+                 "admit_iteration": info.admit_iteration,
+                 "finish_iteration": info.finish_iteration,
+                 "inflight_at_admit": info.inflight_at_admit}
         return BuildResult(anchor_positions=pos, anchor_values=val, stats=stats, **planes)
 
     def stats(self) -> dict:

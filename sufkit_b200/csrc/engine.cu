@@ -2280,6 +2280,11 @@ struct ServedRequest {
   std::vector<u8> anchor_pos, anchor_val;
   u64 anchor_count = 0;
   u32 anchor_bits = 0;
+  // Worker iterations (doubling rounds of the shared batch) completed when
+  // the request was admitted and when it finished, and how many requests
+  // were already in flight (mid-rounds) at its admission.
+  u64 admit_iteration = 0, finish_iteration = 0;
+  u32 inflight_at_admit = 0;
   std::chrono::steady_clock::time_point submitted, admitted, finished;
 };
 
@@ -2499,6 +2504,8 @@ void server_loop(sufgpu_server* S) {
         if (total + r->n > best_len) break;
         r->begin = best_begin + total;
         r->admitted = std::chrono::steady_clock::now();
+        r->admit_iteration = S->iterations;
+        r->inflight_at_admit = static_cast<u32>(S->inflight.size());
         total += r->n;
         group.push_back(r);
         S->queue.pop_front();
@@ -2594,6 +2601,7 @@ void server_loop(sufgpu_server* S) {
     for (auto& r : finished) {
       r->done = true;
       r->finished = now;
+      r->finish_iteration = S->iterations;
       S->latencies.push_back(std::chrono::duration<double>(now - r->submitted).count());
       ++S->completed;
       S->symbols_done += r->n;
@@ -2718,6 +2726,10 @@ static sufgpu_status request_info(const ReqPtr& r, sufgpu_request_info* info) {
     info->anchors = sufgpu_anchors{r->anchor_pos.empty() ? nullptr : r->anchor_pos.data(),
                                    r->anchor_val.empty() ? nullptr : r->anchor_val.data(),
                                    r->anchor_count, r->anchor_bits};
+    info->admit_iteration = r->admit_iteration;
+    info->finish_iteration = r->finish_iteration;
+    info->inflight_at_admit = r->inflight_at_admit;
+    info->reserved = 0;
   }
   return r->status;
 }

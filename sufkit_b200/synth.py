@@ -264,6 +264,32 @@ def uneven_reference(index: int, total: int, seed: Optional[int] = None) -> Refe
     return Reference(_split(_bases(rng, total, gc), lengths))
 
 
+def _uneven_text(task) -> np.ndarray:
+    index, total, seed = task
+    return uneven_reference(index, total, seed).logical_text()
+
+
+def uneven_texts(count: int = 1024, scale: float = 1.0, indices=None,
+                 seed: Optional[int] = None, workers: Optional[int] = None) -> list[np.ndarray]:
+    """Logical texts of references `indices` (default: all) of a bacterial
+    collection of `count` (uneven_sizes lengths, uneven_reference streams),
+    generated in spawned worker processes when the total is large; the result
+    does not depend on the number of workers."""
+    sizes = uneven_sizes(count, scale, None if seed is None else seed)
+    idx = list(range(count)) if indices is None else list(indices)
+    tasks = [(i, sizes[i], seed) for i in idx]
+    if workers is None:
+        import os
+        total = sum(sizes[i] for i in idx)
+        workers = min(32, os.cpu_count() or 1) if total >= 64_000_000 else 1
+    if workers > 1 and len(tasks) > 1:
+        import multiprocessing as mp
+        from concurrent.futures import ProcessPoolExecutor
+        with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+            return list(ex.map(_uneven_text, tasks, chunksize=4))
+    return [_uneven_text(t) for t in tasks]
+
+
 def strain_collection(copies: int = 50, genome_bp: int = 2_000_000,
                       rng: Optional[np.random.Generator] = None) -> Reference:
     """50 copies of one random genome at 0.1% SNP + 0.01% indel divergence."""

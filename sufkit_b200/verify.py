@@ -104,3 +104,126 @@ def plcp_from(sa: np.ndarray, lcp: np.ndarray) -> np.ndarray:
     out = np.empty(sa.size, np.uint64)
     out[np.asarray(sa, np.int64)] = np.asarray(lcp, np.uint64)
     return out
+
+
+# ---------------------------------------------------------------------------
+# The same checks on device tensors (torch), for builds whose host copies
+# would not fit: a 3.1 Gsym text needs ~80 GB of device memory here.
+# ---------------------------------------------------------------------------
+def _u32(t, torch):
+    """int32 tensor holding uint32 bits -> int64 values."""
+    return t.to(torch.int64) & 0xFFFFFFFF
+
+
+def _device_powers(p: int, count: int, torch, dev):
+    """B^k mod p for k < count as small[k & 0xffff] * big[k >> 16] mod p."""
+    small = [1] * 65536
+    for i in range(1, 65536):
+        small[i] = small[i - 1] * _BASE % p
+    step = small[65535] * _BASE % p
+    big_n = count // 65536 + 2
+    big = [1] * big_n
+    for i in range(1, big_n):
+        big[i] = big[i - 1] * step % p
+    return (torch.tensor(small, dtype=torch.int64, device=dev),
+            torch.tensor(big, dtype=torch.int64, device=dev))
+
+
+def _pow_of(k, tables, p):
+    small, big = tables
+    return small[k & 0xFFFF] * big[k >> 16] % p
+
+
+def check_suffix_array_device(d_text, d_sa, d_lcp, torch, chunk: int = 1 << 26) -> None:
+    """check_suffix_array for device tensors: d_text uint8 (n), d_sa and d_lcp
+    int32 holding uint32 values (n rows).  (1) and (3) exactly, (2) by the
+    polynomial hash H[i] = sum_{j<i} (t[j]+1) B^j mod p (two 31-bit primes),
+    comparing (H[a+l]-H[a]) B^b with (H[b+l]-H[b]) B^a."""
+    dev = d_text.device
+    n = int(d_text.numel())
+    assert int(d_sa.numel()) == n and int(d_lcp.numel()) == n
+    if n == 0:
+        return
+    # (1) permutation: every entry in [0, n) and every position hit.
+    seen = torch.zeros(n, dtype=torch.uint8, device=dev)
+    for s in range(0, n, chunk):
+        v = _u32(d_sa[s:s + chunk], torch)
+        assert int(v.max().item()) < n, "SA entry out of range"
+        seen[v] = 1
+    assert bool((seen == 1).all().item()), "SA is not a permutation"
+    del seen
+    assert int(_u32(d_lcp[:1], torch).item()) == 0, "LCP[0] must be 0"
+    # (3) order at the first mismatch, and the LCP range.
+    for s in range(1, n, chunk):
+        e = min(n, s + chunk)
+        a = _u32(d_sa[s - 1:e - 1], torch)
+        b = _u32(d_sa[s:e], torch)
+        l = _u32(d_lcp[s:e], torch)
+        assert bool(((a + l <= n) & (b + l <= n)).all().item()), "LCP exceeds suffix length"
+        a_end = a + l == n
+        inside = ~a_end & (b + l < n)
+        ta = d_text[torch.where(inside, a + l, torch.zeros_like(a))].to(torch.int16)
+        tb = d_text[torch.where(inside, b + l, torch.zeros_like(b))].to(torch.int16)
+        ok = a_end | (inside & (ta < tb))
+        if not bool(ok.all().item()):
+            bad = torch.nonzero(~ok).flatten()[:5] + s
+            raise AssertionError(f"order/LCP mismatch at rows {bad.tolist()}")
+    # (2) equal prefixes of length l, one prime at a time.
+    for p in _PRIMES:
+        tables = _device_powers(p, n + 1, torch, dev)
+        h = torch.zeros(n + 1, dtype=torch.int64, device=dev)
+        carry = 0
+        for s in range(0, n, chunk):
+            e = min(n, s + chunk)
+            k = torch.arange(s, e, dtype=torch.int64, device=dev)
+            terms = (d_text[s:e].to(torch.int64) + 1) * _pow_of(k, tables, p) % p
+            c = torch.cumsum(terms, 0)  # < 2^26 * 2^31: no overflow
+            h[s + 1:e + 1] = (c + carry) % p
+            carry = int(h[e].item())
+            del k, terms, c
+        for s in range(1, n, chunk):
+            e = min(n, s + chunk)
+            a = _u32(d_sa[s - 1:e - 1], torch)
+            b = _u32(d_sa[s:e], torch)
+            l = _u32(d_lcp[s:e], torch)
+            ha = (h[a + l] - h[a]) % p
+            hb = (h[b + l] - h[b]) % p
+            lhs = ha * _pow_of(b, tables, p) % p
+            rhs = hb * _pow_of(a, tables, p) % p
+            if not bool((lhs == rhs).all().item()):
+                bad = torch.nonzero(lhs != rhs).flatten()[:5] + s
+                raise AssertionError(f"prefix mismatch at rows {bad.tolist()}")
+        del h
+
+
+def bytecode_device(d_sa, d_lcp, torch, chunk: int = 1 << 26):
+    """Byte-coded LCP of a single text from its exact SA and row LCP on the
+    device: primary[r] = min(LCP[r], 255) and the text-ordered anchors, the
+    positions p with PLCP[p] >= 255 that do not continue the run of p-1
+    (PLCP[p-1] >= 255 and PLCP[p-1] - 1 == PLCP[p]); the restated rule of
+    LcpStorage::BuildByteDataDirect (src/lcp_storage.cpp:394-412).  Returns
+    (primary uint8, anchor positions int64, anchor values int64) tensors."""
+    dev = d_sa.device
+    n = int(d_sa.numel())
+    primary = torch.empty(n, dtype=torch.uint8, device=dev)
+    plcp = torch.empty(n, dtype=torch.int32, device=dev)
+    for s in range(0, n, chunk):
+        l = _u32(d_lcp[s:s + chunk], torch)
+        primary[s:s + chunk] = torch.clamp(l, max=255).to(torch.uint8)
+        plcp[_u32(d_sa[s:s + chunk], torch)] = d_lcp[s:s + chunk]
+    pos, val = [], []
+    for s in range(0, n, chunk):
+        e = min(n, s + chunk)
+        cur = _u32(plcp[s:e], torch)
+        prev = torch.empty_like(cur)
+        prev[1:] = cur[:-1]
+        prev[0] = _u32(plcp[s - 1:s], torch)[0] if s > 0 else 0
+        over = cur >= 255
+        cont = over & (prev >= 255) & (prev - 1 == cur)
+        if s == 0:
+            cont[0] = False
+        opens = torch.nonzero(over & ~cont).flatten()
+        pos.append(opens + s)
+        val.append(cur[opens])
+    del plcp
+    return primary, torch.cat(pos), torch.cat(val)

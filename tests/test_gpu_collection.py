@@ -1,9 +1,11 @@
 """GPU: collections built in sub-batches on several contexts side by side
-(sufgpu_build_collection).  Every instance equals a single build of it."""
+(sufgpu_build_collection).  Every instance equals a single build of it and
+the oracle's build of it."""
 import numpy as np
 import pytest
 
 import sufkit_b200 as sg
+from conftest import assert_oracle, oracle_build
 from sufkit_b200 import synth
 
 pytestmark = pytest.mark.gpu
@@ -29,6 +31,7 @@ def test_collection_equals_single_builds(ctx, workers, batch_symbols):
                                validate=True, batch_symbols=batch_symbols, workers=workers)
     assert ctx.last_stats["symbols"] == sum(t.size for t in ts)
     for t, r in zip(ts, got):
+        assert_oracle(r, t, sg.LcpEncoding.RAW32)
         one = ctx.build(t, sa_bits=32, isa_bits=32, lcp=sg.LcpEncoding.RAW32)
         assert (r.sa_low == one.sa_low).all()
         assert (r.isa_low == one.isa_low).all()
@@ -44,6 +47,7 @@ def test_collection_sa_and_lcp_only(ctx, lcp, workers):
     got = ctx.build_collection(ts, sa_bits=32, isa_bits=0, lcp=lcp, validate=True,
                                batch_symbols=120_000, workers=workers)
     for t, r in zip(ts, got):
+        assert_oracle(r, t, lcp)
         one = ctx.build(t, sa_bits=32, isa_bits=0, lcp=lcp)
         assert (r.sa_low == one.sa_low).all()
         if lcp != sg.LcpEncoding.NONE:
@@ -72,6 +76,7 @@ def test_collection_byte_coded_anchors_survive(ctx):
     got = ctx.build_collection(ts, sa_bits=40, lcp=sg.LcpEncoding.BYTE32, batch_symbols=100_000,
                                workers=2)
     for t, r in zip(ts, got):
+        assert_oracle(r, t, sg.LcpEncoding.BYTE32)
         one = ctx.build(t, sa_bits=40, isa_bits=0, lcp=sg.LcpEncoding.BYTE32)
         assert (r.sa == one.sa).all() and (r.lcp == one.lcp).all()
         assert (r.anchor_positions == one.anchor_positions).all()

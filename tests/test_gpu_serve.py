@@ -1,13 +1,15 @@
 """GPU: continuously batched (served) builds equal standalone builds.
 
 Requests of mixed size and encoding are submitted while earlier ones are on
-the GPU; each result must equal Context.build of the same text (and hence the
-reference's divsufsort64 build)."""
+the GPU; each result must equal Context.build of the same text and the
+oracle's build (the reference's divsufsort64 when it was compiled), and the
+server's per-request iteration counts must show that requests were merged
+into a batch whose earlier members were still mid-rounds."""
 import numpy as np
 import pytest
 
-import oracle
 import sufkit_b200 as sg
+from conftest import assert_oracle, oracle_build
 from sufkit_b200 import synth
 
 pytestmark = pytest.mark.gpu
@@ -55,12 +57,47 @@ def test_served_results_equal_standalone(ctx):
     assert stats["p99_seconds"] >= stats["p50_seconds"] > 0
     for i, t in enumerate(texts):
         sa_bits, isa_bits, lcp = ENCODINGS[i % len(ENCODINGS)]
+        assert_oracle(results[i], t, lcp)
         alone = ctx.build(t, sa_bits, isa_bits, lcp)
         _same(results[i], alone)
-    # And against the reference for one mixed-in request.
-    t = texts[7]
-    sa, isa, lcp_ref = oracle.full_build(t) if oracle.ref() is None else oracle.ref_adapter(t)[:3]
-    assert (results[7].sa == sa).all()
+
+
+def test_served_requests_overlap_in_the_running_batch(ctx):
+    """Continuous batching, not a queue: a request admitted while others are
+    mid-rounds shares their doubling rounds.  The long-LCP strain collection
+    (about 14 rounds) is submitted first; small requests follow while it runs.
+    Some request must be admitted at an iteration > 0 with requests in flight,
+    and finish before a request admitted earlier does; every result is the
+    same in the mix as alone and as the oracle's."""
+    rng = np.random.default_rng(17)
+    long_lcp = synth.strain_collection(copies=12, genome_bp=200_000, rng=rng).logical_text()
+    small = [synth.random_text(rng, int(n), 4) for n in (3_000, 40_000, 120_000, 7_000, 60_000)]
+    texts = [long_lcp] + small
+    expected = [oracle_build(t) for t in texts]
+    with sg.Server(0, capacity_symbols=1 << 24, max_instances=16) as server:
+        tickets = [server.submit(long_lcp, 32, 0, sg.LcpEncoding.BYTE32)]
+        import time
+        deadline = time.monotonic() + 30
+        while server.stats()["iterations"] < 1 and time.monotonic() < deadline:
+            time.sleep(0.0005)  # the long request is on the GPU, mid-rounds
+        for t in small:
+            tickets.append(server.submit(t, 32, 32, sg.LcpEncoding.RAW32))
+        results = [server.wait(k) for k in tickets]
+        stats = server.stats()
+    assert stats["max_inflight"] > 1
+    infos = [r.stats for r in results]
+    merged = [i for i, st in enumerate(infos) if st["inflight_at_admit"] > 0
+              and st["admit_iteration"] > 0]
+    assert merged, f"no request joined a running batch: {infos}"
+    # Overlap: a request admitted later finished no later than one admitted earlier.
+    assert any(infos[j]["admit_iteration"] > infos[i]["admit_iteration"]
+               and infos[j]["finish_iteration"] <= infos[i]["finish_iteration"]
+               for i in range(len(infos)) for j in range(len(infos)) if i != j)
+    for t, r, e, lcp in zip(texts, results, expected,
+                            [sg.LcpEncoding.BYTE32] + [sg.LcpEncoding.RAW32] * len(small)):
+        assert_oracle(r, t, lcp, e)
+        alone = ctx.build(t, 32, 0 if lcp == sg.LcpEncoding.BYTE32 else 32, lcp)
+        _same(r, alone)
 
 
 def test_served_admission_under_small_arena(ctx):
@@ -72,6 +109,7 @@ def test_served_admission_under_small_arena(ctx):
         stats = server.stats()
     assert stats["completed"] == len(texts) and stats["max_inflight"] <= 8
     for t, r in zip(texts, results):
+        assert_oracle(r, t, sg.LcpEncoding.RAW32)
         alone = ctx.build(t, 32, 32, sg.LcpEncoding.RAW32)
         _same(r, alone)
 
