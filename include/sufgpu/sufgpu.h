@@ -59,6 +59,12 @@ typedef enum sufgpu_lcp_encoding {
  * stats.plane_crc (single builds).  A section's CRC follows from its header
  * bytes and these with zlib's crc32_combine. */
 #define SUFGPU_FLAG_PLANE_CRC 2u
+/* Also build the compact CHILD table (up / down / next-L links, one row
+ * index per row, n = no link) of the row LCP into outputs.child as uint32
+ * rows; the table BuildChildFor (src/suffix_array.cpp:1438-1496) builds for
+ * the kLcpChild and kFull accelerations.  Single complete builds with an LCP
+ * encoding other than none. */
+#define SUFGPU_FLAG_CHILD 4u
 
 /* What to build.  Stored widths follow CoordinateStorageWidth
  * (include/sufkit/types.hpp:100-111): 32 native, 40 split low32+high8,
@@ -95,6 +101,7 @@ typedef struct sufgpu_outputs {
   void *isa_high;
   void *lcp;
   void *prefix_intervals; /* 4^prefix_k uint64 entries (desc.prefix_k > 0) */
+  void *child;            /* n uint32 rows (SUFGPU_FLAG_CHILD) */
 } sufgpu_outputs;
 
 /* Byte-coded overflow anchors (text-ordered positions with their LCP values,

@@ -64,6 +64,8 @@ def port() -> ctypes.CDLL:
         lib.oracle_bytecode_exact.restype = U64
         lib.oracle_pack.argtypes = [P, U64, U64, ctypes.c_int, P, P, P]
         lib.oracle_is_permutation.argtypes = [P, U64]
+        lib.oracle_child.argtypes = [P, U64, P]
+        lib.oracle_child.restype = None
         _port = lib
     return _port
 
@@ -173,6 +175,14 @@ def pack(values: np.ndarray, symbol_count: int, bits: int):
     if width == 48:
         return width, low, high16
     return width, low, None
+
+
+def child(lcp: np.ndarray) -> np.ndarray:
+    """Compact CHILD table of a row-order LCP array (uint64; n = no link)."""
+    l = np.ascontiguousarray(lcp, np.uint64)
+    out = np.empty(l.size, np.uint64)
+    port().oracle_child(_p(l), l.size, _p(out))
+    return out
 
 
 def full_build(text: np.ndarray):
@@ -440,3 +450,45 @@ def uneven_reference_digests(task) -> tuple[int, int, str, str]:
     sa, _, lcp, _ = ref_adapter(text, 64)
     d_sa, d_lcp = digest_planes(sa, lcp)
     return index, int(text.size), d_sa, d_lcp
+
+
+# --------------------------------------------------------------------------
+# Reading coordinate sections of a saved .sufidx (container layout of
+# src/serialization.cpp:305-360: an 80-byte header, then 32-byte section
+# entries {type u32, flags u32, offset u64, size u64, crc u32, 0 u32};
+# coordinate sections of src/sa_codec.cpp:466-512: a 56-byte codec header
+# {magic, version, codec, 0 (u32 each); symbols, count, low bytes, high bytes,
+# 0 (u64 each)}, then the low plane and the high plane)
+# --------------------------------------------------------------------------
+SECTION_SUFFIX_ARRAY, SECTION_ISA, SECTION_LCP, SECTION_CHILD = 3, 5, 6, 7
+
+
+def sufidx_sections(path) -> dict:
+    import struct
+    data = Path(path).read_bytes()
+    count = struct.unpack_from("<I", data, 24)[0]
+    out = {}
+    for k in range(count):
+        typ, _flags, off, size, _crc, _pad = struct.unpack_from("<IIQQII", data, 80 + 32 * k)
+        out[typ] = (off, size)
+    return out
+
+
+def sufidx_coordinates(path, section: int) -> np.ndarray:
+    """The values of one coordinate section (SA, ISA or CHILD) as uint64."""
+    import struct
+    off, size = sufidx_sections(path)[section]
+    with open(path, "rb") as f:
+        f.seek(off)
+        blob = f.read(size)
+    _magic, _version, _codec, _zero, _symbols, count, low_bytes, high_bytes, _res = \
+        struct.unpack_from("<IIIIQQQQQ", blob, 0)
+    body = blob[56:]
+    if low_bytes == count * 8:
+        return np.frombuffer(body, np.uint64, count).copy()
+    low = np.frombuffer(body, np.uint32, count).astype(np.uint64)
+    if high_bytes == count:
+        low |= np.frombuffer(body, np.uint8, count, low_bytes).astype(np.uint64) << np.uint64(32)
+    elif high_bytes == 2 * count:
+        low |= np.frombuffer(body, np.uint16, count, low_bytes).astype(np.uint64) << np.uint64(32)
+    return low

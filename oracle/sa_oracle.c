@@ -214,3 +214,45 @@ int oracle_pack(const uint64_t *values, uint64_t count, uint64_t symbol_count,
   }
   return width;
 }
+
+/* Compact CHILD table (up / down / next-L links in one entry per row) of a
+ * row-order LCP array: BuildChildFor, src/suffix_array.cpp:1438-1496.  The
+ * first monotone-stack pass writes down links at the stack entry below each
+ * popped interval and up links at index - 1; the second pass writes next-L
+ * links between equal LCP values, overriding.  `none` (n) marks no link. */
+void oracle_child(const uint64_t *lcp, uint64_t n, uint64_t *child) {
+  if (n == 0) return;
+  const uint64_t none = n;
+  uint64_t *stack = (uint64_t *)malloc(n * sizeof(uint64_t));
+  if (!stack) return;
+  for (uint64_t i = 0; i < n; ++i) child[i] = none;
+  uint64_t top = 0; /* number of entries */
+  stack[top++] = 0;
+  for (uint64_t i = 1; i < n; ++i) {
+    const uint64_t cur = lcp[i];
+    uint64_t last = none;
+    while (top > 0 && cur < lcp[stack[top - 1]]) {
+      last = stack[--top];
+      if (top > 0 && cur <= lcp[stack[top - 1]] && lcp[stack[top - 1]] != lcp[last]) {
+        child[stack[top - 1]] = last;
+      }
+    }
+    if (last != none) child[i - 1] = last;
+    stack[top++] = i;
+  }
+  while (top > 0 && lcp[stack[top - 1]] > 0) {
+    const uint64_t last = stack[--top];
+    if (top > 0 && lcp[stack[top - 1]] != lcp[last]) child[stack[top - 1]] = last;
+  }
+  top = 0;
+  stack[top++] = 0;
+  for (uint64_t i = 1; i < n; ++i) {
+    while (top > 0 && lcp[i] < lcp[stack[top - 1]]) --top;
+    if (top > 0 && lcp[i] == lcp[stack[top - 1]]) {
+      const uint64_t last = stack[--top];
+      child[last] = i;
+    }
+    stack[top++] = i;
+  }
+  free(stack);
+}

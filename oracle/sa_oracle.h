@@ -64,6 +64,10 @@ int oracle_pack(const uint64_t *values, uint64_t count, uint64_t symbol_count,
 /* Permutation check used before packing: every value < n and seen once. */
 int oracle_is_permutation(const uint64_t *sa, uint64_t n);
 
+/* Compact CHILD table of a row-order LCP (src/suffix_array.cpp:1438-1496);
+ * child[i] = n marks no link. */
+void oracle_child(const uint64_t *lcp, uint64_t n, uint64_t *child);
+
 #ifdef __cplusplus
 }
 #endif

@@ -58,6 +58,7 @@ class LcpEncoding(enum.IntEnum):
 
 FLAG_VALIDATE = 1
 FLAG_PLANE_CRC = 2
+FLAG_CHILD = 4
 
 
 class _Desc(ctypes.Structure):
@@ -72,7 +73,8 @@ class _Desc(ctypes.Structure):
 class _Outputs(ctypes.Structure):
     _fields_ = [("sa_low", ctypes.c_void_p), ("sa_high", ctypes.c_void_p),
                 ("isa_low", ctypes.c_void_p), ("isa_high", ctypes.c_void_p),
-                ("lcp", ctypes.c_void_p), ("prefix_intervals", ctypes.c_void_p)]
+                ("lcp", ctypes.c_void_p), ("prefix_intervals", ctypes.c_void_p),
+                ("child", ctypes.c_void_p)]
 
 
 class _Anchors(ctypes.Structure):
@@ -263,6 +265,7 @@ class BuildResult:
     anchor_positions: Optional[np.ndarray] = None
     anchor_values: Optional[np.ndarray] = None
     prefix_intervals: Optional[np.ndarray] = None
+    child: Optional[np.ndarray] = None
     stats: dict = field(default_factory=dict)
 
     @property
@@ -352,7 +355,7 @@ class Context:
     def _outputs(planes: dict) -> _Outputs:
         return _Outputs(*(_ptr(planes.get(k)) for k in
                           ("sa_low", "sa_high", "isa_low", "isa_high", "lcp",
-                           "prefix_intervals")))
+                           "prefix_intervals", "child")))
 
     @staticmethod
     def _anchors(a: _Anchors, lcp: LcpEncoding):
@@ -369,19 +372,23 @@ class Context:
     def build(self, text, sa_bits: int = 32, isa_bits: int = 32,
               lcp: LcpEncoding = LcpEncoding.RAW32, validate: bool = False,
               sampling_rate: int = 1, prefix_k: int = 0,
-              plane_crc: bool = False) -> BuildResult:
+              plane_crc: bool = False, child: bool = False) -> BuildResult:
         """One complete build of ``text`` (the logical text including its
         sentinel).  Returns host planes; see include/sufgpu/sufgpu.h.  With
         sampling_rate K > 1 the planes hold the ceil(n / K) suffixes at
         positions that are multiples of K.  prefix_k > 0 also returns the Fast
-        index's k-mer directory (4^k entries begin | end << 32)."""
+        index's k-mer directory (4^k entries begin | end << 32).  child also
+        returns the compact CHILD table (uint32 rows, n = no link)."""
         t = _as_text(text)
         n = int(t.size)
         lcp = LcpEncoding(lcp)
         planes = self._alloc_outputs(_rows(n, sampling_rate), sa_bits, isa_bits, lcp)
         if prefix_k:
             planes["prefix_intervals"] = np.empty(1 << (2 * prefix_k), np.uint64)
-        flags = (FLAG_VALIDATE if validate else 0) | (FLAG_PLANE_CRC if plane_crc else 0)
+        if child:
+            planes["child"] = np.empty(n, np.uint32)
+        flags = ((FLAG_VALIDATE if validate else 0) | (FLAG_PLANE_CRC if plane_crc else 0)
+                 | (FLAG_CHILD if child else 0))
         desc = _Desc(sa_bits, isa_bits, int(lcp), flags, int(sampling_rate), int(prefix_k))
         out = self._outputs(planes)
         anchors = _Anchors()
@@ -530,7 +537,7 @@ class Context:
         (raw pointers, e.g. from torch tensors).  Returns the stats."""
         desc = _Desc(sa_bits, isa_bits, int(LcpEncoding(lcp)), FLAG_VALIDATE if validate else 0)
         out = _Outputs(*(out_ptrs.get(k) for k in ("sa_low", "sa_high", "isa_low", "isa_high", "lcp",
-                                                   "prefix_intervals")))
+                                                   "prefix_intervals", "child")))
         anchors = _Anchors()
         stats = _Stats()
         status = self._lib.sufgpu_build(self._h, text_ptr, n, ctypes.byref(desc), ctypes.byref(out),

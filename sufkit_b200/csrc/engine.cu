@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "../../include/sufgpu/sufgpu.h"
+#include "child.cuh"
 #include "common.cuh"
 #include "doubling.cuh"
 #include "lcp.cuh"
@@ -1448,6 +1449,43 @@ void emit_sampled(Engine& e, const sufgpu_build_desc& d, sufgpu_outputs* outs, u
   e.sync();
 }
 
+// CHILD table of the row LCP (child.cuh) into dst (host or device): the
+// minima tree and the nse/up/down arrays in k0/k1 (free once the LCP planes
+// are out), the table staged in x.
+void emit_child(Engine& e, const u32* lcp, void* dst) {
+  Layout& L = e.L;
+  const u64 n = e.n;
+  u32* nse = reinterpret_cast<u32*>(L.k0);
+  u32* down = nse + n;
+  u32* up = reinterpret_cast<u32*>(L.k1);
+  u32* tree = up + n;
+  MinTree t{};
+  t.level[0] = lcp;
+  t.size[0] = n;
+  t.levels = 1;
+  u32* at = tree;
+  while (t.size[t.levels - 1] > kChildFan) {
+    if (t.levels >= kChildMaxLevels) throw BuildError{SUFGPU_BUILD_FAILURE, "CHILD tree too deep"};
+    const u64 below = t.size[t.levels - 1];
+    const u64 size = (below + kChildFan - 1) / kChildFan;
+    e.launch("child_tree", below * 4 + size * 4, child_min_level_kernel,
+             e.grid_stride_blocks(size, 256), 256, 0, t.level[t.levels - 1], below, at, size);
+    t.level[t.levels] = at;
+    t.size[t.levels] = size;
+    ++t.levels;
+    at += size;
+  }
+  e.zero(down, n * 4);
+  SG_CUDA(cudaMemsetAsync(up, 0xff, n * 4, e.c.stream));  // > every row: atomicMin start
+  e.launch("child_links", n * 12, child_links_kernel, e.grid_stride_blocks(n, 256), 256, 0, t,
+           nse, down, up);
+  u32* child = L.x;
+  e.launch("child_final", n * 20, child_final_kernel, e.grid_stride_blocks(n, 256), 256, 0, lcp,
+           n, static_cast<const u32*>(nse), static_cast<const u32*>(down),
+           static_cast<const u32*>(up), child);
+  copy_out(e.c, dst, child, n * 4);
+}
+
 void emit_outputs(Engine& e, const sufgpu_build_desc& d, sufgpu_outputs* outs,
                   sufgpu_anchors* anchors, u32 count) {
   sufgpu_ctx& c = e.c;
@@ -1608,6 +1646,7 @@ void emit_outputs(Engine& e, const sufgpu_build_desc& d, sufgpu_outputs* outs,
         }
       }
     }
+    if (d.flags & SUFGPU_FLAG_CHILD) emit_child(e, ph.lcp, outs[0].child);
   }
   SG_CUDA(cudaEventRecord(c.ev[5], c.stream));
   e.sync();
@@ -1799,6 +1838,10 @@ static sufgpu_status check_desc(sufgpu_ctx* ctx, const sufgpu_build_desc* d) {
   if (d->prefix_k && d->sampling_rate > 1) {
     return fail(ctx, SUFGPU_INVALID_INPUT, "the prefix directory needs a complete suffix array");
   }
+  if ((d->flags & SUFGPU_FLAG_CHILD) &&
+      (d->sampling_rate > 1 || d->lcp_encoding == SUFGPU_LCP_NONE)) {
+    return fail(ctx, SUFGPU_INVALID_INPUT, "CHILD needs a complete build with LCP");
+  }
   return SUFGPU_OK;
 }
 
@@ -1862,6 +1905,9 @@ sufgpu_status sufgpu_build(sufgpu_ctx* ctx, const uint8_t* text, uint64_t n,
   if (n > sufgpu_max_symbols()) return fail(ctx, SUFGPU_INVALID_INPUT, "text exceeds 2^32-1 symbols");
   if (n > 0 && !text) return fail(ctx, SUFGPU_INVALID_INPUT, "text is null");
   if (!out) return fail(ctx, SUFGPU_INVALID_INPUT, "outputs are null");
+  if ((desc->flags & SUFGPU_FLAG_CHILD) && n > 0 && !out->child) {
+    return fail(ctx, SUFGPU_INVALID_INPUT, "child is null");
+  }
   if (desc->prefix_k) {
     if (!out->prefix_intervals) return fail(ctx, SUFGPU_INVALID_INPUT, "prefix_intervals is null");
     // The directory is staged in the 8n-byte key buffer.
@@ -1966,6 +2012,9 @@ static sufgpu_status build_batch(sufgpu_ctx* ctx, sufgpu_instance* instances, ui
   }
   if (desc->flags & SUFGPU_FLAG_PLANE_CRC) {
     return fail(ctx, SUFGPU_INVALID_INPUT, "plane checksums are kept for single builds");
+  }
+  if (desc->flags & SUFGPU_FLAG_CHILD) {
+    return fail(ctx, SUFGPU_INVALID_INPUT, "the CHILD table is built for single references");
   }
   std::vector<u64> begin(count + 1, 0);
   for (u32 j = 0; j < count; ++j) {
@@ -2694,7 +2743,9 @@ sufgpu_status sufgpu_server_submit(sufgpu_server* S, const uint8_t* text, uint64
   if (!S || !desc || !out || !ticket || (n && !text)) return SUFGPU_INVALID_INPUT;
   if (auto s = check_desc(S->ctx, desc)) return s;
   // Served builds return complete arrays without the prefix directory.
-  if (desc->sampling_rate > 1 || desc->prefix_k) return SUFGPU_INVALID_INPUT;
+  if (desc->sampling_rate > 1 || desc->prefix_k || (desc->flags & SUFGPU_FLAG_CHILD)) {
+    return SUFGPU_INVALID_INPUT;
+  }
   if (n == 0 || n > sufgpu_max_symbols()) return SUFGPU_INVALID_INPUT;
   auto r = std::make_shared<ServedRequest>();
   r->text = text;

@@ -132,3 +132,31 @@ def test_prefix_directory_restatement_matches_reference():
         mine = oracle.prefix_directory(t, sa, k)
         assert (mine == table).all()
         assert int((mine != (t.size | (t.size << 32))).sum()) == entries
+
+
+def test_child_restatement_matches_reference_sufidx(tmp_path):
+    """The C restatement of BuildChildFor equals the CHILD section the
+    reference's SuffixArray::Build saves (acceleration kLcpChild)."""
+    from sufkit_b200 import synth
+    if oracle.ref() is None:
+        pytest.skip("the reference library was not built")
+    refs = [synth.repeat_rich_100mbp(scale=0.001), synth.human_scale_3gbp(scale=0.0002),
+            synth.plain_4mbp(scale=0.005),
+            synth.strain_collection(4, 5_000, np.random.default_rng(2))]
+    for i, ref in enumerate(refs):
+        fasta = tmp_path / f"{i}.fa"
+        ref.write_fasta(fasta)
+        out = oracle.sufkit_index(fasta, tmp_path / f"{i}.sufidx", 0, 32, 32, acceleration=2)
+        assert out["rc"] == 0, out.get("error")
+        child = oracle.sufidx_coordinates(tmp_path / f"{i}.sufidx", oracle.SECTION_CHILD)
+        sa_file = oracle.sufidx_coordinates(tmp_path / f"{i}.sufidx", oracle.SECTION_SUFFIX_ARRAY)
+        sa, isa, lcp = oracle.full_build(ref.logical_text())
+        assert np.array_equal(sa_file, sa)
+        assert np.array_equal(oracle.child(lcp), child)
+
+
+def test_child_restatement_edge_cases():
+    # Decreasing, increasing, constant and single-row LCP arrays.
+    for lcp in ([0], [0, 5, 4, 3, 2, 1], [0, 1, 2, 3, 4], [0, 2, 2, 2, 2], [3, 1, 3, 1, 3]):
+        out = oracle.child(np.array(lcp, np.uint64))
+        assert out.size == len(lcp) and (out <= len(lcp)).all()
