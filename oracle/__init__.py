@@ -88,6 +88,8 @@ def ref() -> Optional[ctypes.CDLL]:
         lib.sufref_pack.argtypes = [P, U64, U64, ctypes.c_int, P, P, P, P]
         lib.sufref_bytecoded_direct.argtypes = [P, U64, P, P, ctypes.c_int, P, P, P, U64, P]
         lib.sufref_bytecoded_from_raw.argtypes = [P, P, U64, ctypes.c_int, P, P, P, U64, P]
+        lib.sufref_bytecoded_direct_sampled.argtypes = [P, U64, P, P, U64, ctypes.c_uint32,
+                                                        ctypes.c_int, P, P, P, U64, P]
         lib.sufref_bytecoded_exact.argtypes = [P, U64, P, P, U64, P, P, U64, P]
         lib.sufref_encode_fasta.argtypes = [ctypes.c_char_p, P, U64, P, P]
         lib.sufref_encode_fasta.restype = ctypes.c_int64
@@ -316,6 +318,44 @@ def ref_bytecode(text: np.ndarray, sa: np.ndarray, isa: np.ndarray, width: int =
                                             _p(pos), _p(val), cap, ctypes.addressof(count)))
     k = count.value
     return primary, pos[:k].copy(), val[:k].copy()
+
+
+def ref_bytecode_sampled(text: np.ndarray, sa_k: np.ndarray, isa_k: np.ndarray, rate: int,
+                         width: int = 32):
+    """LcpStorage::BuildByteCodedDirect of a sampled build (rate K): primary
+    bytes per sampled row, anchor positions and values (uint64)."""
+    lib = ref()
+    t = np.ascontiguousarray(text, np.uint8)
+    sa = np.ascontiguousarray(sa_k, np.uint64)
+    isa = np.ascontiguousarray(isa_k, np.uint64)
+    rows = sa.size
+    primary = np.empty(max(rows, 1), np.uint8)
+    cap = rows + 1
+    pos = np.empty(cap, np.uint64)
+    val = np.empty(cap, np.uint64)
+    count = ctypes.c_uint64()
+    _check(lib, lib.sufref_bytecoded_direct_sampled(_p(t), t.size, _p(sa), _p(isa), rows, rate,
+                                                    width, _p(primary), _p(pos), _p(val), cap,
+                                                    ctypes.byref(count)))
+    k = count.value
+    return primary[:rows].copy(), pos[:k].copy(), val[:k].copy()
+
+
+def sample_bytecode(sa_k: np.ndarray, isa_k: np.ndarray, lcp_k: np.ndarray, rate: int):
+    """Restatement of the sampled byte coding (src/lcp_storage.cpp:304-420,
+    K > 1) from a sampled build's SA, dense ISA and row LCP: primary =
+    min(LCP, 255) per sampled row; an anchor opens at sample position s*K
+    when PLCP_K[s] >= 255 unless sample s-1 overflowed too with PLCP_K[s-1]
+    >= K and PLCP_K[s-1] - K == PLCP_K[s]."""
+    lcp = np.asarray(lcp_k, np.int64)
+    primary = np.minimum(lcp, 255).astype(np.uint8)
+    plcp = lcp[np.asarray(isa_k, np.int64)]
+    over = plcp >= 255
+    prev = np.concatenate([[-1], plcp[:-1]])
+    prev_over = np.concatenate([[False], over[:-1]])
+    cont = prev_over & (prev >= rate) & (prev - rate == plcp)
+    opens = np.flatnonzero(over & ~cont)
+    return primary, (opens * rate).astype(np.uint64), plcp[opens].astype(np.uint64)
 
 
 def ref_bytecode_from_raw(lcp: np.ndarray, isa: np.ndarray, width: int = 32):

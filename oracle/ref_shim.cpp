@@ -311,6 +311,25 @@ int sufref_bytecoded_direct(const uint8_t* text, uint64_t n,
   }
 }
 
+// The same for a sampled suffix array (rate K > 1): rows = ceil(n / K)
+// sampled SA rows and the dense sampled ISA (src/lcp_storage.cpp:304-420).
+int sufref_bytecoded_direct_sampled(const uint8_t* text, uint64_t n, const uint64_t* sa,
+                                    const uint64_t* isa, uint64_t rows, uint32_t rate,
+                                    int coordinate_width, uint8_t* primary,
+                                    uint64_t* anchor_pos, uint64_t* anchor_val,
+                                    uint64_t anchor_cap, uint64_t* anchor_count) {
+  try {
+    auto storage = LcpStorage::BuildByteCodedDirect(
+        text, n, IntegerArrayView(sa, rows), IntegerArrayView(isa, rows), rate,
+        static_cast<std::uint8_t>(coordinate_width), ErrorCode::kBuildFailure);
+    ExportByteCoded(storage, primary, anchor_pos, anchor_val, anchor_cap,
+                    anchor_count);
+    return 0;
+  } catch (const std::exception& error) {
+    return Fail(error);
+  }
+}
+
 // LcpStorage::BuildByteCoded from a raw row-order LCP and the ISA.
 int sufref_bytecoded_from_raw(const uint64_t* lcp, const uint64_t* isa,
                               uint64_t n, int coordinate_width,

@@ -1374,7 +1374,8 @@ u64 high_bytes(u32 bits, u64 rows) { return bits == 40 ? rows : bits == 48 ? 2 *
 // Sampled outputs (rate K > 1): complete SA, ISA and row LCP first, then the
 // kept rows (sample_kernel) packed into each instance's planes of
 // ceil(n_i / K) rows.
-void emit_sampled(Engine& e, const sufgpu_build_desc& d, sufgpu_outputs* outs, u32 count) {
+void emit_sampled(Engine& e, const sufgpu_build_desc& d, sufgpu_outputs* outs,
+                  sufgpu_anchors* anchors, u32 count) {
   sufgpu_ctx& c = e.c;
   Layout& L = e.L;
   const u64 n = e.n;
@@ -1432,7 +1433,9 @@ void emit_sampled(Engine& e, const sufgpu_build_desc& d, sufgpu_outputs* outs, u
   if (d.isa_storage_bits) emit(isa_k, d.isa_storage_bits, true);
   emit(sa_k, d.sa_storage_bits, false);
   SG_CUDA(cudaEventRecord(c.ev[4], c.stream));
-  if (want_lcp) {
+  const bool byte_coded =
+      d.lcp_encoding == SUFGPU_LCP_BYTE32 || d.lcp_encoding == SUFGPU_LCP_BYTE64;
+  if (want_lcp && !byte_coded) {
     const bool wide = d.lcp_encoding == SUFGPU_LCP_RAW64;
     const u8* src = reinterpret_cast<const u8*>(lcp_k);
     if (wide) {
@@ -1444,6 +1447,59 @@ void emit_sampled(Engine& e, const sufgpu_build_desc& d, sufgpu_outputs* outs, u
     for (u32 j = 0; j < count; ++j) {
       copy_plane(e, outs[j].lcp, src + off[j] * w, (off[j + 1] - off[j]) * w, kCrcLcp);
     }
+  } else if (byte_coded) {
+    // Primary bytes of the sampled rows, then the anchors in sample order
+    // (sampled_anchor_kernel) with per-instance counts after the offsets.
+    u8* primary = low;  // the packed SA planes above are copied by now (same stream)
+    e.launch("lcp_primary", kept * 5, lcp_primary_kernel, e.grid_stride_blocks(kept, 256), 256,
+             0, static_cast<const u32*>(lcp_k), kept, primary);
+    for (u32 j = 0; j < count; ++j) {
+      copy_plane(e, outs[j].lcp, primary + off[j], off[j + 1] - off[j], kCrcLcp);
+    }
+    const bool wide = d.lcp_encoding == SUFGPU_LCP_BYTE64;
+    const u64 w = wide ? 8 : 4;
+    const u64 cap = (std::max<u64>(n, 1) * 4) / w;  // each of x and y holds 4n bytes
+    u8* pos = reinterpret_cast<u8*>(L.x);
+    u8* val = reinterpret_cast<u8*>(L.y);
+    u64* inst_count = L.digit_start + count + 1;
+    e.zero(inst_count, u64(count) * 8);
+    const u64 atiles = (kept + kScanTile - 1) / kScanTile;
+    e.zero(L.scalars + 4, 8);
+    e.zero(L.status, (atiles + 1) * 8);
+    e.zero(L.counters, 4);
+    if (wide) {
+      e.launch("anchors", kept * 12, sampled_anchor_kernel<u64>, atiles, kScanBlock, 0,
+               static_cast<const u32*>(isa_k), static_cast<const u32*>(lcp_k),
+               static_cast<const u64*>(L.digit_start), count, kept, rate,
+               reinterpret_cast<u64*>(pos), reinterpret_cast<u64*>(val), cap, inst_count,
+               L.status, L.counters, L.scalars + 4, L.flags);
+    } else {
+      e.launch("anchors", kept * 12, sampled_anchor_kernel<u32>, atiles, kScanBlock, 0,
+               static_cast<const u32*>(isa_k), static_cast<const u32*>(lcp_k),
+               static_cast<const u64*>(L.digit_start), count, kept, rate,
+               reinterpret_cast<u32*>(pos), reinterpret_cast<u32*>(val), cap, inst_count,
+               L.status, L.counters, L.scalars + 4, L.flags);
+    }
+    const u64 total = atiles ? e.read_scalar(4) : 0;
+    e.st.anchors = total;
+    if (total > cap) throw BuildError{SUFGPU_BUILD_FAILURE, "anchor buffer overflow"};
+    std::vector<u64> per(count, 0);
+    SG_CUDA(cudaMemcpyAsync(per.data(), inst_count, u64(count) * 8, cudaMemcpyDeviceToHost,
+                            c.stream));
+    c.anchor_pos.resize(std::max<u64>(total * w, 8));
+    c.anchor_val.resize(std::max<u64>(total * w, 8));
+    SG_CUDA(cudaMemcpyAsync(c.anchor_pos.data(), pos, total * w, cudaMemcpyDeviceToHost, c.stream));
+    SG_CUDA(cudaMemcpyAsync(c.anchor_val.data(), val, total * w, cudaMemcpyDeviceToHost, c.stream));
+    e.sync();
+    u64 at = 0;
+    for (u32 j = 0; j < count; ++j) {
+      if (anchors) {
+        anchors[j] = sufgpu_anchors{c.anchor_pos.data() + at * w, c.anchor_val.data() + at * w,
+                                    per[j], static_cast<u32>(w * 8)};
+      }
+      at += per[j];
+    }
+    if (at != total) throw BuildError{SUFGPU_BUILD_FAILURE, "sampled anchor counts disagree"};
   }
   SG_CUDA(cudaEventRecord(c.ev[5], c.stream));
   e.sync();
@@ -1492,7 +1548,7 @@ void emit_outputs(Engine& e, const sufgpu_build_desc& d, sufgpu_outputs* outs,
   Layout& L = e.L;
   const u64 n = e.n;
   if (d.sampling_rate > 1) {
-    emit_sampled(e, d, outs, count);
+    emit_sampled(e, d, outs, anchors, count);
     return;
   }
 
@@ -1826,10 +1882,6 @@ void sufgpu_host_free(void* p) {
 
 static sufgpu_status check_desc(sufgpu_ctx* ctx, const sufgpu_build_desc* d) {
   if (!d) return fail(ctx, SUFGPU_INVALID_INPUT, "build descriptor is null");
-  if (d->sampling_rate > 1 && d->lcp_encoding != SUFGPU_LCP_NONE &&
-      d->lcp_encoding != SUFGPU_LCP_RAW32 && d->lcp_encoding != SUFGPU_LCP_RAW64) {
-    return fail(ctx, SUFGPU_INVALID_INPUT, "sampled builds keep raw LCP only");
-  }
   if (!valid_width(d->sa_storage_bits)) return fail(ctx, SUFGPU_INVALID_INPUT, "invalid SA storage width");
   if (d->isa_storage_bits && !valid_width(d->isa_storage_bits))
     return fail(ctx, SUFGPU_INVALID_INPUT, "invalid ISA storage width");

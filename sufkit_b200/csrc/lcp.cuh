@@ -270,4 +270,82 @@ anchor_kernel(const u64* __restrict__ sorted_pos, const u32* __restrict__ sorted
   }
 }
 
+// Byte-coded overflow anchors of a sampled build (rate K > 1), in sample
+// order: sample t of instance i (s = t - off[i], text position s*K) has
+// PLCP_K = lcp_k[off[i] + isa_k[t]]; it opens an anchor when PLCP_K >= 255
+// unless sample s-1 of the same instance overflowed with a value v' >= K and
+// v' - K == PLCP_K (src/lcp_storage.cpp:394-412 with sampling rate K).
+// Anchors are instance-local positions; inst_count[i] counts instance i's.
+template <class Coord>
+static __global__ void __launch_bounds__(kScanBlock)
+sampled_anchor_kernel(const u32* __restrict__ isa_k, const u32* __restrict__ lcp_k,
+                      const u64* __restrict__ off, u32 count, u64 kept, u32 rate,
+                      Coord* __restrict__ anchor_pos, Coord* __restrict__ anchor_val,
+                      u64 anchor_cap, u64* __restrict__ inst_count, u64* status_sum,
+                      u32* tile_counter, u64* anchor_count, DeviceFlags* flags) {
+  __shared__ u64 warp_smem[kScanBlock / 32];
+  __shared__ u64 tile_prefix;
+  __shared__ u32 tile_slot;
+  const u32 tile = claim_tile(tile_counter, &tile_slot);
+  const u64 t0 = static_cast<u64>(tile) * kScanTile + threadIdx.x * kScanItems;
+  bool open[kScanItems];
+  u32 value[kScanItems];
+  u32 inst_of[kScanItems];
+  u32 opens = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const u64 t = t0 + k;
+    open[k] = false;
+    value[k] = 0;
+    inst_of[k] = 0;
+    if (t >= kept) continue;
+    const u32 inst = count == 1 ? 0 : find_segment(off, count, t);
+    const u64 base = off[inst];
+    const u64 rows = off[inst + 1] - base;
+    const u32 row = isa_k[t];
+    if (row >= rows) {
+      flag_error(flags, kErrBounds);
+      continue;
+    }
+    const u32 v = lcp_k[base + row];
+    if (v < 255) continue;
+    bool continues = false;
+    if (t > base) {
+      const u32 prow = isa_k[t - 1];
+      if (prow < rows) {
+        const u32 pv = lcp_k[base + prow];
+        continues = pv >= 255 && pv >= rate && pv - rate == v;
+      }
+    }
+    open[k] = !continues;
+    value[k] = v;
+    inst_of[k] = inst;
+    opens += open[k];
+  }
+  u64 agg;
+  const u64 excl = block_exclusive_scan<kScanBlock>(opens, SumOp{}, warp_smem, &agg);
+  if ((threadIdx.x >> 5) == 0) {
+    const u64 p = warp_lookback(status_sum, tile, agg, SumOp{}, flags, 9);
+    if ((threadIdx.x & 31) == 0) tile_prefix = p;
+  }
+  __syncthreads();
+  u64 out = tile_prefix + excl;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    if (!open[k]) continue;
+    const u64 t = t0 + k;
+    if (out < anchor_cap) {
+      anchor_pos[out] = static_cast<Coord>((t - off[inst_of[k]]) * rate);
+      anchor_val[out] = static_cast<Coord>(value[k]);
+      atomicAdd(reinterpret_cast<unsigned long long*>(inst_count + inst_of[k]), 1ull);
+    } else {
+      flag_error(flags, kErrQueueOverflow);
+    }
+    ++out;
+  }
+  if (threadIdx.x == 0 && (tile + 1) * static_cast<u64>(kScanTile) >= kept) {
+    *anchor_count = tile_prefix + agg;
+  }
+}
+
 }  // namespace sufgpu

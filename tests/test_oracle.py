@@ -160,3 +160,23 @@ def test_child_restatement_edge_cases():
     for lcp in ([0], [0, 5, 4, 3, 2, 1], [0, 1, 2, 3, 4], [0, 2, 2, 2, 2], [3, 1, 3, 1, 3]):
         out = oracle.child(np.array(lcp, np.uint64))
         assert out.size == len(lcp) and (out <= len(lcp)).all()
+
+
+def test_sampled_bytecode_restatement_matches_reference():
+    """oracle.sample_bytecode (the sampled byte coding restated from a sampled
+    build's SA, ISA and LCP) equals LcpStorage::BuildByteCodedDirect with
+    sampling rate K."""
+    from sufkit_b200 import synth
+    if oracle.ref() is None:
+        pytest.skip("the reference library was not built")
+    rng = np.random.default_rng(4)
+    texts = [synth.strain_collection(3, 3000, rng).logical_text(),
+             np.concatenate([np.full(1500, 2, np.uint8), np.zeros(1, np.uint8)]),
+             synth.human_scale_3gbp(scale=0.0002).logical_text()]
+    for t in texts:
+        for rate in (2, 5, 255, 256, 400):
+            sa, isa, lcp = oracle.ref_adapter_sampled(t, rate)
+            for width in (32, 64):
+                a = oracle.ref_bytecode_sampled(t, sa, isa, rate, width)
+                b = oracle.sample_bytecode(sa, isa, lcp, rate)
+                assert all(np.array_equal(x, y) for x, y in zip(a, b)), (t.size, rate, width)
