@@ -78,7 +78,8 @@ typedef struct sufgpu_build_desc {
    * multiples of K, as BuildDivsufsort's sampling_rate does
    * (src/divsufsort_backend.cpp:62-150): every plane then has ceil(n / K)
    * rows per instance, ISA[p / K] = sampled row, LCP = lcp of consecutive
-   * sampled rows (raw LCP only). */
+   * sampled rows; byte-coded LCP puts anchors at sampled text positions
+   * (src/lcp_storage.cpp:304-420 with rate K). */
   uint32_t sampling_rate;
   /* 0 = none.  1..10 = also build the Fast index's exact k-mer prefix
    * directory for this k (FastPrefixIndex, src/fast_prefix_index.cpp) into
