@@ -390,6 +390,23 @@ SUFGPU_API sufgpu_status sufgpu_encode_fasta(const char *path, uint8_t *out, uin
                                   uint64_t *size, uint64_t *fingerprint,
                                   uint64_t *records);
 
+/* The same normalisation on the device, for FASTA already in memory: raw is
+ * `bytes` bytes of plain (uncompressed) FASTA in host memory; out (host or
+ * device, cap bytes) receives the logical bytes without the sentinel, *size
+ * their count, *fingerprint their FNV-1a 64 (computed on the device; may be
+ * NULL) and *records the record count (may be NULL).  Record names and
+ * sequences are validated as GenomeReference::FromFasta does
+ * (src/genome_reference.cpp:88-122, 222-268).  Returns SUFGPU_UNSUPPORTED for
+ * input this path does not parse -- FASTQ records ('@' headers, '+' lines)
+ * and a lone carriage-return line right after a header, which kseq keeps as
+ * a base -- so the caller reads those with sufgpu_encode_fasta.  Replaces
+ * the per-byte loop of ReferenceBuilder::AppendRecord / AppendByte
+ * (src/genome_reference.cpp:125-156). */
+SUFGPU_API sufgpu_status sufgpu_encode_fasta_device(sufgpu_ctx *ctx, const uint8_t *raw,
+                                                    uint64_t bytes, uint8_t *out, uint64_t cap,
+                                                    uint64_t *size, uint64_t *fingerprint,
+                                                    uint64_t *records);
+
 #ifdef __cplusplus
 }
 #endif

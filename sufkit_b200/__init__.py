@@ -170,6 +170,10 @@ _SIGNATURES = {
                                             ctypes.POINTER(ctypes.c_uint64)]),
     "sufgpu_set_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int64]),
     "sufgpu_prefix_select_k": (ctypes.c_uint32, [ctypes.c_uint64, ctypes.c_uint64]),
+    "sufgpu_encode_fasta_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p,
+                                                  ctypes.c_uint64, ctypes.c_void_p,
+                                                  ctypes.c_uint64, ctypes.c_void_p,
+                                                  ctypes.c_void_p, ctypes.c_void_p]),
     "sufgpu_crc32_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
                                            ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]),
     "sufgpu_set_tuning_class": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_char_p,
@@ -498,6 +502,25 @@ class Context:
             out.append({"worker": int(worker.value), "start": times[0], "gate_in": times[1],
                         "gate_out": times[2], "end": times[3]})
         return out
+
+    def encode_fasta_bytes(self, raw) -> tuple[np.ndarray, int, int]:
+        """FASTA bytes (plain, in host memory) normalised on the device
+        (sufgpu_encode_fasta_device): (logical bytes without the sentinel,
+        FNV-1a 64 fingerprint, record count).  Raises SufkitError with
+        UNSUPPORTED_BACKEND for FASTQ and other input only the host reader
+        (encode_fasta) parses."""
+        buf = np.frombuffer(raw, np.uint8) if isinstance(raw, (bytes, bytearray)) else \
+            np.ascontiguousarray(raw, np.uint8)
+        out = np.empty(buf.size + 1, np.uint8)
+        size = ctypes.c_uint64()
+        fp = ctypes.c_uint64()
+        count = ctypes.c_uint64()
+        status = self._lib.sufgpu_encode_fasta_device(self._h, _ptr(buf), buf.size, _ptr(out),
+                                                      out.size, ctypes.byref(size),
+                                                      ctypes.byref(fp), ctypes.byref(count))
+        if status != 0:
+            _raise(status, self._error())
+        return out[: size.value].copy(), int(fp.value), int(count.value)
 
     def crc32_device(self, ptr: int, nbytes: int, crc_in: int = 0) -> int:
         """zlib's crc32(crc_in, data, nbytes) of device memory at ptr."""

@@ -15,6 +15,7 @@
 #include <chrono>
 #include <condition_variable>
 #include <cstdio>
+#include <cctype>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -24,6 +25,7 @@
 #include <system_error>
 #include <thread>
 #include <unordered_map>
+#include <unordered_set>
 #include <utility>
 #include <vector>
 
@@ -35,6 +37,7 @@
 #include "pack.cuh"
 #include "prefixdir.cuh"
 #include "crc32.cuh"
+#include "fasta.cuh"
 #include "radix.cuh"
 #include "runs.cuh"
 #include "segsort.cuh"
@@ -1848,6 +1851,148 @@ sufgpu_status sufgpu_crc32_device(sufgpu_ctx* ctx, const void* data, uint64_t by
     cudaGetLastError();
     return fail(ctx, SUFGPU_BUILD_FAILURE,
                 std::string("CUDA error in ") + err.what + ": " + cudaGetErrorString(err.code));
+  }
+}
+
+sufgpu_status sufgpu_encode_fasta_device(sufgpu_ctx* ctx, const uint8_t* raw, uint64_t bytes,
+                                         uint8_t* out, uint64_t cap, uint64_t* size,
+                                         uint64_t* fingerprint, uint64_t* records) {
+  if (!ctx || !size || (bytes > 0 && !raw)) return SUFGPU_INVALID_INPUT;
+  *size = 0;
+  // The first record starts at the first '>' or '@' (kseq skips to it).
+  u64 first = 0;
+  while (first < bytes && raw[first] != '>' && raw[first] != '@') ++first;
+  if (first == bytes) return fail(ctx, SUFGPU_INVALID_INPUT, "reference must contain at least one FASTA record");
+  if (raw[first] == '@') return fail(ctx, SUFGPU_UNSUPPORTED, "FASTQ input: use sufgpu_encode_fasta");
+  try {
+    SG_CUDA(cudaSetDevice(ctx->device));
+    sufgpu_ctx& c = *ctx;
+    const u64 tiles = (bytes + kFastaTile - 1) / kFastaTile;
+    const u64 header_cap = std::min<u64>(bytes / 2 + 2, u64(1) << 24);
+    const u64 chunk = bytes > (u64(64) << 20) ? 16384 : 4096;  // FNV chunk (16-byte multiple)
+    const u64 max_chunks = (bytes + 1 + chunk - 1) / chunk;
+    const u64 raw_bytes = round_up(bytes + 64, 256);
+    const u64 out_bytes = round_up(bytes + 64, 256);
+    const u64 status_bytes = round_up(2 * (tiles + 1) * 8, 256);
+    const u64 header_bytes = round_up(header_cap * sizeof(FastaHeader), 256);
+    const u64 fnv_bytes = round_up(max_chunks * 18, 256);
+    const u64 small_bytes = 256 + round_up(sizeof(DeviceFlags), 64);
+    c.arena.reserve(raw_bytes + out_bytes + status_bytes + header_bytes + fnv_bytes + small_bytes);
+    u8* at = static_cast<u8*>(c.arena.base);
+    u8* d_raw = at; at += raw_bytes;
+    u8* d_out = at; at += out_bytes;
+    u64* status = reinterpret_cast<u64*>(at); at += status_bytes;
+    FastaHeader* headers = reinterpret_cast<FastaHeader*>(at); at += header_bytes;
+    u64* mult = reinterpret_cast<u64*>(at);
+    u64* add = mult + max_chunks;
+    u8* fnv_start = reinterpret_cast<u8*>(add + max_chunks);
+    u8* fnv_end = fnv_start + max_chunks;
+    at += fnv_bytes;
+    u64* scalars = reinterpret_cast<u64*>(at);  // [0] header count, [1] out total, [2] counter|unsupported
+    DeviceFlags* flags = reinterpret_cast<DeviceFlags*>(at + 256);
+    cudaStream_t st = c.stream;
+    SG_CUDA(cudaMemcpyAsync(d_raw, raw, bytes, cudaMemcpyDefault, st));
+    SG_CUDA(cudaMemsetAsync(d_raw + bytes, 0, raw_bytes - bytes, st));
+    SG_CUDA(cudaMemsetAsync(status, 0, status_bytes, st));
+    SG_CUDA(cudaMemsetAsync(scalars, 0, small_bytes, st));
+    u32* counters = reinterpret_cast<u32*>(scalars + 2);  // [0] tile counter, [1] unsupported
+    fasta_normalize_kernel<<<static_cast<unsigned>(tiles), kFastaBlock, 0, st>>>(
+        d_raw, bytes, first, d_out, out_bytes - 1, status, status + tiles + 1, counters,
+        headers, header_cap, scalars + 0, counters + 1, scalars + 1, flags);
+    SG_CUDA(cudaGetLastError());
+    ++c.launches;
+    u64 host_scalars[3] = {0, 0, 0};
+    DeviceFlags host_flags{};
+    SG_CUDA(cudaMemcpyAsync(host_scalars, scalars, sizeof(host_scalars), cudaMemcpyDeviceToHost, st));
+    SG_CUDA(cudaMemcpyAsync(&host_flags, flags, sizeof(host_flags), cudaMemcpyDeviceToHost, st));
+    SG_CUDA(cudaStreamSynchronize(st));
+    if (host_flags.error) return fail(ctx, SUFGPU_BUILD_FAILURE, "device check failed in FASTA normalisation");
+    u32 unsupported = 0;
+    std::memcpy(&unsupported, reinterpret_cast<const u8*>(host_scalars + 2) + 4, 4);
+    if (unsupported & kFastaFastq) return fail(ctx, SUFGPU_UNSUPPORTED, "FASTQ records: use sufgpu_encode_fasta");
+    if (unsupported) {
+      return fail(ctx, SUFGPU_UNSUPPORTED,
+                  "a lone carriage-return line after a header: use sufgpu_encode_fasta");
+    }
+    const u64 heads = host_scalars[0];
+    u64 total = host_scalars[1];
+    if (heads > header_cap) return fail(ctx, SUFGPU_INVALID_INPUT, "too many FASTA records");
+    std::vector<FastaHeader> h(heads);
+    if (heads) {
+      SG_CUDA(cudaMemcpyAsync(h.data(), headers, heads * sizeof(FastaHeader), cudaMemcpyDeviceToHost, st));
+      SG_CUDA(cudaStreamSynchronize(st));
+      std::sort(h.begin(), h.end(), [](const FastaHeader& a, const FastaHeader& b) { return a.raw < b.raw; });
+    }
+    // Records: the first at `first`, one more per later header.  A bare '>' at
+    // the very end of the input opens no record (its 1 closes the previous one).
+    bool trailing_bare = heads > 0 && h.back().raw + 1 == bytes;
+    const u64 count = heads + (trailing_bare ? 0 : 1);
+    auto name_of = [&](u64 pos) {
+      u64 e = pos + 1;
+      while (e < bytes && !std::isspace(static_cast<unsigned char>(raw[e]))) ++e;
+      return std::string(reinterpret_cast<const char*>(raw + pos + 1), e - pos - 1);
+    };
+    std::unordered_set<std::string> names;
+    u64 start_out = 0;
+    for (u64 k = 0; k < count; ++k) {
+      const u64 pos = k == 0 ? first : h[k - 1].raw;
+      const u64 sep = k < heads ? h[k].out : total;  // where record k's 1 goes
+      const std::string name = name_of(pos);
+      if (name.empty()) return fail(ctx, SUFGPU_INVALID_INPUT, "FASTA record name must not be empty");
+      if (!names.insert(name).second) return fail(ctx, SUFGPU_INVALID_INPUT, "duplicate FASTA record name: " + name);
+      if (sep <= start_out) return fail(ctx, SUFGPU_INVALID_INPUT, "FASTA record must not be empty: " + name);
+      start_out = sep + 1;
+    }
+    if (!trailing_bare) {
+      SG_CUDA(cudaMemsetAsync(d_out + total, 1, 1, st));
+      ++total;
+    }
+    *size = total;
+    if (records) *records = count;
+    if (total > cap) return fail(ctx, SUFGPU_INVALID_INPUT, "output buffer too small");
+    if (out) SG_CUDA(cudaMemcpyAsync(out, d_out, total, cudaMemcpyDefault, st));
+    if (fingerprint) {
+      // FNV-1a 64 of the logical bytes (fasta.cuh): low byte at every chunk
+      // start from eight XOR-scanned passes, then one affine map per chunk.
+      constexpr u64 kBasis = 14695981039346656037ull;
+      const u64 chunks = (total + chunk - 1) / chunk;
+      std::vector<u8> start(chunks, 0), end_bit(chunks);
+      start[0] = static_cast<u8>(kBasis & 0xff);
+      const unsigned grid = static_cast<unsigned>(std::min<u64>((chunks + 255) / 256, u64(c.sm_count) * 16));
+      for (u32 j = 0; j < 8; ++j) {
+        SG_CUDA(cudaMemcpyAsync(fnv_start, start.data(), chunks, cudaMemcpyHostToDevice, st));
+        fnv_level_kernel<<<grid, 256, 0, st>>>(d_out, total, chunk, chunks, fnv_start, j, fnv_end);
+        SG_CUDA(cudaGetLastError());
+        SG_CUDA(cudaMemcpyAsync(end_bit.data(), fnv_end, chunks, cudaMemcpyDeviceToHost, st));
+        SG_CUDA(cudaStreamSynchronize(st));
+        u8 carry = 0;  // bit j at the start of chunk k: XOR of the end bits before it
+        for (u64 k = 0; k + 1 < chunks; ++k) {
+          carry ^= end_bit[k];
+          start[k + 1] |= static_cast<u8>(carry << j);
+        }
+      }
+      std::vector<u64> m(chunks), a(chunks);
+      SG_CUDA(cudaMemcpyAsync(fnv_start, start.data(), chunks, cudaMemcpyHostToDevice, st));
+      fnv_affine_kernel<<<grid, 256, 0, st>>>(d_out, total, chunk, chunks, fnv_start, mult, add);
+      SG_CUDA(cudaGetLastError());
+      SG_CUDA(cudaMemcpyAsync(m.data(), mult, chunks * 8, cudaMemcpyDeviceToHost, st));
+      SG_CUDA(cudaMemcpyAsync(a.data(), add, chunks * 8, cudaMemcpyDeviceToHost, st));
+      SG_CUDA(cudaStreamSynchronize(st));
+      u64 hash = kBasis;
+      for (u64 k = 0; k < chunks; ++k) hash = hash * m[k] + a[k];
+      *fingerprint = hash;
+      c.launches += 9;
+    }
+    SG_CUDA(cudaStreamSynchronize(st));
+    return SUFGPU_OK;
+  } catch (const CudaError& err) {
+    cudaGetLastError();
+    return fail(ctx, SUFGPU_BUILD_FAILURE,
+                std::string("CUDA error in ") + err.what + ": " + cudaGetErrorString(err.code));
+  } catch (const BuildError& err) {
+    return fail(ctx, err.status, err.message);
+  } catch (const std::exception& err) {
+    return fail(ctx, SUFGPU_BUILD_FAILURE, err.what());
   }
 }
 
