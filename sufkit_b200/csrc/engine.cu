@@ -324,6 +324,15 @@ struct sufgpu_ctx {
   std::vector<KernelTotals> profile;
   int sm_count = 148;
   cudaStream_t stream = nullptr;
+  // Output copies that overlap the LCP phase (single builds): a second
+  // stream, ordered after the compute stream by copy_ready, joined back by
+  // copy_done.
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t copy_ready = nullptr, copy_done = nullptr;
+  // Host threads zero-filling output planes that need no copy (the high
+  // planes of split40/48 coordinates below 2^32); the build joins them
+  // before it returns.
+  std::vector<std::thread> fillers;
   Arena arena;
   std::string last_error;
   u64* host_scalars = nullptr;  // pinned readback slots
@@ -411,7 +420,14 @@ struct Engine {
     gate_out = std::chrono::steady_clock::now();
     gate->unlock();
   }
+  void join_fillers() {
+    for (auto& t : c.fillers) {
+      if (t.joinable()) t.join();
+    }
+    c.fillers.clear();
+  }
   ~Engine() {
+    join_fillers();
     if (gate_held) gate->unlock();
   }
   bool runs_on = false;
@@ -1508,6 +1524,25 @@ void emit_sampled(Engine& e, const sufgpu_build_desc& d, sufgpu_outputs* outs,
   e.sync();
 }
 
+// Fills an output plane of `bytes` zero bytes: on the copy stream for device
+// memory, else by host threads (started now, joined before the build ends).
+void zero_plane(Engine& e, void* dst, u64 bytes) {
+  if (!dst || bytes == 0) return;
+  cudaPointerAttributes attr{};
+  if (cudaPointerGetAttributes(&attr, dst) != cudaSuccess) cudaGetLastError();
+  if (attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged) {
+    SG_CUDA(cudaMemsetAsync(dst, 0, bytes, e.c.copy_stream));
+    return;
+  }
+  const u64 parts = std::max<u64>(1, std::min<u64>(8, bytes >> 26));
+  const u64 step = (bytes + parts - 1) / parts;
+  for (u64 k = 0; k < parts; ++k) {
+    u8* at = static_cast<u8*>(dst) + k * step;
+    const u64 len = std::min(step, bytes - std::min(bytes, k * step));
+    if (len) e.c.fillers.emplace_back([at, len] { std::memset(at, 0, len); });
+  }
+}
+
 // CHILD table of the row LCP (child.cuh) into dst (host or device): the
 // minima tree and the nse/up/down arrays in k0/k1 (free once the LCP planes
 // are out), the table staged in x.
@@ -1619,15 +1654,43 @@ void emit_outputs(Engine& e, const sufgpu_build_desc& d, sufgpu_outputs* outs,
       }
     }
   };
-  if (want_isa) emit(L.rank, d.isa_storage_bits, true);
-  SG_CUDA(cudaEventRecord(c.ev[3], c.stream));
-  if (d.flags & SUFGPU_FLAG_VALIDATE) {
-    e.launch("validate", n * 8, validate_kernel, e.grid_stride_blocks(n, 256), 256, 0, e.sa,
-             L.rank,
-             n, e.segments(), L.flags);
+  // A single build whose coordinates fit 32 bits copies its 32/40/48-bit SA
+  // and ISA low planes straight from the device arrays on the copy stream,
+  // so the copies run under the LCP phase; their high planes are all zero
+  // and are filled without a copy.  64-bit planes are packed and copied on
+  // the compute stream.
+  const bool overlap = count == 1 && !e.want_crc && n <= 0xffffffffull;
+  auto fits32 = [](u32 bits) { return bits == 32 || bits == 40 || bits == 48; };
+  if (overlap) {
+    if (want_isa && !fits32(d.isa_storage_bits)) emit(L.rank, d.isa_storage_bits, true);
+    SG_CUDA(cudaEventRecord(c.ev[3], c.stream));
+    if (d.flags & SUFGPU_FLAG_VALIDATE) {
+      e.launch("validate", n * 8, validate_kernel, e.grid_stride_blocks(n, 256), 256, 0, e.sa,
+               L.rank, n, e.segments(), L.flags);
+    }
+    if (!fits32(d.sa_storage_bits)) emit(e.sa, d.sa_storage_bits, false);
+    SG_CUDA(cudaEventRecord(c.copy_ready, c.stream));
+    SG_CUDA(cudaStreamWaitEvent(c.copy_stream, c.copy_ready, 0));
+    if (want_isa && fits32(d.isa_storage_bits)) {
+      SG_CUDA(cudaMemcpyAsync(outs[0].isa_low, L.rank, n * 4, cudaMemcpyDefault, c.copy_stream));
+      zero_plane(e, outs[0].isa_high, high_bytes(d.isa_storage_bits, n));
+    }
+    if (fits32(d.sa_storage_bits)) {
+      SG_CUDA(cudaMemcpyAsync(outs[0].sa_low, e.sa, n * 4, cudaMemcpyDefault, c.copy_stream));
+      zero_plane(e, outs[0].sa_high, high_bytes(d.sa_storage_bits, n));
+    }
+    SG_CUDA(cudaEventRecord(c.ev[4], c.stream));
+  } else {
+    if (want_isa) emit(L.rank, d.isa_storage_bits, true);
+    SG_CUDA(cudaEventRecord(c.ev[3], c.stream));
+    if (d.flags & SUFGPU_FLAG_VALIDATE) {
+      e.launch("validate", n * 8, validate_kernel, e.grid_stride_blocks(n, 256), 256, 0, e.sa,
+               L.rank,
+               n, e.segments(), L.flags);
+    }
+    emit(e.sa, d.sa_storage_bits, false);
+    SG_CUDA(cudaEventRecord(c.ev[4], c.stream));
   }
-  emit(e.sa, d.sa_storage_bits, false);
-  SG_CUDA(cudaEventRecord(c.ev[4], c.stream));
 
   // LCP.
   if (d.lcp_encoding != SUFGPU_LCP_NONE) {
@@ -1707,8 +1770,13 @@ void emit_outputs(Engine& e, const sufgpu_build_desc& d, sufgpu_outputs* outs,
     }
     if (d.flags & SUFGPU_FLAG_CHILD) emit_child(e, ph.lcp, outs[0].child);
   }
+  if (overlap) {  // the compute stream ends after the overlapped copies
+    SG_CUDA(cudaEventRecord(c.copy_done, c.copy_stream));
+    SG_CUDA(cudaStreamWaitEvent(c.stream, c.copy_done, 0));
+  }
   SG_CUDA(cudaEventRecord(c.ev[5], c.stream));
   e.sync();
+  e.join_fillers();
 }
 
 // The knobs of one build: the context's, overridden by the first size class
@@ -1779,6 +1847,9 @@ sufgpu_status sufgpu_create(sufgpu_ctx** out, int device) {
     SG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     ctx->sm_count = sms;
     SG_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    SG_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+    SG_CUDA(cudaEventCreateWithFlags(&ctx->copy_ready, cudaEventDisableTiming));
+    SG_CUDA(cudaEventCreateWithFlags(&ctx->copy_done, cudaEventDisableTiming));
     SG_CUDA(cudaMallocHost(reinterpret_cast<void**>(&ctx->host_scalars), 64 * 8));
     SG_CUDA(cudaMallocHost(reinterpret_cast<void**>(&ctx->host_small), 1u << 20));
     for (auto& ev : ctx->ev) SG_CUDA(cudaEventCreate(&ev));
@@ -1810,9 +1881,12 @@ void sufgpu_destroy(sufgpu_ctx* ctx) {
   ctx->helpers.clear();
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
   for (auto& ev : ctx->ev) {
     if (ev) cudaEventDestroy(ev);
   }
+  if (ctx->copy_ready) cudaEventDestroy(ctx->copy_ready);
+  if (ctx->copy_done) cudaEventDestroy(ctx->copy_done);
   ctx->drop_round_graphs();
   if (ctx->crc_scratch) cudaFree(ctx->crc_scratch);
   if (ctx->host_scalars) cudaFreeHost(ctx->host_scalars);
@@ -1822,6 +1896,7 @@ void sufgpu_destroy(sufgpu_ctx* ctx) {
     ctx->arena.base = nullptr;
   }
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
   delete ctx;
 }
 
