@@ -31,6 +31,24 @@ def up_to_date() -> bool:
 
 
 DRIVER = HERE.parent / "tests" / "cpp" / "cuda_backend_driver"
+DSS_LIB = HERE / "libdivsufsort_cuda.so"
+DSS_SRC = HERE / "integration" / "divsufsort_cuda.cpp"
+
+
+def build_divsufsort_abi(verbose: bool = False) -> Path:
+    """libdivsufsort_cuda.so: divsufsort / divsufsort64 with libdivsufsort's
+    exact C ABI, linked against libsufgpu.so."""
+    inputs = [DSS_SRC, HERE.parent / "include" / "sufgpu" / "divsufsort_cuda.h", LIB]
+    if DSS_LIB.exists() and DSS_LIB.stat().st_mtime >= max(p.stat().st_mtime for p in inputs):
+        return DSS_LIB
+    cmd = [os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-fPIC", "-shared",
+           "-fvisibility=hidden", f"-I{HERE.parent / 'include'}", "-o", str(DSS_LIB),
+           str(DSS_SRC), f"-L{HERE}", "-lsufgpu", "-Wl,-rpath,$ORIGIN",
+           "-Wl,--exclude-libs,ALL"]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    return DSS_LIB
 
 
 def build_driver(verbose: bool = False) -> Path:
@@ -49,6 +67,7 @@ def build_driver(verbose: bool = False) -> Path:
 def build(force: bool = False, verbose: bool = False) -> Path:
     if not force and up_to_date():
         build_driver(verbose)
+        build_divsufsort_abi(verbose)
         return LIB
     nvcc = os.environ.get("NVCC", "nvcc")
     cmd = [nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
@@ -59,6 +78,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     subprocess.run(cmd, check=True)
     os.replace(str(LIB) + ".tmp", LIB)
     build_driver(verbose)
+    build_divsufsort_abi(verbose)
     return LIB
 
 

@@ -125,3 +125,31 @@ def test_sufkit_dropin_library_fails_loudly_without_a_device(tmp_path):
     assert out["rc"] == 6  # 1 + ErrorCode::kBuildFailure
     assert "CUDA" in out["error"]
     assert not (tmp_path / "g.sufidx").exists()
+
+
+def test_divsufsort_abi_library_exports_exactly_libdivsufsorts_entry_points():
+    """libdivsufsort_cuda.so exports divsufsort and divsufsort64, as
+    include/sufgpu/divsufsort_cuda.h declares them, and nothing else; without
+    a device both return -2 (divsufsort's allocation-failure code) and reject
+    bad arguments with -1."""
+    import ctypes
+    import subprocess
+    import torch
+    root = Path(__file__).resolve().parents[1]
+    lib_path = root / "sufkit_b200" / "libdivsufsort_cuda.so"
+    header = (root / "include" / "sufgpu" / "divsufsort_cuda.h").read_text()
+    declared = sorted(re.findall(r"saint_t\s+(divsufsort\w*)\s*\(", header))
+    assert declared == ["divsufsort", "divsufsort64"]
+    out = subprocess.run(["nm", "-D", "--defined-only", str(lib_path)], capture_output=True,
+                         text=True, check=True).stdout
+    exported = sorted(line.split()[-1] for line in out.splitlines() if " T " in line)
+    assert exported == declared
+    lib = ctypes.CDLL(str(lib_path))
+    lib.divsufsort64.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64]
+    lib.divsufsort.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32]
+    t = np.array([3, 2, 0], np.uint8)
+    sa = np.zeros(3, np.int64)
+    assert lib.divsufsort64(None, sa.ctypes.data, 3) == -1
+    assert lib.divsufsort64(t.ctypes.data, sa.ctypes.data, -1) == -1
+    if not torch.cuda.is_available():
+        assert lib.divsufsort64(t.ctypes.data, sa.ctypes.data, 3) == -2

@@ -164,3 +164,24 @@ def test_workload3_scaled_low_memory(ctx):
     r = check_full(ctx, t, sa_bits=40, isa_bits=0, lcp=sg.LcpEncoding.BYTE32)
     # The N runs are split directly after the seed instead of by ~17 rounds.
     assert r.stats["long_runs"] > 0 and r.stats["rounds"] < 10
+
+
+def test_libdivsufsort_abi_library(ctx):
+    """sufkit_b200/libdivsufsort_cuda.so: divsufsort / divsufsort64 with
+    libdivsufsort's exact C ABI equal the reference's divsufsort64."""
+    import ctypes
+    from pathlib import Path
+    lib = ctypes.CDLL(str(Path(sg.__file__).resolve().parent / "libdivsufsort_cuda.so"))
+    lib.divsufsort64.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64]
+    lib.divsufsort.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32]
+    rng = np.random.default_rng(31)
+    for t in (synth.plain_4mbp(scale=0.02).logical_text(), synth.random_text(rng, 1, 4),
+              rng.integers(0, 256, size=5000).astype(np.uint8)):
+        sa, _, _ = expected(t)
+        sa64 = np.empty(t.size, np.int64)
+        sa32 = np.empty(t.size, np.int32)
+        assert lib.divsufsort64(t.ctypes.data, sa64.ctypes.data, t.size) == 0
+        assert lib.divsufsort(t.ctypes.data, sa32.ctypes.data, t.size) == 0
+        assert (sa64 == sa.astype(np.int64)).all() and (sa32 == sa.astype(np.int32)).all()
+        if oracle.ref() is not None:
+            assert (sa64 == oracle.ref_divsufsort64(t)).all()
