@@ -576,6 +576,57 @@ window_scatter_kernel(const u64* __restrict__ pairs, u64 n, u32* __restrict__ ra
   for (u32 i = threadIdx.x; i < count; i += 256) rank[first + i] = window[i];
 }
 
+// Rank write by window slots (one instance).  Each (position << 32 | head)
+// pair takes the next slot of its window of 2^kSlotBits positions with one
+// atomic and is stored there; a window's pairs are then staged in shared
+// memory and its ranks written out whole.  Windows fill front to back, so
+// the partially written sectors of all windows (32 bytes each) stay in L2 and
+// leave it whole: one pass over the pairs instead of the keys-only radix
+// passes that group them by window.
+constexpr u32 kSlotBits = 13;
+constexpr u32 kSlotWindow = 1u << kSlotBits;
+
+static __global__ void __launch_bounds__(256)
+rank_slot_kernel(const u64* __restrict__ pairs, u64 n, u32* __restrict__ fill,
+                 u64* __restrict__ slotted, DeviceFlags* flags) {
+  const u64 windows = (n + kSlotWindow - 1) >> kSlotBits;
+  const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+  for (u64 r = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; r < n; r += stride) {
+    const u64 v = pairs[r];
+    const u64 w = (v >> 32) >> kSlotBits;
+    if (w >= windows) {
+      flag_error(flags, kErrBounds);  // not a permutation
+      continue;
+    }
+    const u32 slot = atomicAdd(fill + w, 1u);
+    if (slot >= kSlotWindow) {
+      flag_error(flags, kErrBounds);
+      continue;
+    }
+    slotted[(w << kSlotBits) + slot] = v;
+  }
+}
+
+// One block per slot window; dynamic shared memory of kSlotWindow words.
+static __global__ void __launch_bounds__(256)
+slot_window_scatter_kernel(const u64* __restrict__ slotted, u64 n, u32* __restrict__ rank,
+                           DeviceFlags* flags) {
+  extern __shared__ u32 window_smem[];
+  const u64 first = static_cast<u64>(blockIdx.x) << kSlotBits;
+  const u32 count = static_cast<u32>(n - first < kSlotWindow ? n - first : kSlotWindow);
+  for (u32 i = threadIdx.x; i < count; i += 256) {
+    const u64 v = slotted[first + i];
+    const u64 pos = v >> 32;
+    if ((pos >> kSlotBits) != blockIdx.x || (pos & (kSlotWindow - 1)) >= count) {
+      flag_error(flags, kErrBounds);  // not a permutation
+      continue;
+    }
+    window_smem[pos & (kSlotWindow - 1)] = static_cast<u32>(v);
+  }
+  __syncthreads();
+  for (u32 i = threadIdx.x; i < count; i += 256) rank[first + i] = window_smem[i];
+}
+
 // Long-run lookup for the rounds (runs.cuh builds it): sorted run starts and
 // ends plus a bitmap of the 2^kRunBlockBits-position blocks that hold run
 // members.  count == 0 disables it.

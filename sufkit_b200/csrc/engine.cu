@@ -239,6 +239,9 @@ struct Tuning {
   // symbols (rare symbols placed from a side list).
   bool two_bit_seed = true;
   u64 two_bit_min = u64(1) << 22;
+  // Seed rank write of a single instance by window slots (rank_slot_kernel)
+  // instead of radix passes grouping the pairs by window.
+  bool rank_slots = true;
 };
 
 // Overrides for builds whose longest instance has at most max_symbols symbols.
@@ -274,6 +277,8 @@ std::string apply_tuning(Tuning& t, const std::string& k, int64_t value) {
   } else if (k == "two_bit_min") {
     if (value < 0) return "two_bit_min must be >= 0";
     t.two_bit_min = static_cast<u64>(value);
+  } else if (k == "rank_slots") {
+    t.rank_slots = value != 0;
   } else if (k == "sort_block") {
     if (value != 256 && value != 512) return "sort_block must be 256 or 512";
     t.sort_block = static_cast<u32>(value);
@@ -1000,6 +1005,15 @@ struct Engine {
       launch("window_scatter", n * 12, segment_window_scatter_kernel, wbegin[segs], 256, 0,
              static_cast<const u64*>(grouped), segments(), static_cast<const u64*>(L.digit_start),
              L.rank, L.flags);
+    } else if (pos_bits > kWindowBits && c.tune.rank_slots) {
+      const u64 windows = (n + kSlotWindow - 1) >> kSlotBits;
+      u32* fill = reinterpret_cast<u32*>(L.status);  // windows words: n/8192 << status size
+      u64* slotted = pairs == L.k0 ? L.k1 : L.k0;
+      zero(fill, windows * 4);
+      launch("rank_slot", n * 16, rank_slot_kernel, grid_stride_blocks(n, 256), 256, 0,
+             static_cast<const u64*>(pairs), n, fill, slotted, L.flags);
+      launch("window_scatter", n * 12, slot_window_scatter_kernel, windows, 256,
+             kSlotWindow * 4, static_cast<const u64*>(slotted), n, L.rank, L.flags);
     } else if (pos_bits > kWindowBits) {
       const u64 b2[2] = {0, n};
       const u32 t = static_cast<u32>((n + c.tune.sort_tile - 1) / c.tune.sort_tile);
@@ -1014,7 +1028,7 @@ struct Engine {
                                  L.sort_tiles, 1, t, n, 32 + kWindowBits, 32 + pos_bits, false);
       grouped = sw ? other_keys : pairs;
     }
-    if (segs == 1) {
+    if (segs == 1 && !(pos_bits > kWindowBits && c.tune.rank_slots)) {
       launch("window_scatter", n * 12, window_scatter_kernel, (n + kWindow - 1) / kWindow, 256, 0,
              static_cast<const u64*>(grouped), n, L.rank, L.flags);
     }
@@ -1855,6 +1869,9 @@ sufgpu_status sufgpu_create(sufgpu_ctx** out, int device) {
     for (auto& ev : ctx->ev) SG_CUDA(cudaEventCreate(&ev));
     SG_CUDA(cudaFuncSetAttribute(seg_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(sizeof(SegSortSmem))));
+    SG_CUDA(cudaFuncSetAttribute(slot_window_scatter_kernel,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(kSlotWindow * 4)));
     for (bool ballot : {true, false}) {
       for (u32 tile : {2048u, 4096u}) {
         for (u32 block : {256u, 512u}) {

@@ -185,3 +185,15 @@ def test_libdivsufsort_abi_library(ctx):
         assert (sa64 == sa.astype(np.int64)).all() and (sa32 == sa.astype(np.int32)).all()
         if oracle.ref() is not None:
             assert (sa64 == oracle.ref_divsufsort64(t)).all()
+
+
+@pytest.mark.parametrize("slots", [0, 1])
+def test_rank_write_by_slots_or_passes(ctx, slots):
+    """The seed rank write by window slots and by radix passes give the same
+    (oracle-equal) build."""
+    t = synth.repeat_rich_100mbp(scale=0.03).logical_text()
+    ctx.set_tuning("rank_slots", slots)
+    try:
+        check_full(ctx, t, isa_bits=32, lcp=sg.LcpEncoding.RAW32)
+    finally:
+        ctx.set_tuning("rank_slots", 1)
