@@ -1,5 +1,9 @@
 """Autotuner for the build knobs (seed length, radix tile and block shape,
-ballot-ranking threshold, packed-seed threshold, two-bit seed).
+ballot-ranking threshold, packed-seed threshold, two-bit seed, the seed rank
+write by window slots, and the round-compaction threshold at which the graph
+rounds drop to a smaller bound).  The radix digit width is not a knob: every
+radix kernel is compiled for 8-bit digits (their shared-memory histograms and
+look-back words are sized by it).
 
     python -m sufkit_b200.autotune [--out sufkit_b200/tuning.json] [--quick]
 
@@ -32,9 +36,12 @@ CANDIDATES = {
     "ballot_min_elems": [1 << 23, 0, 1 << 62],
     "packed_max_bits": [24, 0],
     "two_bit_seed": [1, 0],
+    "rank_slots": [1, 0],
+    "graph_shrink": [4, 2, 16],
 }
 DEFAULTS = {"seed_symbols": 0, "sort_tile": 4096, "sort_block": 256,
-            "ballot_min_elems": 1 << 23, "packed_max_bits": 24, "two_bit_seed": 1}
+            "ballot_min_elems": 1 << 23, "packed_max_bits": 24, "two_bit_seed": 1,
+            "rank_slots": 1, "graph_shrink": 4}
 
 
 def workloads(quick: bool):
@@ -45,8 +52,8 @@ def workloads(quick: bool):
            [r.logical_text() for r in coll], LcpEncoding.RAW32)
     yield (1 << 28, "repeat-rich 100 Mbp", [synth.repeat_rich_100mbp(s).logical_text()],
            LcpEncoding.RAW32)
-    yield ((1 << 32) - 1, "human-scale 3.1 Gbp (scaled)",
-           [synth.human_scale_3gbp(0.1 if quick else 0.5).logical_text()], LcpEncoding.BYTE32)
+    yield ((1 << 32) - 1, "human-scale 3.1 Gbp" + (" (scaled x0.1)" if quick else ""),
+           [synth.human_scale_3gbp(0.1 if quick else 1.0).logical_text()], LcpEncoding.BYTE32)
 
 
 def timed_build(ctx: Context, texts, lcp, reps: int):

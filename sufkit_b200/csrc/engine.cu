@@ -242,6 +242,10 @@ struct Tuning {
   // Seed rank write of a single instance by window slots (rank_slot_kernel)
   // instead of radix passes grouping the pairs by window.
   bool rank_slots = true;
+  // Round compaction: the graph rounds switch to a graph captured for a
+  // smaller power-of-two bound once the active count falls below
+  // bound / graph_shrink (kernels are launched for the bound).
+  u32 graph_shrink = 4;
 };
 
 // Overrides for builds whose longest instance has at most max_symbols symbols.
@@ -277,6 +281,9 @@ std::string apply_tuning(Tuning& t, const std::string& k, int64_t value) {
   } else if (k == "two_bit_min") {
     if (value < 0) return "two_bit_min must be >= 0";
     t.two_bit_min = static_cast<u64>(value);
+  } else if (k == "graph_shrink") {
+    if (value < 2 || value > 1024) return "graph_shrink must be in [2, 1024]";
+    t.graph_shrink = static_cast<u32>(value);
   } else if (k == "rank_slots") {
     t.rank_slots = value != 0;
   } else if (k == "sort_block") {
@@ -1271,7 +1278,7 @@ struct Engine {
       if (count == 0) break;
       // A much smaller count than the graph's bound wastes empty blocks:
       // switch to the graph of a smaller bound.
-      if (count < bound / 4) bound = pow2(count);
+      if (count < bound / c.tune.graph_shrink) bound = pow2(count);
     }
     SG_CUDA(cudaMemcpyAsync(c.host_scalars + kTotals, L.scalars + kTotals, 16,
                             cudaMemcpyDeviceToHost, c.stream));
