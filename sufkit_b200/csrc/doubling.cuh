@@ -259,7 +259,9 @@ seed_keys_kernel(const u8* __restrict__ text, u64 n, Segments segs,
     }
   }
   __syncthreads();
-  for (u32 i = threadIdx.x; i < kSeedTile; i += kSeedBlock) {
+  // keys == null: histograms (and the rare list) only; seed_sorted_kernel
+  // generates the keys again and writes them partitioned by the first digit.
+  for (u32 i = threadIdx.x; keys && i < kSeedTile; i += kSeedBlock) {
     const u64 at = tile_first + i;
     if (at < n) {
       keys[at] = sm.keys[i];
@@ -599,11 +601,12 @@ rank_slot_kernel(const u64* __restrict__ pairs, u64 n, u32* __restrict__ fill,
       continue;
     }
     const u32 slot = atomicAdd(fill + w, 1u);
-    if (slot >= kSlotWindow) {
+    const u64 at = (w << kSlotBits) + slot;
+    if (slot >= kSlotWindow || at >= n) {  // more pairs than positions: not a permutation
       flag_error(flags, kErrBounds);
       continue;
     }
-    slotted[(w << kSlotBits) + slot] = v;
+    slotted[at] = v;
   }
 }
 

@@ -18,6 +18,7 @@
 #include <cctype>
 #include <cstring>
 #include <deque>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -40,6 +41,7 @@
 #include "fasta.cuh"
 #include "radix.cuh"
 #include "runs.cuh"
+#include "seedsort.cuh"
 #include "segsort.cuh"
 #include "serve.cuh"
 
@@ -242,6 +244,9 @@ struct Tuning {
   // Seed rank write of a single instance by window slots (rank_slot_kernel)
   // instead of radix passes grouping the pairs by window.
   bool rank_slots = true;
+  // Seed keys of one instance generated by the kernel that also does the
+  // first radix pass (seedsort.cuh) instead of written in position order.
+  bool seed_fused = true;
   // Round compaction: the graph rounds switch to a graph captured for a
   // smaller power-of-two bound once the active count falls below
   // bound / graph_shrink (kernels are launched for the bound).
@@ -281,6 +286,8 @@ std::string apply_tuning(Tuning& t, const std::string& k, int64_t value) {
   } else if (k == "two_bit_min") {
     if (value < 0) return "two_bit_min must be >= 0";
     t.two_bit_min = static_cast<u64>(value);
+  } else if (k == "seed_fused") {
+    t.seed_fused = value != 0;
   } else if (k == "graph_shrink") {
     if (value < 2 || value > 1024) return "graph_shrink must be in [2, 1024]";
     t.graph_shrink = static_cast<u32>(value);
@@ -507,10 +514,13 @@ struct Engine {
   // Radix sort (keys, vals) in place over [begin_bit, end_bit) using the
   // alternates as ping-pong buffers.  seg_begin/seg_tiles must be uploaded.
   // Returns true when the result ended in the alternate buffers.
+  // With pass0 set, the first pass is done by that callback (after the digit
+  // offsets are known) into keys/vals, and the launches start at pass 1.
   bool radix_sort(const char* name, u64* keys, u32* vals, u64* keys_alt, u32* vals_alt,
                   const u64* seg_begin, const u32* seg_tiles, u32 seg_count,
                   u32 total_tiles, u64 sort_elems, u32 begin_bit, u32 end_bit,
-                  bool check_needed, bool hist_ready = false) {
+                  bool check_needed, bool hist_ready = false,
+                  const std::function<void()>& pass0 = {}) {
     if (end_bit <= begin_bit || total_tiles == 0) return false;
     const u32 passes = (end_bit - begin_bit + kRadixBits - 1) / kRadixBits;
     SortSegments ss{seg_begin, seg_tiles, seg_count, total_tiles, c.tune.sort_tile};
@@ -544,7 +554,8 @@ struct Engine {
     u32* vin = vals;
     u64* kout = keys_alt;
     u32* vout = vals_alt;
-    for (u32 p = 0; p < passes; ++p) {
+    if (pass0) pass0();
+    for (u32 p = pass0 ? 1 : 0; p < passes; ++p) {
       if (!needed[p]) continue;
       zero(L.status, u64(total_tiles) * kRadixDigits * 8);
       zero(L.counters, 4);
@@ -884,6 +895,7 @@ struct Engine {
 
       // Seed keys and the segmented seed sort.
       seed_bits = sym_bits * symbols + tag;
+      const bool fused = segs == 1 && c.tune.seed_fused && c.tune.sort_tile == kSortTile;
       const u32 seed_passes = (seed_bits + kRadixBits - 1) / kRadixBits;
       zero(L.hist, u64(segs) * seed_passes * kRadixDigits * 4);
       if (two_bit) {
@@ -894,30 +906,50 @@ struct Engine {
         tb.rare_cap = rare_cap;
         tb.rare_count = L.scalars + 44;
         zero(L.scalars + 44, 8);
-        launch("seed_keys", packed_shift ? n * 9 : n * 13, seed_keys_kernel<true>,
+        launch("seed_keys", fused ? n : (packed_shift ? n * 9 : n * 13), seed_keys_kernel<true>,
                (n + kSeedTile - 1) / kSeedTile, kSeedBlock, sizeof(SeedSmem), L.text, n,
                segments(), static_cast<const u16*>(L.code), bits, symbols, seed_passes, L.hist,
-               packed_shift, L.k0, L.v0, tb);
+               packed_shift, fused ? nullptr : L.k0, fused ? nullptr : L.v0, tb);
         // Read back with the sort's pass check below (one synchronisation).
         SG_CUDA(cudaMemcpyAsync(c.host_scalars + 44, L.scalars + 44, 8, cudaMemcpyDeviceToHost,
                                 c.stream));
       } else {
-        launch("seed_keys", packed_shift ? n * 9 : n * 13, seed_keys_kernel<false>,
-               (n + kSeedTile - 1) / kSeedTile, kSeedBlock, sizeof(SeedSmem), L.text, n,
-               segments(), static_cast<const u16*>(L.code), bits, symbols, seed_passes, L.hist,
-               packed_shift, L.k0, L.v0, TwoBitSeed{});
+        launch("seed_keys", fused ? n : (packed_shift ? n * 9 : n * 13),
+               seed_keys_kernel<false>, (n + kSeedTile - 1) / kSeedTile, kSeedBlock,
+               sizeof(SeedSmem), L.text, n, segments(), static_cast<const u16*>(L.code), bits,
+               symbols, seed_passes, L.hist, packed_shift, fused ? nullptr : L.k0,
+               fused ? nullptr : L.v0, TwoBitSeed{});
       }
+      // The fused first pass (seedsort.cuh): generates the keys again and
+      // writes them into (k0, v0) partitioned by the lowest sorted digit.
+      const std::function<void()> pass0 = [&, two_bit_now = two_bit] {
+        zero(L.status, u64(seed_tiles) * kRadixDigits * 8);
+        zero(L.counters, 4);
+        const u64* d0 = L.digit_start;  // segment 0, pass 0
+        if (two_bit_now) {
+          launch("seed_sorted", n * (packed_shift ? 9 : 13), seed_sorted_kernel<true>, seed_tiles,
+                 kSortBlock, sizeof(SeedSortSmem), L.text, n, static_cast<const u16*>(L.code),
+                 bits, symbols, packed_shift, d0, L.k0, L.v0, L.status, L.counters, L.flags, tb);
+        } else {
+          launch("seed_sorted", n * (packed_shift ? 9 : 13), seed_sorted_kernel<false>,
+                 seed_tiles, kSortBlock, sizeof(SeedSortSmem), L.text, n,
+                 static_cast<const u16*>(L.code), bits, symbols, packed_shift, d0, L.k0, L.v0,
+                 L.status, L.counters, L.flags, TwoBitSeed{});
+        }
+      };
       keys = L.k0;
       if (packed_shift) {
         const bool swapped = radix_sort("seed_onesweep", L.k0, nullptr, L.k1, nullptr, L.seg_begin,
                                         L.seg_tiles, segs, seed_tiles, n, packed_shift,
-                                        packed_shift + seed_bits, true, true);
+                                        packed_shift + seed_bits, true, true,
+                                        fused ? pass0 : std::function<void()>());
         keys = swapped ? L.k1 : L.k0;
         sa = L.sa;
         spare = L.v0;
       } else {
         const bool swapped = radix_sort("seed_onesweep", L.k0, L.v0, L.k1, L.sa, L.seg_begin,
-                                        L.seg_tiles, segs, seed_tiles, n, 0, seed_bits, true, true);
+                                        L.seg_tiles, segs, seed_tiles, n, 0, seed_bits, true, true,
+                                        fused ? pass0 : std::function<void()>());
         if (swapped) {
           keys = L.k1;
           sa = L.sa;
@@ -1876,6 +1908,12 @@ sufgpu_status sufgpu_create(sufgpu_ctx** out, int device) {
     for (auto& ev : ctx->ev) SG_CUDA(cudaEventCreate(&ev));
     SG_CUDA(cudaFuncSetAttribute(seg_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(sizeof(SegSortSmem))));
+    SG_CUDA(cudaFuncSetAttribute(seed_sorted_kernel<true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(sizeof(SeedSortSmem))));
+    SG_CUDA(cudaFuncSetAttribute(seed_sorted_kernel<false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(sizeof(SeedSortSmem))));
     SG_CUDA(cudaFuncSetAttribute(slot_window_scatter_kernel,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(kSlotWindow * 4)));

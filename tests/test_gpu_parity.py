@@ -197,3 +197,22 @@ def test_rank_write_by_slots_or_passes(ctx, slots):
         check_full(ctx, t, isa_bits=32, lcp=sg.LcpEncoding.RAW32)
     finally:
         ctx.set_tuning("rank_slots", 1)
+
+
+@pytest.mark.parametrize("fused", [0, 1])
+@pytest.mark.parametrize("two_bit", [0, 1])
+def test_seed_first_pass_fused_or_separate(ctx, fused, two_bit):
+    """Seed keys generated by the kernel that also does the first radix pass,
+    or written in position order and sorted by the separate passes: the same
+    (oracle-equal) build, for code-table and two-bit seeds, packed and not."""
+    for t in (synth.repeat_rich_100mbp(scale=0.02).logical_text(),     # > 2^24: unpacked
+              synth.human_scale_3gbp(scale=0.002).logical_text(),      # N runs
+              synth.plain_4mbp(scale=0.5).logical_text()):             # packed
+        ctx.set_tuning("seed_fused", fused)
+        ctx.set_tuning("two_bit_min", 0 if two_bit else 1 << 62)
+        try:
+            check_full(ctx, t, isa_bits=32, lcp=sg.LcpEncoding.RAW32)
+            check_full(ctx, t, sa_bits=40, isa_bits=0, lcp=sg.LcpEncoding.BYTE32)
+        finally:
+            ctx.set_tuning("seed_fused", 1)
+            ctx.set_tuning("two_bit_min", 1 << 22)
