@@ -895,7 +895,7 @@ struct Engine {
 
       // Seed keys and the segmented seed sort.
       seed_bits = sym_bits * symbols + tag;
-      const bool fused = segs == 1 && c.tune.seed_fused && c.tune.sort_tile == kSortTile;
+      const bool fused = c.tune.seed_fused && c.tune.sort_tile == kSortTile;
       const u32 seed_passes = (seed_bits + kRadixBits - 1) / kRadixBits;
       zero(L.hist, u64(segs) * seed_passes * kRadixDigits * 4);
       if (two_bit) {
@@ -925,16 +925,18 @@ struct Engine {
       const std::function<void()> pass0 = [&, two_bit_now = two_bit] {
         zero(L.status, u64(seed_tiles) * kRadixDigits * 8);
         zero(L.counters, 4);
-        const u64* d0 = L.digit_start;  // segment 0, pass 0
+        const SortSegments ss{L.seg_begin, L.seg_tiles, segs, seed_tiles, kSortTile};
         if (two_bit_now) {
           launch("seed_sorted", n * (packed_shift ? 9 : 13), seed_sorted_kernel<true>, seed_tiles,
-                 kSortBlock, sizeof(SeedSortSmem), L.text, n, static_cast<const u16*>(L.code),
-                 bits, symbols, packed_shift, d0, L.k0, L.v0, L.status, L.counters, L.flags, tb);
+                 kSortBlock, sizeof(SeedSortSmem), L.text, ss, static_cast<const u16*>(L.code),
+                 bits, symbols, packed_shift, seed_passes, static_cast<const u64*>(L.digit_start),
+                 L.k0, L.v0, L.status, L.counters, L.flags, tb);
         } else {
           launch("seed_sorted", n * (packed_shift ? 9 : 13), seed_sorted_kernel<false>,
-                 seed_tiles, kSortBlock, sizeof(SeedSortSmem), L.text, n,
-                 static_cast<const u16*>(L.code), bits, symbols, packed_shift, d0, L.k0, L.v0,
-                 L.status, L.counters, L.flags, TwoBitSeed{});
+                 seed_tiles, kSortBlock, sizeof(SeedSortSmem), L.text, ss,
+                 static_cast<const u16*>(L.code), bits, symbols, packed_shift, seed_passes,
+                 static_cast<const u64*>(L.digit_start), L.k0, L.v0, L.status, L.counters,
+                 L.flags, TwoBitSeed{});
         }
       };
       keys = L.k0;

@@ -1,4 +1,4 @@
-// Seed keys fused with the first pass of the seed sort (one instance).
+// Seed keys fused with the first pass of the segmented seed sort.
 //
 // The seed sort is an LSD radix sort of the seed keys over 8-bit digits.  Its
 // first pass needs no stability: the order it preserves is the order of the
@@ -29,36 +29,48 @@ struct SeedSortSmem {
   long long digit_gbase[kRadixDigits];
   u64 warp_scan[kSortBlock / 32];
   u16 code[256];
-  __align__(16) u8 window[kSortTile + kSeedHalo];
+  // Text of the tile and its halo, staged from the 16-byte boundary at or
+  // below the tile's first position (an instance may start anywhere).
+  __align__(16) u8 window[kSortTile + kSeedHalo + 16];
   u32 tile;
 };
 
-// One tile of kSortTile positions per block (kSortBlock threads x
-// kSortItems consecutive positions each).  shift = the first sorted bit
-// (packed_shift or 0); digit_start = the absolute output offset of every
-// digit of pass 0.  kTwoBit keys as in seed_keys_kernel (rare rows were
-// already listed by the histogram pass).
+// One tile of the segmented seed sort per block (kSortBlock threads x
+// kSortItems consecutive positions each; tiles never cross an instance, as in
+// radix_onesweep_kernel).  shift = the first sorted bit (packed_shift or 0);
+// digit_start = [segment][pass][digit] absolute output offsets, of which pass
+// 0 is used.  kTwoBit keys as in seed_keys_kernel (rare rows were already
+// listed by the histogram pass).
 template <bool kTwoBit>
 static __global__ void __launch_bounds__(kSortBlock, 3)
-seed_sorted_kernel(const u8* __restrict__ text, u64 n, const u16* __restrict__ code_table,
-                   u32 bits, u32 symbols, u32 packed_shift, const u64* __restrict__ digit_start,
-                   u64* __restrict__ keys_out, u32* __restrict__ vals_out, u64* status,
-                   u32* tile_counter, DeviceFlags* flags, TwoBitSeed tb) {
+seed_sorted_kernel(const u8* __restrict__ text, SortSegments ss,
+                   const u16* __restrict__ code_table, u32 bits, u32 symbols, u32 packed_shift,
+                   u32 passes, const u64* __restrict__ digit_start, u64* __restrict__ keys_out,
+                   u32* __restrict__ vals_out, u64* status, u32* tile_counter, DeviceFlags* flags,
+                   TwoBitSeed tb) {
   static_assert(kSortTile == kSortBlock * kSortItems, "tile shape");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SeedSortSmem& sm = *reinterpret_cast<SeedSortSmem*>(smem_raw);
   sm.code[threadIdx.x] = code_table[threadIdx.x];
   sm.hist[threadIdx.x] = 0;
   const u32 tile = claim_tile(tile_counter, &sm.tile);
-  const u64 tile_first = static_cast<u64>(tile) * kSortTile;
-  for (int i = threadIdx.x; i < (kSortTile + kSeedHalo) / 16; i += kSortBlock) {
-    const u64 at = tile_first + static_cast<u64>(i) * 16;
+  u32 seg;
+  u64 first, last;
+  segment_of_tile(ss, tile, &seg, &first, &last);
+  const u64 seg_lo = ss.begin[seg];
+  const u64 seg_end = ss.begin[seg + 1];
+  const bool first_tile_of_segment = tile == ss.tile_begin[seg];
+  const u64 base = first & ~static_cast<u64>(15);
+  const u32 off = static_cast<u32>(first - base);
+  const u64 text_end = ss.begin[ss.count];  // the text buffer is padded past it
+  for (int i = threadIdx.x; i < (kSortTile + kSeedHalo + 16) / 16; i += kSortBlock) {
+    const u64 at = base + static_cast<u64>(i) * 16;
     uint4 v = make_uint4(0, 0, 0, 0);
-    if (at < n) v = *reinterpret_cast<const uint4*>(text + at);
+    if (at < text_end) v = *reinterpret_cast<const uint4*>(text + at);
     *reinterpret_cast<uint4*>(sm.window + i * 16) = v;
   }
   __syncthreads();
-  const u64 count = n - tile_first < kSortTile ? n - tile_first : kSortTile;
+  const u64 count = last - first;
   const u64 mask = symbols * bits >= 64 ? ~0ull : ((1ull << (symbols * bits)) - 1);
   const u64 mask2 = 2 * symbols >= 64 ? ~0ull : ((1ull << (2 * symbols)) - 1);
   const u32 smask = symbols >= 32 ? ~0u : ((1u << symbols) - 1);
@@ -78,24 +90,27 @@ seed_sorted_kernel(const u8* __restrict__ text, u64 n, const u16* __restrict__ c
 #pragma unroll
   for (int r = 0; r < kSortItems; ++r) {
     const u32 local = local0 + r;
-    const u64 pos = tile_first + local;
+    const u64 pos = first + local;
     out_key[r] = 0;
     rank[r] = 0;
     if (local >= count) continue;
     if (r == 0) {
-      for (u32 t = 0; t < symbols; ++t) push(pos + t < n ? sm.code[sm.window[local + t]] : 0u);
+      for (u32 t = 0; t < symbols; ++t) {
+        push(pos + t < seg_end ? sm.code[sm.window[off + local + t]] : 0u);
+      }
     } else {
       const u64 q = pos + symbols - 1;
-      push(q < n ? sm.code[sm.window[local + symbols - 1]] : 0u);
+      push(q < seg_end ? sm.code[sm.window[off + local + symbols - 1]] : 0u);
     }
     u64 sort_key = key;
     if (kTwoBit) sort_key = two_bit_key(key, k2, irregular, symbols, bits, tb);
-    out_key[r] = packed_shift ? (sort_key << packed_shift) | pos : sort_key;
+    out_key[r] = packed_shift ? (sort_key << packed_shift) | (pos - seg_lo) : sort_key;
     const u32 digit = static_cast<u32>((out_key[r] >> packed_shift) & 0xff);
     rank[r] = atomicAdd(&sm.hist[digit], 1u);  // unstable: see the file comment
   }
   __syncthreads();
-  // Per digit: the tile-local start, then the global start by look-back.
+  // Per digit: the tile-local start, then the global start by look-back
+  // (a segment's first tile seeds it from digit_start).
   const u32 d = threadIdx.x;
   const u32 digit_count = sm.hist[d];
   u64 tile_total;
@@ -104,8 +119,8 @@ seed_sorted_kernel(const u8* __restrict__ text, u64 n, const u16* __restrict__ c
   sm.digit_excl[d] = static_cast<u32>(local_start);
   u64* my_status = status + static_cast<u64>(tile) * kRadixDigits + d;
   u64 global_start;
-  if (tile == 0) {
-    global_start = digit_start[d];
+  if (first_tile_of_segment) {
+    global_start = digit_start[(static_cast<u64>(seg) * passes) * kRadixDigits + d];
     store_status(my_status, kFlagPrefix | ((global_start + digit_count) & kValueMask));
   } else {
     store_status(my_status, kFlagAggregate | digit_count);
@@ -129,14 +144,14 @@ seed_sorted_kernel(const u8* __restrict__ text, u64 n, const u16* __restrict__ c
     const u32 digit = static_cast<u32>((out_key[r] >> packed_shift) & 0xff);
     const u32 slot = sm.digit_excl[digit] + rank[r];
     sm.keys[slot] = out_key[r];
-    sm.vals[slot] = static_cast<u32>(tile_first + local);
+    sm.vals[slot] = static_cast<u32>(first + local);
   }
   __syncthreads();
   for (u32 s = threadIdx.x; s < count; s += kSortBlock) {
     const u64 k = sm.keys[s];
     const u32 digit = static_cast<u32>((k >> packed_shift) & 0xff);
     const u64 out = static_cast<u64>(sm.digit_gbase[digit] + static_cast<long long>(s));
-    if (out >= n) {  // only after a failed look-back
+    if (out < seg_lo || out >= seg_end) {  // only after a failed look-back
       flag_error(flags, kErrBounds);
       continue;
     }

@@ -41,3 +41,25 @@ def test_batch_against_oracle(ctx):
         # and the C restatement agrees with the compiled reference
         sa, isa, lcp = oracle.full_build(t)
         assert (b.sa_low == sa).all() and (b.lcp == lcp).all()
+
+
+@pytest.mark.parametrize("fused", [0, 1])
+def test_batch_seed_first_pass_fused_or_separate(ctx, fused):
+    """Batches whose seed keys come from the fused first-pass kernel (tiles
+    follow instance boundaries, instances start at any byte offset) equal the
+    oracle, as do batches sorted by the separate passes; packed (instances up
+    to 2^24 symbols) and unpacked."""
+    rng = np.random.default_rng(41)
+    texts = [synth.random_text(rng, int(n), 4) for n in (1, 7, 4095, 4097, 10_001, 65_536)]
+    texts += [r.logical_text() for r in synth.uneven_collection(count=5, scale=0.02)]
+    big = [synth.repeat_rich_100mbp(scale=0.18).logical_text(),   # > 2^24 symbols: unpacked
+           synth.random_text(rng, 3_333, 2)]
+    ctx.set_tuning("seed_fused", fused)
+    try:
+        for batch_texts in (texts, big):
+            batch = ctx.build_batch(batch_texts, sa_bits=32, isa_bits=32,
+                                    lcp=sg.LcpEncoding.RAW32, validate=True)
+            for t, b in zip(batch_texts, batch):
+                assert_oracle(b, t, sg.LcpEncoding.RAW32)
+    finally:
+        ctx.set_tuning("seed_fused", 1)
