@@ -124,6 +124,10 @@ struct TwoBitSeed {
   u32* rare_pos = nullptr;
   u64 rare_cap = 0;
   u64* rare_count = nullptr;  // may exceed rare_cap: the host then falls back
+  // Batches: a rare row's listed key carries its instance above the exact
+  // key's bits (instance << inst_shift | exact), so the list sorts by
+  // instance, then key.  0 for one instance.
+  u32 inst_shift = 0;
 };
 
 // Two-bit key from the window's exact key, its regular codes k2 (2 bits per
@@ -239,7 +243,7 @@ seed_keys_kernel(const u8* __restrict__ text, u64 n, Segments segs,
     if (kTwoBit) {
       const u64 slot = warp_append(tb.rare_count, rare);
       if (rare && slot < tb.rare_cap) {
-        tb.rare_key[slot] = key;
+        tb.rare_key[slot] = tb.inst_shift ? key | (static_cast<u64>(seg) << tb.inst_shift) : key;
         tb.rare_pos[slot] = static_cast<u32>(pos);
       }
     }
@@ -452,35 +456,49 @@ seed_rank_kernel(const u64* __restrict__ keys, u32* __restrict__ sa,
 // instance-local index below when packed).
 static __global__ void __launch_bounds__(256)
 rare_place_kernel(const u64* __restrict__ keys, u64 n, u32 packed_shift, RareRows rare,
-                  u32 bits, u32 symbols, u32* __restrict__ sa, u64* __restrict__ pairs,
-                  u32* __restrict__ lcp, DeviceFlags* flags) {
+                  u32 bits, u32 symbols, Segments segs, u32* __restrict__ sa,
+                  u64* __restrict__ pairs, u32* __restrict__ lcp, DeviceFlags* flags) {
   const u64 local_mask = packed_shift ? (1ull << packed_shift) - 1 : 0;
   const u32 unused = 64 - bits * symbols;
-  auto row_pos = [&](u64 r) -> u32 {  // a non-rare row's position
-    return packed_shift ? static_cast<u32>(keys[r] & local_mask) : sa[r];
-  };
-  auto rare_row = [&](u64 r) { return ((keys[r] >> packed_shift) & 1) == 0; };
+  const bool batch = segs.count > 1;
+  // Two-bit keys of a batch's rare list carry the instance above their bits.
+  const u32 k2_bits = 2 * symbols + 2;
+  const u64 k2_mask = k2_bits >= 64 ? ~0ull : (1ull << k2_bits) - 1;
   for (u64 idx = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; idx < rare.count;
        idx += static_cast<u64>(gridDim.x) * blockDim.x) {
     const u64 k = rare.k2[idx];
+    const u64 inst = batch ? k >> k2_bits : 0;
+    if (inst >= segs.count) {
+      flag_error(flags, kErrBounds);
+      continue;
+    }
+    const u64 lo = segs.begin[inst], hi = segs.begin[inst + 1];  // the instance's rows
+    const u64 kk = batch ? k & k2_mask : k;
+    auto row_pos = [&](u64 r) -> u32 {  // a non-rare row's (global) position
+      return packed_shift ? static_cast<u32>(lo + (keys[r] & local_mask)) : sa[r];
+    };
+    auto rare_row = [&](u64 r) { return ((keys[r] >> packed_shift) & 1) == 0; };
     const u64 i0 = lower_bound_u64(rare.k2, 0, idx, k);
-    const u64 g = lower_bound_u64(keys, 0, n, k << packed_shift);
+    const u64 g = lower_bound_u64(keys, lo, hi, kk << packed_shift);
     const u64 row = g + (idx - i0);
-    if (row >= n || (keys[row] >> packed_shift) != k) {
+    if (row >= hi || (keys[row] >> packed_shift) != kk) {
       flag_error(flags, kErrBounds);
       continue;
     }
     const u32 p = rare.pos[idx];
     const u64 ek = rare.key[idx];
     const u64 e0 = lower_bound_u64(rare.key, i0, idx, ek);
-    if (p >= n) {
+    if (p < lo || p >= hi) {
       flag_error(flags, kErrBounds);
       continue;
     }
     sa[row] = p;
-    pairs[row] = (static_cast<u64>(p) << 32) | static_cast<u32>(g + (e0 - i0));
+    // Batches pair the instance-local position with the head row (the rank
+    // write groups by windows of each instance).
+    const u64 pair_pos = batch ? p - lo : p;
+    pairs[row] = (pair_pos << 32) | static_cast<u32>(g + (e0 - i0));
     u32 v;
-    if (row == 0) {
+    if (row == lo) {
       v = 0;
     } else if (e0 < idx) {
       v = kLcpUnknown;  // the same window as the row before
@@ -492,12 +510,12 @@ rare_place_kernel(const u64* __restrict__ keys, u64 n, u32 packed_shift, RareRow
       const u32 x = static_cast<u32>(__clzll(static_cast<long long>(ek ^ rare.key[idx - 1])));
       v = (x - unused) / bits;
     } else {
-      v = window_lcp(rare.text, n, p, row_pos(row - 1), symbols);
+      v = window_lcp(rare.text, hi, p, row_pos(row - 1), symbols);
     }
     lcp[row] = v;
     const bool last = idx + 1 == rare.count || rare.k2[idx + 1] != k;
-    if (last && row + 1 < n && !rare_row(row + 1)) {
-      lcp[row + 1] = window_lcp(rare.text, n, row_pos(row + 1), p, symbols);
+    if (last && row + 1 < hi && !rare_row(row + 1)) {
+      lcp[row + 1] = window_lcp(rare.text, hi, row_pos(row + 1), p, symbols);
     }
   }
 }
@@ -508,7 +526,13 @@ rare_two_bit_kernel(const u64* __restrict__ key, u64 count, u32 symbols, u32 bit
                     TwoBitSeed tb, u64* __restrict__ k2) {
   for (u64 i = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
        i += static_cast<u64>(gridDim.x) * blockDim.x) {
-    k2[i] = two_bit_of_exact(key[i], symbols, bits, tb);
+    if (tb.inst_shift) {
+      const u64 inst = key[i] >> tb.inst_shift;
+      const u64 exact = key[i] & ((1ull << tb.inst_shift) - 1);
+      k2[i] = two_bit_of_exact(exact, symbols, bits, tb) | (inst << (2 * symbols + 2));
+    } else {
+      k2[i] = two_bit_of_exact(key[i], symbols, bits, tb);
+    }
   }
 }
 

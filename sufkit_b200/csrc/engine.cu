@@ -244,6 +244,8 @@ struct Tuning {
   // Seed rank write of a single instance by window slots (rank_slot_kernel)
   // instead of radix passes grouping the pairs by window.
   bool rank_slots = true;
+  // Two-bit seed keys for batches too (per-instance rare lists).
+  bool two_bit_batch = true;
   // Seed keys of one instance generated by the kernel that also does the
   // first radix pass (seedsort.cuh) instead of written in position order.
   bool seed_fused = true;
@@ -286,6 +288,8 @@ std::string apply_tuning(Tuning& t, const std::string& k, int64_t value) {
   } else if (k == "two_bit_min") {
     if (value < 0) return "two_bit_min must be >= 0";
     t.two_bit_min = static_cast<u64>(value);
+  } else if (k == "two_bit_batch") {
+    t.two_bit_batch = value != 0;
   } else if (k == "seed_fused") {
     t.seed_fused = value != 0;
   } else if (k == "graph_shrink") {
@@ -824,7 +828,8 @@ struct Engine {
     TwoBitSeed tb{};
     bool two_bit = false;
     bool keep_runs[256] = {};
-    if (allow_two_bit && segs == 1 && c.tune.two_bit_seed && n >= c.tune.two_bit_min && sigma >= 4 && bits <= 4) {
+    if (allow_two_bit && (segs == 1 || c.tune.two_bit_batch) && c.tune.two_bit_seed &&
+        n >= c.tune.two_bit_min && sigma >= 4 && bits <= 4) {
       int lo_byte = -1;
       u64 best = 0;
       for (int b = 0; b + 3 < 256; ++b) {
@@ -869,7 +874,9 @@ struct Engine {
       // Symbols per key: sym_bits each (+ 2 tag bits for the two-bit key).
       const u32 sym_bits = two_bit ? 2 : bits;
       const u32 tag = two_bit ? 2 : 0;
-      const u32 cap_symbols = two_bit ? std::min<u32>(64 / bits, 31) : 64 / bits;
+      // A batch's rare list keys carry the instance above the exact key.
+      const u32 inst_bits = segs > 1 ? std::max<u32>(1, bits_for(segs - 1)) : 0;
+      const u32 cap_symbols = two_bit ? std::min<u32>((64 - inst_bits) / bits, 31) : 64 / bits;
       symbols = (64 - tag) / sym_bits;
       if (c.tune.seed_symbols) {
         symbols = std::min(symbols, c.tune.seed_symbols);
@@ -882,8 +889,9 @@ struct Engine {
       // local index rides in the low key bits and the sort moves keys only.
       packed_shift = 0;
       if (c.tune.packed_max_bits && index_bits <= c.tune.packed_max_bits) {
-        u32 packed_symbols = std::min((64 - index_bits - tag) / sym_bits, cap_symbols);
-        if (c.tune.seed_symbols) packed_symbols = std::min(packed_symbols, c.tune.seed_symbols);
+        // No longer than the seed rule asks (fewer passes), no longer than
+        // the bits beside the index allow.
+        u32 packed_symbols = std::min({(64 - index_bits - tag) / sym_bits, cap_symbols, symbols});
         if (packed_symbols >= std::min<u32>(symbols, 12)) {
           packed_shift = index_bits;
           symbols = packed_symbols;
@@ -905,6 +913,7 @@ struct Engine {
         tb.rare_pos = rare_pos;
         tb.rare_cap = rare_cap;
         tb.rare_count = L.scalars + 44;
+        tb.inst_shift = segs > 1 ? bits * symbols : 0;
         zero(L.scalars + 44, 8);
         launch("seed_keys", fused ? n : (packed_shift ? n * 9 : n * 13), seed_keys_kernel<true>,
                (n + kSeedTile - 1) / kSeedTile, kSeedBlock, sizeof(SeedSmem), L.text, n,
@@ -979,8 +988,9 @@ struct Engine {
       SG_CUDA(cudaMemcpyAsync(L.sort_begin, c.host_small + 16384, 16, cudaMemcpyHostToDevice, c.stream));
       SG_CUDA(cudaMemcpyAsync(L.sort_tiles, c.host_small + 16384 + 16, 8, cudaMemcpyHostToDevice,
                               c.stream));
+      const u32 rare_bits = bits * symbols + (segs > 1 ? std::max<u32>(1, bits_for(segs - 1)) : 0);
       const bool sw = radix_sort("rare_sort", rare_key, rare_pos, rare_key_alt, rare_pos_alt,
-                                 L.sort_begin, L.sort_tiles, 1, t, rare_count, 0, bits * symbols,
+                                 L.sort_begin, L.sort_tiles, 1, t, rare_count, 0, rare_bits,
                                  false);
       rare.key = sw ? rare_key_alt : rare_key;
       rare.pos = sw ? rare_pos_alt : rare_pos;
@@ -1004,7 +1014,7 @@ struct Engine {
            L.scalars + 0, L.flags, runs_on ? 1u : 0u, segs > 1 ? 1u : 0u);
     if (rare.count > 0) {
       launch("rare_place", rare.count * 32, rare_place_kernel, grid_stride_blocks(rare.count, 256),
-             256, 0, static_cast<const u64*>(keys), n, packed_shift, rare, bits, symbols, sa,
+             256, 0, static_cast<const u64*>(keys), n, packed_shift, rare, bits, symbols, segments(), sa,
              pairs, L.lcp, L.flags);
       // Rare rows in shared windows join the active list (count in [45]).
       const u64 rare_tiles = (rare.count + kScanTile - 1) / kScanTile;

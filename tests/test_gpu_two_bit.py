@@ -160,3 +160,30 @@ def test_workload_shapes_match_code_table_seed(make):
         assert (a is None and b is None) or (a == b).all(), f
     sa, isa, _ = expected(t)
     assert (two.sa == sa).all() and (two.isa == isa).all()
+
+
+@pytest.mark.parametrize("two_bit_batch", [0, 1])
+def test_two_bit_seed_in_batches(ctx, two_bit_batch):
+    """Batches with two-bit seed keys: each instance's rare rows (windows that
+    reach a separator, the sentinel, an N or the instance end) sorted by
+    (instance, exact key) and placed within the instance.  Every instance
+    equals the oracle, with and without the batch two-bit seed; instances of
+    different sizes, N runs, contigs, and exact-key ties across instances."""
+    from conftest import assert_oracle
+    rng = np.random.default_rng(77)
+    texts = [r.logical_text() for r in synth.uneven_collection(count=6, scale=0.01)]
+    same = synth.random_text(rng, 3000, 4)
+    texts += [same.copy(), same.copy()]                       # identical instances
+    texts.append(synth.human_scale_3gbp(scale=0.0005).logical_text())  # N runs
+    texts.append(np.concatenate([np.full(50, 6, np.uint8), synth.random_text(rng, 2000, 4)]))
+    ctx.set_tuning("two_bit_min", 0)
+    ctx.set_tuning("two_bit_batch", two_bit_batch)
+    try:
+        for lcp in (sg.LcpEncoding.RAW32, sg.LcpEncoding.BYTE32):
+            batch = ctx.build_batch(texts, sa_bits=32, isa_bits=32, lcp=lcp, validate=True)
+            assert (ctx.last_stats["seed_code_bits"] == 2) == bool(two_bit_batch)
+            for t, b in zip(texts, batch):
+                assert_oracle(b, t, lcp)
+    finally:
+        ctx.set_tuning("two_bit_min", 1 << 22)
+        ctx.set_tuning("two_bit_batch", 1)
