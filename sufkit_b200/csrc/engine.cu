@@ -210,8 +210,18 @@ OnesweepVariant variant_for(u32 block, u32 tile) {
 }
 
 // Onesweep variants: ranking by ballots or match-any; 4096-key tiles (256x16,
-// 512x8) or 2048-key tiles (256x8); key-value pairs or keys only.
-OnesweepVariant onesweep_variant(bool ballot, u32 block, u32 tile, bool vals) {
+// 512x8) or 2048-key tiles (256x8); key-value pairs or keys only.  tma: the
+// 256x16 tile's keys by one bulk copy (single-segment sorts only).
+OnesweepVariant onesweep_variant(bool ballot, u32 block, u32 tile, bool vals, bool tma = false) {
+  if (tma && tile == 4096 && block == 256) {
+    const u64 smem = sizeof(OnesweepSmem<256, 4096>);
+    if (ballot) {
+      return vals ? OnesweepVariant{radix_onesweep_kernel<true, 256, 16, true, true>, 256, smem}
+                  : OnesweepVariant{radix_onesweep_kernel<true, 256, 16, false, true>, 256, smem};
+    }
+    return vals ? OnesweepVariant{radix_onesweep_kernel<false, 256, 16, true, true>, 256, smem}
+                : OnesweepVariant{radix_onesweep_kernel<false, 256, 16, false, true>, 256, smem};
+  }
   if (ballot) return vals ? variant_for<true, true>(block, tile) : variant_for<true, false>(block, tile);
   return vals ? variant_for<false, true>(block, tile) : variant_for<false, false>(block, tile);
 }
@@ -244,6 +254,8 @@ struct Tuning {
   // Seed rank write of a single instance by window slots (rank_slot_kernel)
   // instead of radix passes grouping the pairs by window.
   bool rank_slots = true;
+  // Onesweep tiles of single-segment sorts loaded by one bulk (TMA) copy.
+  bool tma_tile = false;
   // Two-bit seed keys for batches too (per-instance rare lists).
   bool two_bit_batch = true;
   // Seed keys of one instance generated by the kernel that also does the
@@ -288,6 +300,8 @@ std::string apply_tuning(Tuning& t, const std::string& k, int64_t value) {
   } else if (k == "two_bit_min") {
     if (value < 0) return "two_bit_min must be >= 0";
     t.two_bit_min = static_cast<u64>(value);
+  } else if (k == "tma_tile") {
+    t.tma_tile = value != 0;
   } else if (k == "two_bit_batch") {
     t.two_bit_batch = value != 0;
   } else if (k == "seed_fused") {
@@ -564,7 +578,8 @@ struct Engine {
       zero(L.status, u64(total_tiles) * kRadixDigits * 8);
       zero(L.counters, 4);
       const OnesweepVariant v = onesweep_variant(c.tune.ballot_rank && elems >= c.tune.ballot_min_elems,
-                                                 c.tune.sort_block, c.tune.sort_tile, vals != nullptr);
+                                                 c.tune.sort_block, c.tune.sort_tile, vals != nullptr,
+                                                 c.tune.tma_tile && seg_count == 1);
       launch(name, elems * (vals ? 24 : 16), v.fn, total_tiles, v.block, v.smem,
              kin, vin, kout, vout, ss, begin_bit + p * kRadixBits, p, passes,
              L.digit_start, L.status, L.counters, L.flags);
@@ -1933,9 +1948,11 @@ sufgpu_status sufgpu_create(sufgpu_ctx** out, int device) {
       for (u32 tile : {2048u, 4096u}) {
         for (u32 block : {256u, 512u}) {
           for (bool vals : {true, false}) {
-            const OnesweepVariant v = onesweep_variant(ballot, block, tile, vals);
-            SG_CUDA(cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(v.smem)));
+            for (bool tma : {false, true}) {
+              const OnesweepVariant v = onesweep_variant(ballot, block, tile, vals, tma);
+              SG_CUDA(cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           static_cast<int>(v.smem)));
+            }
           }
         }
       }

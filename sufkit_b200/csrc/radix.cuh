@@ -124,14 +124,57 @@ struct OnesweepSmem {
   u32 digit_excl[kRadixDigits];
   long long digit_gbase[kRadixDigits];
   u64 warp_scan[kBlock / 32];
+  u64 mbar;  // completion barrier of the bulk tile load (kTma)
   u32 tile;
 };
+
+// Bulk (TMA engine) copy of `bytes` contiguous bytes from this GPU's global
+// memory into the CTA's shared memory, completing on an mbarrier: one
+// cp.async.bulk, no multicast.  dst, src 16-byte aligned; bytes a multiple
+// of 16.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, u32 bytes, u64* mbar) {
+  const u32 d = static_cast<u32>(__cvta_generic_to_shared(dst));
+  const u32 m = static_cast<u32>(__cvta_generic_to_shared(mbar));
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      :: "r"(d), "l"(src), "r"(bytes), "r"(m) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(u64* mbar, u32 count) {
+  const u32 m = static_cast<u32>(__cvta_generic_to_shared(mbar));
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(m), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(u64* mbar, u32 bytes) {
+  const u32 m = static_cast<u32>(__cvta_generic_to_shared(mbar));
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+               :: "r"(m), "r"(bytes) : "memory");
+}
+
+// Waits for phase 0 of the barrier; false after the spin limit (the caller
+// flags an error instead of hanging).
+__device__ __forceinline__ bool mbar_wait0(u64* mbar) {
+  const u32 m = static_cast<u32>(__cvta_generic_to_shared(mbar));
+  for (u32 spins = 0; spins < kSpinLimit; ++spins) {
+    u32 done = 0;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done) : "r"(m), "r"(0u) : "memory");
+    if (done) return true;
+  }
+  return false;
+}
 
 // kVals = false sorts keys only (vals_in/vals_out unused): the packed seed
 // carries each suffix's instance-local index in the low key bits.
 // Blocks per SM: three 256x16, four 256x8, two 512x8.  Registers are capped so
 // that occupancy, not the allocator, decides.
-template <bool kBallot, int kBlock, int kItems, bool kVals = true>
+// kTma: the tile's keys arrive by one bulk copy into shared memory (single-
+// segment sorts, whose tiles start on 4096-key boundaries) instead of
+// per-thread loads; the rest is the same.
+template <bool kBallot, int kBlock, int kItems, bool kVals = true, bool kTma = false>
 static __global__ void __launch_bounds__(kBlock, kBlock == 512 ? 2 : (kItems <= 8 ? 4 : 3))
 radix_onesweep_kernel(const u64* __restrict__ keys_in,
                       const u32* __restrict__ vals_in,
@@ -161,11 +204,26 @@ radix_onesweep_kernel(const u64* __restrict__ keys_in,
   u64 key[kItems];
   u32 rank[kItems];
   const u32 warp_base = warp * 32 * kItems;
+  u32 bulk = 0;  // keys that arrived by the bulk copy (an even count: 16-byte multiple)
+  if (kTma) {
+    bulk = count & ~1u;
+    if (threadIdx.x == 0) mbar_init(&sm.mbar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      mbar_expect_tx(&sm.mbar, bulk * 8);
+      if (bulk) bulk_load(sm.keys, keys_in + first, bulk * 8, &sm.mbar);
+    }
+    if (!mbar_wait0(&sm.mbar)) {
+      flag_error(flags, kErrLookbackTimeout, 30);
+      bulk = 0;  // fall back to global loads (the build already failed)
+    }
+  }
 #pragma unroll
   for (int i = 0; i < kItems; ++i) {
     const u32 slot = warp_base + i * 32 + lane;
-    key[i] = slot < count ? keys_in[first + slot] : ~0ull;
+    key[i] = slot < count ? (slot < bulk ? sm.keys[slot] : keys_in[first + slot]) : ~0ull;
   }
+  if (kTma) __syncthreads();  // sm.keys is the scatter buffer below
   // Stable warp-level ranking by digit; invalid slots never update counters.
   // kBallot selects peers with eight ballots over the digit bits instead of
   // one match-any.

@@ -216,3 +216,16 @@ def test_seed_first_pass_fused_or_separate(ctx, fused, two_bit):
         finally:
             ctx.set_tuning("seed_fused", 1)
             ctx.set_tuning("two_bit_min", 1 << 22)
+
+
+@pytest.mark.parametrize("tma", [0, 1])
+def test_onesweep_bulk_tile_load(ctx, tma):
+    """Single-segment radix passes with the tile's keys loaded by one bulk
+    (TMA) copy or by per-thread loads: the same (oracle-equal) build."""
+    t = synth.repeat_rich_100mbp(scale=0.03).logical_text()
+    ctx.set_tuning("tma_tile", tma)
+    try:
+        check_full(ctx, t, isa_bits=32, lcp=sg.LcpEncoding.RAW32)
+        check_full(ctx, synth.random_text(np.random.default_rng(3), 9_999, 2))
+    finally:
+        ctx.set_tuning("tma_tile", 0)
