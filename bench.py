@@ -676,6 +676,15 @@ def main():
                              "libdivsufsort64 + Kasai LCP via detail::BuildDivsufsort64, "
                              "1 thread (divsufsort is serial)",
                    "host": host_info()}
+            # The second CPU baseline: CaPS-SA as sufkit vendors it, all host
+            # threads, SA + its construction LCP, same sample.
+            threads = os.cpu_count() or 1
+            width = 32 if sample.size <= 0xFFFFFFFF else 64
+            _, _, caps_sec = oracle.ref_caps(sample, threads=threads, width=width)
+            cpu["caps_sa"] = {"value": sample.size / caps_sec / 1e9, "unit": "Gsym/s",
+                              "cores": threads, "kind": "reference",
+                              "sample": f"the same {sample.size} symbols, detail::BuildCaps"
+                                        f"{width} with LCP, {threads} threads"}
 
     if rank == 0:
         line = {

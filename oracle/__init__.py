@@ -88,6 +88,7 @@ def ref() -> Optional[ctypes.CDLL]:
         lib.sufref_pack.argtypes = [P, U64, U64, ctypes.c_int, P, P, P, P]
         lib.sufref_bytecoded_direct.argtypes = [P, U64, P, P, ctypes.c_int, P, P, P, U64, P]
         lib.sufref_bytecoded_from_raw.argtypes = [P, P, U64, ctypes.c_int, P, P, P, U64, P]
+        lib.sufref_caps_build.argtypes = [ctypes.c_int, P, U64, ctypes.c_uint32, P, P, P]
         lib.sufref_bytecoded_direct_sampled.argtypes = [P, U64, P, P, U64, ctypes.c_uint32,
                                                         ctypes.c_int, P, P, P, U64, P]
         lib.sufref_bytecoded_exact.argtypes = [P, U64, P, P, U64, P, P, U64, P]
@@ -213,6 +214,19 @@ def ref_adapter(text: np.ndarray, width: int = 64, threads: int = 1):
     _check(lib, lib.sufref_adapter_build(width, _p(t), t.size, 1, 1, threads, _p(sa), _p(isa),
                                          _p(lcp), sec))
     return sa, isa, lcp, list(sec)
+
+
+def ref_caps(text: np.ndarray, threads: int = 1, width: int = 32, lcp: bool = True):
+    """detail::BuildCaps32/64 (CaPS-SA as vendored by sufkit): (sa, lcp or
+    None, seconds) with `threads` workers."""
+    lib = ref()
+    t = np.ascontiguousarray(text, np.uint8)
+    sa = np.empty(max(t.size, 1), np.uint64)
+    l = np.empty(max(t.size, 1), np.uint64) if lcp else None
+    sec = (ctypes.c_double * 1)()
+    _check(lib, lib.sufref_caps_build(width, _p(t), t.size, threads, _p(sa),
+                                      _p(l) if lcp else None, sec))
+    return sa[: t.size], (l[: t.size] if lcp else None), sec[0]
 
 
 def ref_adapter_sampled(text: np.ndarray, rate: int, width: int = 64, threads: int = 1):

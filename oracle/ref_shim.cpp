@@ -10,6 +10,7 @@
 //   LcpStorage::BuildByteCoded*    src/lcp_storage.cpp:217-420, 532-563
 //   GenomeReference::FromFasta     src/genome_reference.cpp:222-268
 //   SuffixArray::Build / Save      src/suffix_array.cpp:4086-4390, 4853-4916
+//   detail::BuildCaps32/64         src/caps_backend.cpp (CaPS-SA, third_party/caps-sa)
 
 #include <algorithm>
 #include <chrono>
@@ -31,6 +32,7 @@
 
 #include <sufkit/sufkit.hpp>
 
+#include "caps_backend.hpp"
 #include "coordinate_storage.hpp"
 #include "divsufsort_backend.hpp"
 #include "fast_prefix_index.hpp"
@@ -285,6 +287,32 @@ int sufref_pack(const uint64_t* values, uint64_t count, uint64_t symbol_count,
         std::move(input), WidthFromBits(storage_bits), symbol_count,
         ErrorCode::kBuildFailure, "suffix array");
     ExportCoordinates(storage, low32, high, native64, width_out);
+    return 0;
+  } catch (const std::exception& error) {
+    return Fail(error);
+  }
+}
+
+// detail::BuildCaps32/64: the CaPS-SA parallel constructor sufkit vendors,
+// SA (and its construction LCP when lcp_out is not null) as uint64 rows;
+// seconds[0] = wall time of the call.
+int sufref_caps_build(int width, const uint8_t* text, uint64_t n, uint32_t threads,
+                      uint64_t* sa_out, uint64_t* lcp_out, double* seconds) {
+  try {
+    std::vector<uint8_t> t(text, text + n);
+    const auto begin = std::chrono::steady_clock::now();
+    auto copy = [&](const auto& built) {
+      if (seconds) {
+        seconds[0] = std::chrono::duration<double>(std::chrono::steady_clock::now() - begin)
+                         .count();
+      }
+      for (uint64_t i = 0; i < built.suffix_array.size(); ++i) sa_out[i] = built.suffix_array[i];
+      if (lcp_out) {
+        for (uint64_t i = 0; i < built.lcp.size(); ++i) lcp_out[i] = built.lcp[i];
+      }
+    };
+    if (width == 32) copy(sufkit::detail::BuildCaps32(t, threads, lcp_out != nullptr));
+    else copy(sufkit::detail::BuildCaps64(t, threads, lcp_out != nullptr));
     return 0;
   } catch (const std::exception& error) {
     return Fail(error);

@@ -180,3 +180,18 @@ def test_sampled_bytecode_restatement_matches_reference():
                 a = oracle.ref_bytecode_sampled(t, sa, isa, rate, width)
                 b = oracle.sample_bytecode(sa, isa, lcp, rate)
                 assert all(np.array_equal(x, y) for x, y in zip(a, b)), (t.size, rate, width)
+
+
+def test_caps_sa_baseline_matches_divsufsort():
+    """The CaPS-SA constructor sufkit vendors (compiled into the oracle as the
+    second CPU baseline) gives divsufsort's SA and LCP."""
+    from sufkit_b200 import synth
+    if oracle.ref() is None:
+        pytest.skip("the reference library was not built")
+    rng = np.random.default_rng(12)
+    for t in (synth.repeat_rich_100mbp(scale=0.002).logical_text(),
+              synth.human_scale_3gbp(scale=0.0001).logical_text(),
+              synth.random_text(rng, 5000, 2)):
+        sa, lcp, sec = oracle.ref_caps(t, threads=4)
+        ref_sa, _, ref_lcp, _ = oracle.ref_adapter(t, 64)
+        assert np.array_equal(sa, ref_sa) and np.array_equal(lcp, ref_lcp) and sec >= 0
