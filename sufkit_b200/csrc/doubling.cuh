@@ -654,6 +654,71 @@ slot_window_scatter_kernel(const u64* __restrict__ slotted, u64 n, u32* __restri
   for (u32 i = threadIdx.x; i < count; i += 256) rank[first + i] = window_smem[i];
 }
 
+// The same for a batch: windows of 2^kSlotBits instance-local positions,
+// numbered per instance from wbegin (wbegin[j] = the first window of
+// instance j); pairs carry instance-local positions.  The slots of window w
+// of instance j are rows begin_j + w * 2^kSlotBits onward.
+static __global__ void __launch_bounds__(256)
+rank_slot_segments_kernel(const u64* __restrict__ pairs, Segments segs,
+                          const u64* __restrict__ wbegin, u32* __restrict__ fill,
+                          u64* __restrict__ slotted, DeviceFlags* flags) {
+  const u64 n = segs.begin[segs.count];
+  const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
+  SegCursor cur;
+  for (u64 r = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; r < n; r += stride) {
+    cur.locate(segs.begin, segs.count, r);
+    const u64 v = pairs[r];
+    const u64 local = v >> 32;
+    const u64 len = cur.hi - cur.lo;
+    if (local >= len) {
+      flag_error(flags, kErrBounds);  // not a permutation
+      continue;
+    }
+    const u64 w = local >> kSlotBits;
+    const u32 slot = atomicAdd(fill + wbegin[cur.j] + w, 1u);
+    const u64 at = cur.lo + (w << kSlotBits) + slot;
+    if (slot >= kSlotWindow || at >= cur.hi) {
+      flag_error(flags, kErrBounds);
+      continue;
+    }
+    slotted[at] = v;
+  }
+}
+
+// One block per window of the batch; dynamic shared memory of kSlotWindow words.
+static __global__ void __launch_bounds__(256)
+slot_segment_window_scatter_kernel(const u64* __restrict__ slotted, Segments segs,
+                                   const u64* __restrict__ wbegin, u32* __restrict__ rank,
+                                   DeviceFlags* flags) {
+  extern __shared__ u32 window_smem[];
+  u32 lo = 0, hi = segs.count;  // instance j with wbegin[j] <= blockIdx.x < wbegin[j + 1]
+  while (hi - lo > 1) {
+    const u32 mid = (lo + hi) >> 1;
+    if (wbegin[mid] <= blockIdx.x) lo = mid;
+    else hi = mid;
+  }
+  const u64 w = blockIdx.x - wbegin[lo];
+  const u64 base = segs.begin[lo];
+  const u64 len = segs.begin[lo + 1] - base;
+  const u64 first = w << kSlotBits;
+  if (first >= len) {
+    flag_error(flags, kErrBounds);
+    return;
+  }
+  const u32 count = static_cast<u32>(len - first < kSlotWindow ? len - first : kSlotWindow);
+  for (u32 i = threadIdx.x; i < count; i += 256) {
+    const u64 v = slotted[base + first + i];
+    const u64 local = v >> 32;
+    if ((local >> kSlotBits) != w || (local & (kSlotWindow - 1)) >= count) {
+      flag_error(flags, kErrBounds);  // not a permutation
+      continue;
+    }
+    window_smem[local & (kSlotWindow - 1)] = static_cast<u32>(v);
+  }
+  __syncthreads();
+  for (u32 i = threadIdx.x; i < count; i += 256) rank[base + first + i] = window_smem[i];
+}
+
 // Long-run lookup for the rounds (runs.cuh builds it): sorted run starts and
 // ends plus a bitmap of the 2^kRunBlockBits-position blocks that hold run
 // members.  count == 0 disables it.

@@ -1048,7 +1048,27 @@ struct Engine {
     // per 8 bits of the longest instance above 11, not of the whole batch).
     const u32 pos_bits = std::max<u32>(1, bits_for(n - 1));
     u64* grouped = pairs;
-    if (segs > 1) {
+    if (segs > 1 && c.tune.rank_slots) {
+      // Window slots per instance (rank_slot_segments_kernel): no grouping passes.
+      std::vector<u64> wbegin(segs + 1, 0);
+      for (u32 j = 0; j < segs; ++j) {
+        wbegin[j + 1] = wbegin[j] + (begin[j + 1] - begin[j] + kSlotWindow - 1) / kSlotWindow;
+      }
+      const u64 windows = wbegin[segs];
+      u32* fill = reinterpret_cast<u32*>(L.status);  // windows words: n/8192 + segs
+      u64* slotted = pairs == L.k0 ? L.k1 : L.k0;
+      sync();
+      std::memcpy(c.host_small, wbegin.data(), (segs + 1) * 8);
+      SG_CUDA(cudaMemcpyAsync(L.digit_start, c.host_small, (segs + 1) * 8, cudaMemcpyHostToDevice,
+                              c.stream));
+      zero(fill, windows * 4);
+      launch("rank_slot", n * 16, rank_slot_segments_kernel, grid_stride_blocks(n, 256), 256, 0,
+             static_cast<const u64*>(pairs), segments(), static_cast<const u64*>(L.digit_start),
+             fill, slotted, L.flags);
+      launch("window_scatter", n * 12, slot_segment_window_scatter_kernel, windows, 256,
+             kSlotWindow * 4, static_cast<const u64*>(slotted), segments(),
+             static_cast<const u64*>(L.digit_start), L.rank, L.flags);
+    } else if (segs > 1) {
       u64 longest = 1;
       std::vector<u64> wbegin(segs + 1, 0);
       for (u32 j = 0; j < segs; ++j) {
@@ -1941,6 +1961,9 @@ sufgpu_status sufgpu_create(sufgpu_ctx** out, int device) {
     SG_CUDA(cudaFuncSetAttribute(seed_sorted_kernel<false>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(sizeof(SeedSortSmem))));
+    SG_CUDA(cudaFuncSetAttribute(slot_segment_window_scatter_kernel,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(kSlotWindow * 4)));
     SG_CUDA(cudaFuncSetAttribute(slot_window_scatter_kernel,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(kSlotWindow * 4)));

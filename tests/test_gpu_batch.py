@@ -63,3 +63,21 @@ def test_batch_seed_first_pass_fused_or_separate(ctx, fused):
                 assert_oracle(b, t, sg.LcpEncoding.RAW32)
     finally:
         ctx.set_tuning("seed_fused", 1)
+
+
+@pytest.mark.parametrize("slots", [0, 1])
+def test_batch_rank_write_by_slots_or_passes(ctx, slots):
+    """A batch's seed rank write by per-instance window slots or by grouping
+    passes: the same (oracle-equal) instances, including instances shorter
+    than a window and exactly one window long."""
+    rng = np.random.default_rng(43)
+    texts = [synth.random_text(rng, int(n), 4) for n in (1, 2, 8191, 8192, 8193, 20_000)]
+    texts += [r.logical_text() for r in synth.uneven_collection(count=4, scale=0.01)]
+    ctx.set_tuning("rank_slots", slots)
+    try:
+        batch = ctx.build_batch(texts, sa_bits=32, isa_bits=32, lcp=sg.LcpEncoding.RAW32,
+                                validate=True)
+        for t, b in zip(texts, batch):
+            assert_oracle(b, t, sg.LcpEncoding.RAW32)
+    finally:
+        ctx.set_tuning("rank_slots", 1)
