@@ -127,3 +127,40 @@ def test_served_strain_collection_full_size_against_divsufsort():
     assert np.array_equal(r.lcp, primary), "byte-coded primaries differ"
     assert np.array_equal(r.anchor_positions.astype(np.uint64), pos), "anchor positions differ"
     assert np.array_equal(r.anchor_values.astype(np.uint64), val), "anchor values differ"
+
+
+def _mem_available_gb() -> float:
+    try:
+        for line in open("/proc/meminfo"):
+            if line.startswith("MemAvailable"):
+                return int(line.split()[1]) / 1048576
+    except OSError:
+        pass
+    return 0.0
+
+
+@pytest.mark.skipif(os.environ.get("SUFGPU_FULL_REFERENCE_3G") != "1",
+                    reason="opt-in (SUFGPU_FULL_REFERENCE_3G=1): divsufsort64 at 3.1 Gsym takes "
+                           "about 10 minutes and 80 GB of host memory")
+def test_human_scale_3gbp_word_for_word_against_divsufsort64():
+    """The full 3.1 Gbp build word for word against the reference's
+    BuildDivsufsort64 (SA and LCP compared by blake2b digests of their rows).
+    Needs about 110 GB of free host memory; skipped below that."""
+    torch = pytest.importorskip("torch")
+    _need_reference()
+    if _mem_available_gb() < 110:
+        pytest.skip("not run: host RAM")
+    text = synth.human_scale_3gbp().logical_text()
+    n = int(text.size)
+    dev = torch.device("cuda", 0)
+    d_text = torch.from_numpy(text).to(dev)
+    sa = torch.empty(n, dtype=torch.int32, device=dev)
+    lcp = torch.empty(n, dtype=torch.int32, device=dev)
+    with sg.Context(0) as ctx:
+        ctx.build_device(d_text.data_ptr(), n, {"sa_low": sa.data_ptr(), "lcp": lcp.data_ptr()},
+                         sa_bits=32, isa_bits=0, lcp=sg.LcpEncoding.RAW32, validate=True)
+    ours = oracle.digest_planes(sa.cpu().numpy().view(np.uint32), lcp.cpu().numpy().view(np.uint32))
+    del sa, lcp, d_text
+    torch.cuda.empty_cache()
+    ref_sa, _, ref_lcp, _ = oracle.ref_adapter(text, 64)
+    assert ours == oracle.digest_planes(ref_sa, ref_lcp)
