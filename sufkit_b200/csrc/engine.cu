@@ -254,6 +254,9 @@ struct Tuning {
   // Seed rank write of a single instance by window slots (rank_slot_kernel)
   // instead of radix passes grouping the pairs by window.
   bool rank_slots = true;
+  // Round sort tiles whose groups have at most this many rows rank by
+  // counting inside each group (0: always the shared-memory radix passes).
+  u32 seg_small_group = kSegSmallGroup;
   // Onesweep tiles of single-segment sorts loaded by one bulk (TMA) copy.
   bool tma_tile = false;
   // Two-bit seed keys for batches too (per-instance rare lists).
@@ -300,6 +303,9 @@ std::string apply_tuning(Tuning& t, const std::string& k, int64_t value) {
   } else if (k == "two_bit_min") {
     if (value < 0) return "two_bit_min must be >= 0";
     t.two_bit_min = static_cast<u64>(value);
+  } else if (k == "seg_small_group") {
+    if (value < 0 || value > 4096) return "seg_small_group must be in [0, 4096]";
+    t.seg_small_group = static_cast<u32>(value);
   } else if (k == "tma_tile") {
     t.tma_tile = value != 0;
   } else if (k == "two_bit_batch") {
@@ -1179,7 +1185,7 @@ struct Engine {
     launch("seg_sort", bound * 24, seg_sort_kernel, (bound + kSegWindow - 1) / kSegWindow,
            kSegBlock, sizeof(SegSortSmem), static_cast<const u64*>(L.k0), other, rs.count,
            static_cast<const u32*>(gstart()), static_cast<const u64*>(L.scalars + 1),
-           bits_for(n), L.k1, act, L.counters + 48, abort, tag, L.flags);
+           bits_for(n), L.k1, act, L.counters + 48, abort, tag, L.flags, c.tune.seg_small_group);
   }
 
   // Global passes over (id, second) bits for `active` rows: (k0, other) ->

@@ -1,5 +1,11 @@
 // Segmented sort of a doubling round's composite keys inside shared memory.
 //
+// Rows arrive grouped (each group is a contiguous run of the active list), so
+// a tile whose groups are all small (at most small_group rows) needs no
+// passes at all: each row's place in its group is the number of rows of the
+// group with a smaller second key (ties by position), O(group size) shared
+// memory reads per row.  Tiles with a larger group take the radix passes.
+//
 // A round sorts the active rows by (dense group id, second key), but rows only
 // move inside their own group, and groups are small (copies of a repeat).  So
 // instead of LSD passes over all id and key bits through HBM, each block takes
@@ -22,6 +28,10 @@ constexpr int kSegBlock = 256;
 constexpr int kSegItems = 16;
 constexpr int kSegCap = kSegBlock * kSegItems;  // rows one block sorts
 constexpr int kSegWindow = kSegCap / 2;          // group starts per block
+// Default for small_group: tiles whose groups all have at most this many
+// rows rank each row by counting inside its group instead of running the
+// radix passes.
+constexpr u32 kSegSmallGroup = 96;
 
 struct SegSortSmem {
   u64 keys[kSegCap];
@@ -30,6 +40,7 @@ struct SegSortSmem {
   u32 digit_excl[kRadixDigits];
   u64 warp_scan[kSegBlock / 32];
   u32 range[4];  // lo, hi, first group, groups
+  u32 largest;   // rows of the tile's largest group
 };
 
 // First index in gstart[0, groups) with gstart[i] >= x (groups if none).
@@ -55,7 +66,7 @@ seg_sort_kernel(const u64* __restrict__ ckey, const u32* __restrict__ cval,
                 const u64* __restrict__ count_ptr,
                 const u32* __restrict__ gstart, const u64* __restrict__ group_count,
                 u32 second_bits, u64* __restrict__ out_keys, u32* __restrict__ out_vals,
-                u32* big, u64* abort, u64 abort_tag, DeviceFlags* flags) {
+                u32* big, u64* abort, u64 abort_tag, DeviceFlags* flags, u32 small_group) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SegSortSmem& sm = *reinterpret_cast<SegSortSmem*>(smem_raw);
   constexpr int kWarps = kSegBlock / 32;
@@ -95,10 +106,46 @@ seg_sort_kernel(const u64* __restrict__ ckey, const u32* __restrict__ cval,
   }
   // Tile-local composite keys: (local group << second_bits) | second.
   const u64 second_mask = (1ull << second_bits) - 1;
+  if (threadIdx.x == 0) sm.largest = 0;
   for (u32 s = threadIdx.x; s < n_rows; s += kSegBlock) {
     const u64 k = ckey[lo + s];
     sm.keys[s] = (((k >> second_bits) - g_first) << second_bits) | (k & second_mask);
     sm.vals[0][s] = cval[lo + s];
+  }
+  // The tile's largest group.
+  u32 largest = 0;
+  for (u32 g = threadIdx.x; g < n_groups; g += kSegBlock) {
+    const u32 gs = gstart[g_first + g];
+    const u32 ge = g + 1 < n_groups ? gstart[g_first + g + 1] : lo + n_rows;
+    largest = max(largest, ge - gs);
+  }
+  for (int offset = 16; offset > 0; offset >>= 1) {
+    largest = max(largest, __shfl_xor_sync(0xffffffffu, largest, offset));
+  }
+  __syncthreads();  // sm.largest = 0 is visible
+  if (lane == 0 && largest) atomicMax(&sm.largest, largest);
+  __syncthreads();
+  if (sm.largest <= small_group) {
+    // Rank by counting inside the group; positions are tile-local.
+    for (u32 s = threadIdx.x; s < n_rows; s += kSegBlock) {
+      const u64 k = sm.keys[s];
+      const u32 g = static_cast<u32>(k >> second_bits);
+      const u32 gs = gstart[g_first + g] - lo;
+      const u32 ge = g + 1 < n_groups ? gstart[g_first + g + 1] - lo : n_rows;
+      if (gs > s || ge <= s || ge > n_rows) {  // inconsistent group table
+        flag_error(flags, kErrBounds);
+        continue;
+      }
+      const u64 mine = k & second_mask;
+      u32 below = 0;
+      for (u32 j = gs; j < ge; ++j) {
+        const u64 other = sm.keys[j] & second_mask;
+        below += (other < mine) || (other == mine && j < s);
+      }
+      out_keys[lo + gs + below] = (static_cast<u64>(g + g_first) << second_bits) | mine;
+      out_vals[lo + gs + below] = sm.vals[0][s];
+    }
+    return;
   }
   const u32 total_bits = second_bits + max(1u, bits_for(n_groups > 0 ? n_groups - 1 : 0));
   const u32 passes = (total_bits + kRadixBits - 1) / kRadixBits;

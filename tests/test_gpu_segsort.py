@@ -91,3 +91,26 @@ def test_graph_rounds_equal_host_rounds(ctx, kind):
         assert r.stats["seg_sort_fallbacks"] == host.stats["seg_sort_fallbacks"]
     if kind == "tandem":
         assert host.stats["seg_sort_fallbacks"] > 0
+
+
+@pytest.mark.parametrize("small", [0, 2, 96, 4096])
+def test_rank_by_counting_or_passes(ctx, small):
+    """Round tiles ranked by counting inside their groups (groups of at most
+    `small` rows) or by the shared-memory radix passes (0: always passes;
+    4096: counting for every tile that fits a block): the same oracle-equal
+    build on repeat-rich text, tandem repeats and a long run."""
+    rng = np.random.default_rng(5)
+    texts = [synth.repeat_rich_100mbp(scale=0.01).logical_text(),
+             np.concatenate([np.tile(synth.random_text(rng, 7, 4)[:6], 3000),
+                             synth.random_text(rng, 20000, 4)]),
+             np.concatenate([np.full(30000, 2, np.uint8), synth.random_text(rng, 5000, 4)])]
+    ctx.set_tuning("seg_small_group", small)
+    ctx.set_tuning("graph_rounds", 0)  # cached round graphs hold the knob of their capture
+    try:
+        for t in texts:
+            r = ctx.build(t, sa_bits=32, isa_bits=32, lcp=sg.LcpEncoding.RAW32, validate=True)
+            sa, isa, lcp = expected(t)
+            assert (r.sa_low == sa).all() and (r.isa_low == isa).all() and (r.lcp == lcp).all()
+    finally:
+        ctx.set_tuning("seg_small_group", 96)
+        ctx.set_tuning("graph_rounds", 1)
