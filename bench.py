@@ -85,6 +85,21 @@ def workload(name: str, scale: float = 1.0, count: int = 256):
                 "0.1% N runs; Fast profile SA+ISA+raw LCP32, 32-bit storage")
         return [ref.logical_text()], desc
     if name == "plain3g":
+        # SUFGPU_SYNTH_CACHE=<dir> keeps the generated text between runs of
+        # one session (the generator is seeded: the file is the same text).
+        cache = os.environ.get("SUFGPU_SYNTH_CACHE")
+        desc = ("human-scale 3.1 Gbp plain build: 25 contigs (50-250 Mbp), GC 41%, 50% "
+                "interspersed repeats, 1% segmental duplications, 150 Mbp of N in runs of "
+                "10 kbp-3 Mbp; Low-memory profile: 64-bit construction, split40 SA storage, "
+                "byte-coded LCP (32-bit anchors), no resident ISA")
+        if cache:
+            path = Path(cache) / f"human_scale_3gbp_{scale}.npy"
+            if path.exists():
+                return [np.load(path)], desc
+            text = synth.human_scale_3gbp(scale).logical_text()
+            path.parent.mkdir(parents=True, exist_ok=True)
+            np.save(path, text)
+            return [text], desc
         ref = synth.human_scale_3gbp(scale)
         desc = ("human-scale 3.1 Gbp plain build: 25 contigs (50-250 Mbp), GC 41%, 50% "
                 "interspersed repeats, 1% segmental duplications, 150 Mbp of N in runs of "
