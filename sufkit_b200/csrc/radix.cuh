@@ -206,7 +206,11 @@ radix_onesweep_kernel(const u64* __restrict__ keys_in,
   const u32 warp_base = warp * 32 * kItems;
   u32 bulk = 0;  // keys that arrived by the bulk copy (an even count: 16-byte multiple)
   if (kTma) {
-    bulk = count & ~1u;
+    // The bulk copy needs a 16-byte aligned source; some callers sort
+    // buffers at 8-byte offsets (a second ping-pong half), which take the
+    // per-thread loads instead (bulk = 0: the barrier completes at once).
+    const bool aligned = (reinterpret_cast<uintptr_t>(keys_in + first) & 15) == 0;
+    bulk = aligned ? count & ~1u : 0;
     if (threadIdx.x == 0) mbar_init(&sm.mbar, 1);
     __syncthreads();
     if (threadIdx.x == 0) {

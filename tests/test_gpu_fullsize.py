@@ -16,8 +16,9 @@
   exact SA and LCP of a raw build of the same text, and the Low-memory planes
   (split40 SA, byte primaries, anchors) are compared word for word with that
   build and with the byte coding restated from it on the device;
-* one served strain collection at full size (50 copies of a 2 Mbp genome,
-  LCPs up to ~2 Mbp): SA and byte-coded LCP against divsufsort64.
+* one served strain collection at full size (50 copies of a 2 Mbp genome at
+  0.1% SNP + 0.01% indel, so most suffixes share kbp prefixes with 49 others):
+  SA and byte-coded LCP against divsufsort64.
 """
 import multiprocessing as mp
 import os
@@ -121,7 +122,7 @@ def test_served_strain_collection_full_size_against_divsufsort():
         ticket = server.submit(text, 32, 0, sg.LcpEncoding.BYTE32)
         r = server.wait(ticket)
     sa, isa, lcp, _ = oracle.ref_adapter(text, 64)
-    assert int(lcp.max()) > 1_000_000  # the long-LCP shape
+    assert int(lcp.max()) > 1_000  # copies agree over kbp stretches between their SNPs
     assert np.array_equal(r.sa_low, sa.astype(np.uint32)), "SA differs"
     primary, pos, val = oracle.bytecode(text, sa, isa, 32)
     assert np.array_equal(r.lcp, primary), "byte-coded primaries differ"
