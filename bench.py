@@ -107,12 +107,16 @@ def workload(name: str, scale: float = 1.0, count: int = 256):
                 "byte-coded LCP (32-bit anchors), no resident ISA")
         return [ref.logical_text()], desc
     if name == "batched":
-        refs = synth.uneven_collection(count=count, scale=scale)
+        # Per-reference random streams (synth.uneven_reference), generated in
+        # parallel: the collection tests/test_gpu_fullsize.py checks against
+        # divsufsort64 reference by reference.
+        texts = synth.uneven_texts(1024 if count <= 1024 else count, scale,
+                                   indices=range(count))
         desc = (f"batched uneven collection: first {count} of 1,024 bacterial-like references "
                 "(log-normal sizes, median 4 Mbp, clipped 0.5-12 Mbp, GC 30-70%, 1-8 contigs); "
                 "SA + raw LCP32 per reference, 32-bit, HBM-admitted batch launches, "
                 "compared with the plain build one reference at a time")
-        return [r.logical_text() for r in refs], desc
+        return texts, desc
     ref = synth.repeat_rich_100mbp(scale)
     desc = ("repeat-rich 100 Mbp plain build: 24 contigs, GC 41%, 25% interspersed "
             "repeats (500 families, 5-15% divergence), 3% tandem repeats, 0.5% N runs; "

@@ -47,9 +47,8 @@ DEFAULTS = {"seed_symbols": 0, "sort_tile": 4096, "sort_block": 256,
 def workloads(quick: bool):
     """(max_symbols, name, texts, lcp) per size class."""
     s = 0.25 if quick else 1.0
-    coll = synth.uneven_collection(count=32 if quick else 256)
-    yield (1 << 24, "bacterial collection (batched)",
-           [r.logical_text() for r in coll], LcpEncoding.RAW32)
+    coll = synth.uneven_texts(1024, indices=range(32 if quick else 256))
+    yield (1 << 24, "bacterial collection (batched)", coll, LcpEncoding.RAW32)
     yield (1 << 28, "repeat-rich 100 Mbp", [synth.repeat_rich_100mbp(s).logical_text()],
            LcpEncoding.RAW32)
     yield ((1 << 32) - 1, "human-scale 3.1 Gbp" + (" (scaled x0.1)" if quick else ""),
