@@ -94,6 +94,7 @@ constexpr int kSeedBlock = 256;
 constexpr int kSeedRun = 16;
 constexpr int kSeedTile = kSeedBlock * kSeedRun;
 constexpr int kSeedHalo = 64;
+constexpr int kMaxSeedPasses = 8;  // 64-bit keys, 8-bit digits
 
 struct SeedSmem {
   u64 keys[kSeedTile];
@@ -195,7 +196,6 @@ seed_keys_kernel(const u8* __restrict__ text, u64 n, Segments segs,
   const u64 mask2 = 2 * symbols >= 64 ? ~0ull : ((1ull << (2 * symbols)) - 1);
   const u32 smask = symbols >= 32 ? ~0u : ((1u << symbols) - 1);
   const u32 local0 = threadIdx.x * kSeedRun;
-  const u32 lane = threadIdx.x & 31;
   u64 pos = tile_first + local0;
   u32 seg = segs.count == 1 ? 0 : (pos < n ? find_segment(segs.begin, segs.count, pos) : block_seg);
   u64 end = pos < n ? segs.begin[seg + 1] : n;
@@ -212,6 +212,9 @@ seed_keys_kernel(const u8* __restrict__ text, u64 n, Segments segs,
       irregular = ((irregular << 1) | (reg ? 0u : 1u)) & smask;
     }
   };
+  u32 run_digit[kMaxSeedPasses], run_len[kMaxSeedPasses];
+#pragma unroll
+  for (int p = 0; p < kMaxSeedPasses; ++p) run_digit[p] = run_len[p] = 0;
   for (int r = 0; r < kSeedRun; ++r, ++pos) {
     const bool valid = pos < n;
     if (valid && pos >= end) {  // crossed into the next instance
@@ -247,19 +250,32 @@ seed_keys_kernel(const u8* __restrict__ text, u64 n, Segments segs,
         tb.rare_pos[slot] = static_cast<u32>(pos);
       }
     }
-    // Histogram of every pass; a warp whose lanes agree adds once.
+    // Histogram of every pass.  The thread's keys are consecutive
+    // positions, so equal digits come in runs (long runs of one symbol give
+    // whole runs of equal keys): count each run in registers and add it with
+    // one shared-memory atomic when the digit changes.
     const bool mine = valid && seg == block_seg;
-    const bool all_mine = __all_sync(0xffffffffu, mine);
-    for (u32 p = 0; p < passes; ++p) {
+#pragma unroll
+    for (int p = 0; p < kMaxSeedPasses; ++p) {
+      if (p >= static_cast<int>(passes)) break;
       const u32 digit = static_cast<u32>((sort_key >> (p * 8)) & 0xff);
-      const u32 d0 = __shfl_sync(0xffffffffu, digit, 0);
-      if (all_mine && __all_sync(0xffffffffu, digit == d0)) {
-        if (lane == 0) atomicAdd(&sm.hist[p][d0], 32u);
-      } else if (mine) {
-        atomicAdd(&sm.hist[p][digit], 1u);
+      if (mine) {
+        if (run_len[p] && digit == run_digit[p]) {
+          ++run_len[p];
+        } else {
+          if (run_len[p]) atomicAdd(&sm.hist[p][run_digit[p]], run_len[p]);
+          run_digit[p] = digit;
+          run_len[p] = 1;
+        }
       } else if (valid) {
         atomicAdd(&hist_out[(static_cast<u64>(seg) * passes + p) * 256 + digit], 1u);
       }
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < kMaxSeedPasses; ++p) {
+    if (p < static_cast<int>(passes) && run_len[p]) {
+      atomicAdd(&sm.hist[p][run_digit[p]], run_len[p]);
     }
   }
   __syncthreads();
