@@ -36,7 +36,7 @@ CANDIDATES = {
     "ballot_min_elems": [1 << 23, 0, 1 << 62],
     "packed_max_bits": [24, 0],
     "two_bit_seed": [1, 0],
-    "rank_slots": [1, 0],
+    "rank_slots": [1, 0, 2],
     "graph_shrink": [4, 2, 16],
 }
 DEFAULTS = {"seed_symbols": 0, "sort_tile": 4096, "sort_block": 256,

@@ -251,9 +251,12 @@ struct Tuning {
   // symbols (rare symbols placed from a side list).
   bool two_bit_seed = true;
   u64 two_bit_min = u64(1) << 22;
-  // Seed rank write of a single instance by window slots (rank_slot_kernel)
-  // instead of radix passes grouping the pairs by window.
-  bool rank_slots = true;
+  // Seed rank write by window slots (rank_slot kernels) instead of radix
+  // passes grouping the pairs by window: 0 never, 1 batches only, 2 always.
+  // Measured on B200: slots win for batches of bacterial references (the
+  // grouping passes there run per instance) and lose for single texts of
+  // 100 Mbp and more (atomic throughput).
+  u32 rank_slots = 1;
   // Round sort tiles whose groups have at most this many rows rank by
   // counting inside each group (0: always the shared-memory radix passes).
   u32 seg_small_group = kSegSmallGroup;
@@ -316,7 +319,8 @@ std::string apply_tuning(Tuning& t, const std::string& k, int64_t value) {
     if (value < 2 || value > 1024) return "graph_shrink must be in [2, 1024]";
     t.graph_shrink = static_cast<u32>(value);
   } else if (k == "rank_slots") {
-    t.rank_slots = value != 0;
+    if (value < 0 || value > 2) return "rank_slots must be 0, 1 or 2";
+    t.rank_slots = static_cast<u32>(value);
   } else if (k == "sort_block") {
     if (value != 256 && value != 512) return "sort_block must be 256 or 512";
     t.sort_block = static_cast<u32>(value);
@@ -1054,7 +1058,7 @@ struct Engine {
     // per 8 bits of the longest instance above 11, not of the whole batch).
     const u32 pos_bits = std::max<u32>(1, bits_for(n - 1));
     u64* grouped = pairs;
-    if (segs > 1 && c.tune.rank_slots) {
+    if (segs > 1 && c.tune.rank_slots >= 1) {
       // Window slots per instance (rank_slot_segments_kernel): no grouping passes.
       std::vector<u64> wbegin(segs + 1, 0);
       for (u32 j = 0; j < segs; ++j) {
@@ -1097,7 +1101,7 @@ struct Engine {
       launch("window_scatter", n * 12, segment_window_scatter_kernel, wbegin[segs], 256, 0,
              static_cast<const u64*>(grouped), segments(), static_cast<const u64*>(L.digit_start),
              L.rank, L.flags);
-    } else if (pos_bits > kWindowBits && c.tune.rank_slots) {
+    } else if (pos_bits > kWindowBits && c.tune.rank_slots == 2) {
       const u64 windows = (n + kSlotWindow - 1) >> kSlotBits;
       u32* fill = reinterpret_cast<u32*>(L.status);  // windows words: n/8192 << status size
       u64* slotted = pairs == L.k0 ? L.k1 : L.k0;
@@ -1120,7 +1124,7 @@ struct Engine {
                                  L.sort_tiles, 1, t, n, 32 + kWindowBits, 32 + pos_bits, false);
       grouped = sw ? other_keys : pairs;
     }
-    if (segs == 1 && !(pos_bits > kWindowBits && c.tune.rank_slots)) {
+    if (segs == 1 && !(pos_bits > kWindowBits && c.tune.rank_slots == 2)) {
       launch("window_scatter", n * 12, window_scatter_kernel, (n + kWindow - 1) / kWindow, 256, 0,
              static_cast<const u64*>(grouped), n, L.rank, L.flags);
     }

@@ -187,10 +187,10 @@ def test_libdivsufsort_abi_library(ctx):
             assert (sa64 == oracle.ref_divsufsort64(t)).all()
 
 
-@pytest.mark.parametrize("slots", [0, 1])
+@pytest.mark.parametrize("slots", [0, 2])
 def test_rank_write_by_slots_or_passes(ctx, slots):
-    """The seed rank write by window slots and by radix passes give the same
-    (oracle-equal) build."""
+    """The seed rank write of a single text by window slots (rank_slots=2)
+    and by radix passes (0) give the same (oracle-equal) build."""
     t = synth.repeat_rich_100mbp(scale=0.03).logical_text()
     ctx.set_tuning("rank_slots", slots)
     try:
