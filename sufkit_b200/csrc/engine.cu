@@ -1428,8 +1428,9 @@ struct Engine {
     u32* pending = spare;
     const u64 pending_cap = n;
     zero(L.scalars + 5, 16);
-    launch("lcp_rows", n * 4 + st.active_first * 9, lcp_rows_kernel, grid_stride_blocks(n, 256),
-           256, 0, L.text, static_cast<const u32*>(sa), n, segments(), seed_length, lcp, longs,
+    launch("lcp_rows", n * 4 + st.active_first * 9, lcp_rows_kernel,
+           grid_stride_blocks((n + kLcpChunk / 32 - 1) / (kLcpChunk / 32), kLcpRowsBlock),
+           kLcpRowsBlock, 0, L.text, static_cast<const u32*>(sa), n, segments(), seed_length, lcp, longs,
            long_cap, L.scalars + 5, pending, pending_cap, L.scalars + 6, L.flags);
     SG_CUDA(cudaMemcpyAsync(c.host_scalars + 5, L.scalars + 5, 16, cudaMemcpyDeviceToHost, c.stream));
     sync();

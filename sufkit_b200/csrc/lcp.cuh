@@ -52,69 +52,118 @@ struct LongRow {
 // With known_prefix > 0, rows whose lcp[] is already set (seed-group heads,
 // resolved from the seed keys) are skipped and the others start comparing at
 // known_prefix, the seed length they are known to share.
-static __global__ void __launch_bounds__(256)
+// Each warp inspects kLcpChunk consecutive rows at a time, lists the ones that
+// still need a compare in shared memory and then gives one listed row to each
+// lane: the compare loop runs with full warps instead of idling the lanes of
+// the (usually most) rows that are already resolved.
+constexpr int kLcpChunk = 128;
+constexpr int kLcpRowsBlock = 256;
+
+// Number of leading equal bytes of text[b + m, ...) and text[a + m, ...)
+// from m up to budget (at least budget once reached; the caller clamps).
+// Reads aligned 8-byte words and carries each one into the next step, so a
+// step costs one load per side; the last word read ends at most 15 bytes
+// past position b + m (resp. a + m) < the instance end.  Sets *mismatch when
+// a differing byte was found before budget.
+__device__ __forceinline__ u32 match_length(const u8* __restrict__ text, u32 b, u32 a, u32 m,
+                                            u32 budget, bool* mismatch) {
+  *mismatch = false;
+  if (m >= budget) return m;
+  const u64 pb = static_cast<u64>(b) + m, pa = static_cast<u64>(a) + m;
+  const u32 sb = static_cast<u32>(pb & 7) * 8, sa = static_cast<u32>(pa & 7) * 8;
+  const unsigned long long* wb = reinterpret_cast<const unsigned long long*>(text + (pb & ~7ull));
+  const unsigned long long* wa = reinterpret_cast<const unsigned long long*>(text + (pa & ~7ull));
+  u64 lob = __ldg(wb), loa = __ldg(wa);
+  while (true) {
+    const u64 hib = __ldg(++wb), hia = __ldg(++wa);
+    const u64 xb = sb ? (lob >> sb) | (hib << (64 - sb)) : lob;
+    const u64 xa = sa ? (loa >> sa) | (hia << (64 - sa)) : loa;
+    const u64 x = xb ^ xa;
+    if (x) {
+      *mismatch = true;
+      return m + (static_cast<u32>(__ffsll(static_cast<long long>(x)) - 1) >> 3);
+    }
+    m += 8;
+    if (m >= budget) return m;
+    lob = hib;
+    loa = hia;
+  }
+}
+
+static __global__ void __launch_bounds__(kLcpRowsBlock)
 lcp_rows_kernel(const u8* __restrict__ text, const u32* __restrict__ sa, u64 n,
                 Segments segs, u32 known_prefix, u32* __restrict__ lcp,
                 LongRow* __restrict__ longs, u64 long_cap, u64* long_count,
                 u32* __restrict__ pending, u64 pending_cap, u64* pending_count,
                 DeviceFlags* flags) {
-  const u64 stride = static_cast<u64>(gridDim.x) * blockDim.x;
-  const u64 rows = (n + 31) / 32 * 32;  // whole warps stay converged
+  constexpr int kWarps = kLcpRowsBlock / 32;
+  __shared__ u32 listed[kWarps][kLcpChunk];
+  const u32 lane = threadIdx.x & 31;
+  const u32 warp = threadIdx.x >> 5;
+  const u32 lanemask_lt = (1u << lane) - 1;
+  const u64 chunks = (n + kLcpChunk - 1) / kLcpChunk;
+  const u64 warps_total = static_cast<u64>(gridDim.x) * kWarps;
   SegCursor cur;
-  for (u64 r = static_cast<u64>(blockIdx.x) * blockDim.x + threadIdx.x; r < rows; r += stride) {
-    bool is_long = false, irreducible = false;
-    u32 b = 0, a = 0, l = 0;
-    if (r < n && (known_prefix == 0 || lcp[r] == kLcpUnknown)) {
-      b = sa[r];
-      cur.locate(segs.begin, segs.count, r);
-      const u64 seg_first = cur.lo;
-      // A caller-supplied SA (sufgpu_lcp_noalloc) may hold entries outside
-      // the row's instance: flag them and skip the row instead of reading
-      // text past the instance end.
-      const bool b_bad = b < seg_first || b >= cur.hi;
-      const bool a_bad = r != seg_first && (sa[r - 1] < seg_first || sa[r - 1] >= cur.hi);
-      if (b_bad || a_bad) {
-        flag_error(flags, kErrBounds);
-        lcp[r] = 0;
-      } else if (r == seg_first) {
-        lcp[r] = 0;
-      } else {
-        a = sa[r - 1];
-        const u64 end = cur.hi;
-        const u64 far = a > b ? a : b;
-        const u64 limit = end - far;
-        const u64 budget = limit < known_prefix + kDirectLcpBytes ? limit : known_prefix + kDirectLcpBytes;
-        u64 m = known_prefix < limit ? known_prefix : limit;
-        bool mismatch = false;
-        while (m < budget) {
-          const u64 x = load8(text, b + m) ^ load8(text, a + m);
-          if (x) {
-            m += static_cast<u64>(__ffsll(static_cast<long long>(x)) - 1) >> 3;
-            mismatch = true;
-            break;
-          }
-          m += 8;
-        }
-        if (m > limit) m = limit;
-        if (mismatch || m >= limit) {
-          lcp[r] = static_cast<u32>(m);
+  for (u64 ch = static_cast<u64>(blockIdx.x) * kWarps + warp; ch < chunks; ch += warps_total) {
+    const u64 r0 = ch * kLcpChunk;
+    u32 count = 0;
+#pragma unroll
+    for (int k = 0; k < kLcpChunk / 32; ++k) {
+      const u64 r = r0 + k * 32 + lane;
+      const bool need = r < n && (known_prefix == 0 || lcp[r] == kLcpUnknown);
+      const u32 mask = __ballot_sync(0xffffffffu, need);
+      if (need) listed[warp][count + __popc(mask & lanemask_lt)] = k * 32 + lane;
+      count += __popc(mask);
+    }
+    __syncwarp();
+    for (u32 base = 0; base < count; base += 32) {
+      bool is_long = false, irreducible = false;
+      u32 b = 0, a = 0, l = 0;
+      u64 r = 0;
+      if (base + lane < count) {
+        r = r0 + listed[warp][base + lane];
+        b = sa[r];
+        cur.locate(segs.begin, segs.count, r);
+        const u64 seg_first = cur.lo;
+        // A caller-supplied SA (sufgpu_lcp_noalloc) may hold entries outside
+        // the row's instance: flag them and skip the row instead of reading
+        // text past the instance end.
+        const bool b_bad = b < seg_first || b >= cur.hi;
+        const bool a_bad = r != seg_first && (sa[r - 1] < seg_first || sa[r - 1] >= cur.hi);
+        if (b_bad || a_bad) {
+          flag_error(flags, kErrBounds);
+          lcp[r] = 0;
+        } else if (r == seg_first) {
+          lcp[r] = 0;
         } else {
-          is_long = true;
-          l = static_cast<u32>(m);
-          irreducible = b == seg_first || a == seg_first || text[b - 1] != text[a - 1];
+          a = sa[r - 1];
+          const u32 far = a > b ? a : b;
+          const u32 limit = static_cast<u32>(cur.hi - far);
+          const u32 budget = min(limit, known_prefix + kDirectLcpBytes);
+          bool mismatch;
+          u32 m = match_length(text, b, a, min(known_prefix, limit), budget, &mismatch);
+          if (m > limit) m = limit;
+          if (mismatch || m >= limit) {
+            lcp[r] = m;
+          } else {
+            is_long = true;
+            l = m;
+            irreducible = b == seg_first || a == seg_first || text[b - 1] != text[a - 1];
+          }
         }
       }
+      const u64 q = warp_append(long_count, is_long && irreducible);
+      if (is_long && irreducible) {
+        if (q < long_cap) longs[q] = LongRow{static_cast<u32>(r), b, a, l};
+        else flag_error(flags, kErrQueueOverflow);
+      }
+      const u64 sidx = warp_append(pending_count, is_long && !irreducible);
+      if (is_long && !irreducible) {
+        if (sidx < pending_cap) pending[sidx] = static_cast<u32>(r);
+        else flag_error(flags, kErrQueueOverflow);
+      }
     }
-    const u64 q = warp_append(long_count, is_long && irreducible);
-    if (is_long && irreducible) {
-      if (q < long_cap) longs[q] = LongRow{static_cast<u32>(r), b, a, l};
-      else flag_error(flags, kErrQueueOverflow);
-    }
-    const u64 s = warp_append(pending_count, is_long && !irreducible);
-    if (is_long && !irreducible) {
-      if (s < pending_cap) pending[s] = static_cast<u32>(r);
-      else flag_error(flags, kErrQueueOverflow);
-    }
+    __syncwarp();  // the list is rewritten for the next chunk
   }
 }
 

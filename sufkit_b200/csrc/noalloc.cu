@@ -149,7 +149,9 @@ extern "C" sufgpu_status sufgpu_lcp_noalloc(const uint8_t* text, const uint32_t*
   NA_CUDA(cudaStreamSynchronize(stream));  // seg_host lives on this stack frame
 
   const Segments segs{seg_begin, 1};
-  lcp_rows_kernel<<<static_cast<unsigned>(blocks_for(n)), 256, 0, stream>>>(
+  lcp_rows_kernel<<<static_cast<unsigned>(blocks_for((n + kLcpChunk / 32 - 1) / (kLcpChunk / 32))),
+                    kLcpRowsBlock, 0,
+                    stream>>>(
       d_text, sa, n, segs, 0, lcp, longs, kMax, scalars + 0, pending, kMax, scalars + 1, flags);
   NA_CUDA(cudaGetLastError());
   u64 counts[2] = {0, 0};

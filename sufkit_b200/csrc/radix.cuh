@@ -120,8 +120,8 @@ template <int kBlock, int kTile = kSortTile>
 struct OnesweepSmem {
   u64 keys[kTile];
   u32 vals[kTile];
+  u32 staged[kTile];  // values in tile order (asynchronous copies)
   u32 warp_hist[kBlock / 32][kRadixDigits];
-  u32 digit_excl[kRadixDigits];
   long long digit_gbase[kRadixDigits];
   u64 warp_scan[kBlock / 32];
   u64 mbar;  // completion barrier of the bulk tile load (kTma)
@@ -167,6 +167,17 @@ __device__ __forceinline__ bool mbar_wait0(u64* mbar) {
   return false;
 }
 
+// Asynchronous 4-byte copy global -> shared (no register round trip); the
+// issuing thread sees the data after cp_async_wait_all().
+// dst is a shared-memory address (__cvta_generic_to_shared).
+__device__ __forceinline__ void cp_async4(u32 dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" :: "r"(dst), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+}
+
 // kVals = false sorts keys only (vals_in/vals_out unused): the packed seed
 // carries each suffix's instance-local index in the low key bits.
 // Blocks per SM: three 256x16, four 256x8, two 512x8.  Registers are capped so
@@ -204,6 +215,17 @@ radix_onesweep_kernel(const u64* __restrict__ keys_in,
   u64 key[kItems];
   u32 rank[kItems];
   const u32 warp_base = warp * 32 * kItems;
+  // Values travel by asynchronous copies into sm.staged now, so that their
+  // latency overlaps the ranking and the look-back; each thread moves its
+  // own slots to sorted order afterwards.
+  if (kVals) {
+    const u32 dst = static_cast<u32>(__cvta_generic_to_shared(&sm.staged[warp_base + lane]));
+    const u32* src = vals_in + first + warp_base + lane;
+#pragma unroll
+    for (int i = 0; i < kItems; ++i) {
+      if (warp_base + i * 32 + lane < count) cp_async4(dst + i * 32 * 4, src + i * 32);
+    }
+  }
   u32 bulk = 0;  // keys that arrived by the bulk copy (an even count: 16-byte multiple)
   if (kTma) {
     // The bulk copy needs a 16-byte aligned source; some callers sort
@@ -262,25 +284,30 @@ radix_onesweep_kernel(const u64* __restrict__ keys_in,
   }
   __syncthreads();
 
-  // Per digit: exclusive offsets across warps, tile count, tile-local start.
+  // Per digit: tile count and tile-local start; then warp_hist[w][d] becomes
+  // the first sorted slot of warp w's keys of digit d.
   const u32 d = threadIdx.x;
   u32 digit_count = 0;
   if (d < kRadixDigits) {
 #pragma unroll
-    for (int w = 0; w < kWarps; ++w) {
-      const u32 c = sm.warp_hist[w][d];
-      sm.warp_hist[w][d] = digit_count;
-      digit_count += c;
-    }
+    for (int w = 0; w < kWarps; ++w) digit_count += sm.warp_hist[w][d];
   }
   u64 tile_total;
   const u64 local_start =
       block_exclusive_scan<kBlock>(digit_count, SumOp{}, sm.warp_scan, &tile_total);
+  if (d < kRadixDigits) {
+    u32 running = static_cast<u32>(local_start);
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+      const u32 c = sm.warp_hist[w][d];
+      sm.warp_hist[w][d] = running;
+      running += c;
+    }
+  }
 
   // Decoupled look-back, one digit per thread.  Prefix values are absolute
   // output positions; a segment's first tile seeds them from digit_start.
   if (d < kRadixDigits) {
-    sm.digit_excl[d] = static_cast<u32>(local_start);
     u64* my_status = status + static_cast<u64>(tile) * kRadixDigits + d;
     u64 global_start;
     if (first_tile_of_segment) {
@@ -306,22 +333,15 @@ radix_onesweep_kernel(const u64* __restrict__ keys_in,
   __syncthreads();
 
   // Keys and values to their tile-local sorted slot, then runs out.
-  u32 local_slot[kItems];
+  if (kVals) cp_async_wait_all();  // this thread's own staged slots
 #pragma unroll
   for (int i = 0; i < kItems; ++i) {
     const u32 slot = warp_base + i * 32 + lane;
     if (slot < count) {
       const u32 digit = static_cast<u32>((key[i] >> shift) & 0xff);
-      local_slot[i] = sm.digit_excl[digit] + sm.warp_hist[warp][digit] + rank[i];
-      sm.keys[local_slot[i]] = key[i];
-    }
-  }
-  __syncthreads();
-  if (kVals) {
-#pragma unroll
-    for (int i = 0; i < kItems; ++i) {
-      const u32 slot = warp_base + i * 32 + lane;
-      if (slot < count) sm.vals[local_slot[i]] = vals_in[first + slot];
+      const u32 local_slot = sm.warp_hist[warp][digit] + rank[i];
+      sm.keys[local_slot] = key[i];
+      if (kVals) sm.vals[local_slot] = sm.staged[slot];
     }
   }
   __syncthreads();
