@@ -200,7 +200,7 @@ struct OnesweepVariant {
 template <bool kBallot, int kBlock, int kItems, bool kVals>
 OnesweepVariant variant_of() {
   return {radix_onesweep_kernel<kBallot, kBlock, kItems, kVals>, kBlock,
-          sizeof(OnesweepSmem<kBlock, kBlock * kItems>)};
+          sizeof(OnesweepSmem<kBlock, kBlock * kItems, kVals>)};
 }
 
 template <bool kBallot, bool kVals>
@@ -212,9 +212,13 @@ OnesweepVariant variant_for(u32 block, u32 tile) {
 // Onesweep variants: ranking by ballots or match-any; 4096-key tiles (256x16,
 // 512x8) or 2048-key tiles (256x8); key-value pairs or keys only.  tma: the
 // 256x16 tile's keys by one bulk copy (single-segment sorts only).
+// Measured on B200 (one 8-bit pass over 10^9 random keys): pairs 8.7 ms as
+// 256x16 (three blocks per SM) against 9.5 ms as 512x8; keys only 7.4 ms as
+// 512x8 (three blocks) against 7.6 ms as 256x16 alone, but within 2% the
+// other way round inside whole builds, where 256x16 stays the default.
 OnesweepVariant onesweep_variant(bool ballot, u32 block, u32 tile, bool vals, bool tma = false) {
   if (tma && tile == 4096 && block == 256) {
-    const u64 smem = sizeof(OnesweepSmem<256, 4096>);
+    const u64 smem = vals ? sizeof(OnesweepSmem<256, 4096, true>) : sizeof(OnesweepSmem<256, 4096, false>);
     if (ballot) {
       return vals ? OnesweepVariant{radix_onesweep_kernel<true, 256, 16, true, true>, 256, smem}
                   : OnesweepVariant{radix_onesweep_kernel<true, 256, 16, false, true>, 256, smem};
@@ -240,11 +244,17 @@ struct Tuning {
   bool run_split = true;
   // Sort each round's groups in shared memory (segsort.cuh).
   bool seg_sort = true;
+  // With seg_sort: the shared-memory sort also writes the round's SA rows,
+  // ranks and next active list (seg_rank_kernel) instead of leaving sorted
+  // keys to round_rank.
+  bool seg_rank = false;
   // Run the rounds as captured CUDA graphs of two rounds (needs seg_sort;
   // builds with the per-kernel profile on are driven round by round).
   bool graph_rounds = true;
-  // Onesweep block size (256 threads x 16 keys or 512 x 8).
+  // Onesweep block size (256 threads x 16 keys or 512 x 8) for key-value
+  // sorts and for keys-only sorts (4096-key tiles).
   u32 sort_block = 256;
+  u32 keys_sort_block = 256;
   // Keys per onesweep tile (2048 or 4096).
   u32 sort_tile = 4096;
   // Two-bit seed keys for single DNA-like texts of at least two_bit_min
@@ -297,6 +307,8 @@ std::string apply_tuning(Tuning& t, const std::string& k, int64_t value) {
     t.sort_tile = static_cast<u32>(value);
   } else if (k == "seg_sort") {
     t.seg_sort = value != 0;
+  } else if (k == "seg_rank") {
+    t.seg_rank = value != 0;
   } else if (k == "graph_rounds") {
     t.graph_rounds = value != 0;
   } else if (k == "run_split") {
@@ -324,6 +336,9 @@ std::string apply_tuning(Tuning& t, const std::string& k, int64_t value) {
   } else if (k == "sort_block") {
     if (value != 256 && value != 512) return "sort_block must be 256 or 512";
     t.sort_block = static_cast<u32>(value);
+  } else if (k == "keys_sort_block") {
+    if (value != 256 && value != 512) return "keys_sort_block must be 256 or 512";
+    t.keys_sort_block = static_cast<u32>(value);
   } else {
     return "unknown tuning key " + k;
   }
@@ -570,9 +585,11 @@ struct Engine {
       sync();
       std::memcpy(needed, c.host_small, 4 * passes);
     } else {
-      zero(L.hist, u64(seg_count) * passes * kRadixDigits * 4);
-      launch("radix_histogram", elems * 8, radix_histogram_kernel, total_tiles, kSortBlock, 0,
-             keys, ss, begin_bit, passes, L.hist);
+      if (!hist_ready) {
+        zero(L.hist, u64(seg_count) * passes * kRadixDigits * 4);
+        launch("radix_histogram", elems * 8, radix_histogram_kernel, total_tiles, kSortBlock, 0,
+               keys, ss, begin_bit, passes, L.hist);
+      }
       launch("radix_offsets", u64(seg_count) * passes * kRadixDigits * 12, radix_offsets_kernel,
              seg_count, kRadixDigits, 0, L.hist, seg_begin, passes, L.digit_start,
              L.counters + 32);
@@ -588,7 +605,8 @@ struct Engine {
       zero(L.status, u64(total_tiles) * kRadixDigits * 8);
       zero(L.counters, 4);
       const OnesweepVariant v = onesweep_variant(c.tune.ballot_rank && elems >= c.tune.ballot_min_elems,
-                                                 c.tune.sort_block, c.tune.sort_tile, vals != nullptr,
+                                                 vals ? c.tune.sort_block : c.tune.keys_sort_block,
+                                                 c.tune.sort_tile, vals != nullptr,
                                                  c.tune.tma_tile && seg_count == 1);
       launch(name, elems * (vals ? 24 : 16), v.fn, total_tiles, v.block, v.smem,
              kin, vin, kout, vout, ss, begin_bit + p * kRadixBits, p, passes,
@@ -598,6 +616,28 @@ struct Engine {
       swapped = !swapped;
     }
     return swapped;
+  }
+
+  // Digit counts of a radix sort whose keys hold a permutation of [0, n) at
+  // key bit 32 (the rank write's (position << 32 | head) pairs): for the
+  // digit of position bits [b, b + 8), each period of 2^(b+8) positions gives
+  // every digit 2^b of them, and the remainder fills digits from 0 upwards.
+  // Written to L.hist for one segment, so the sort needs no histogram pass.
+  void upload_permutation_hist(u64 count, u32 begin_bit, u32 end_bit) {
+    const u32 passes = (end_bit - begin_bit + kRadixBits - 1) / kRadixBits;
+    std::vector<u32> h(u64(passes) * kRadixDigits);
+    for (u32 p = 0; p < passes; ++p) {
+      const u32 b = begin_bit + p * kRadixBits - 32;
+      const u64 width = u64(1) << b;
+      const u64 period = width << kRadixBits;
+      const u64 full = count / period, rem = count % period;
+      for (u32 d = 0; d < kRadixDigits; ++d) {
+        const u64 lo = u64(d) * width;
+        const u64 extra = rem > lo ? std::min<u64>(width, rem - lo) : 0;
+        h[u64(p) * kRadixDigits + d] = static_cast<u32>(full * width + extra);
+      }
+    }
+    upload(L.hist, h.data(), h.size() * 4);
   }
 
   void upload_segments(const std::vector<u64>& b) {
@@ -1120,8 +1160,10 @@ struct Engine {
       SG_CUDA(cudaMemcpyAsync(L.sort_begin, c.host_small + 4096, 16, cudaMemcpyHostToDevice, c.stream));
       SG_CUDA(cudaMemcpyAsync(L.sort_tiles, c.host_small + 4096 + 16, 8, cudaMemcpyHostToDevice, c.stream));
       u64* other_keys = pairs == L.k0 ? L.k1 : L.k0;
+      upload_permutation_hist(n, 32 + kWindowBits, 32 + pos_bits);
       const bool sw = radix_sort("rank_group", pairs, nullptr, other_keys, nullptr, L.sort_begin,
-                                 L.sort_tiles, 1, t, n, 32 + kWindowBits, 32 + pos_bits, false);
+                                 L.sort_tiles, 1, t, n, 32 + kWindowBits, 32 + pos_bits, false,
+                                 true);
       grouped = sw ? other_keys : pairs;
     }
     if (segs == 1 && !(pos_bits > kWindowBits && c.tune.rank_slots == 2)) {
@@ -1192,6 +1234,29 @@ struct Engine {
            bits_for(n), L.k1, act, L.counters + 48, abort, tag, L.flags, c.tune.seg_small_group);
   }
 
+  // Fused group sort and round step 2: (k0, other) -> SA rows, ranks and the
+  // next active list in act (*big > 0: a window did not fit; the host redoes
+  // the round).  abort: the device abort word (graph rounds) or null.
+  void round_seg_rank(const u32* other, u32* act, const RoundState& rs, u64 bound, u64* abort,
+                      u64 tag) {
+    const u64 windows = (bound + kSegWindow - 1) / kSegWindow;
+    zero(L.status, (windows + 1) * 8);
+    zero(L.counters, 4);
+    zero(L.counters + 48, 4);
+    launch("seg_rank", bound * 36, seg_rank_kernel, windows, kSegBlock, sizeof(SegRankSmem),
+           static_cast<const u64*>(L.k0), static_cast<const u32*>(other), rs,
+           static_cast<const u32*>(gstart()), static_cast<const u32*>(ghead()),
+           static_cast<const u64*>(L.scalars + 1), u64(n / 2), bits_for(n), rank_rows, sa, L.rank,
+           act, L.status, L.counters, L.counters + 48, abort, tag, L.flags, c.tune.seg_small_group);
+  }
+
+  // The round's h doubling and totals after seg_rank (graph rounds).
+  void round_close(const RoundState& rs) {
+    launch("round_close", 0, round_close_kernel, 1, 1, 0, rs);
+  }
+
+  bool fused_rounds() const { return c.tune.seg_sort && c.tune.seg_rank; }
+
   // Global passes over (id, second) bits for `active` rows: (k0, other) ->
   // (k1, act) or back in place; returns true when the result is in (k1, act).
   bool round_global_sort(u32* act, u32* other, u64 active) {
@@ -1241,6 +1306,25 @@ struct Engine {
     // Rows only move inside their groups: sort whole groups in shared memory
     // (segsort.cuh) unless some group is too large for a block, in which case
     // the round takes the global passes over (id, second) bits.
+    if (fused_rounds()) {
+      round_seg_rank(other, act, rs, active, nullptr, 0);
+      SG_CUDA(cudaMemcpyAsync(c.host_small + 8192, L.counters + 48, 4, cudaMemcpyDeviceToHost,
+                              c.stream));
+      sync();
+      u32 big = 0;
+      std::memcpy(&big, c.host_small + 8192, 4);
+      if (big == 0) return read_scalar(kCountB);  // next active list in act
+      ++st.seg_sort_fallbacks;
+      const bool sw = round_global_sort(act, other, active);
+      u64* ck = sw ? L.k1 : L.k0;
+      u32* cv = sw ? act : other;
+      u32* next = sw ? other : act;
+      round_rank(ck, cv, next, rs, active);
+      const u64 next_count = read_scalar(kCountB);
+      other = sw ? act : other;
+      act = next;
+      return next_count;
+    }
     bool sw = false;
     bool sorted = false;
     if (c.tune.seg_sort) {
@@ -1275,12 +1359,13 @@ struct Engine {
   // shared-memory sort stops the pair (abort); the host finishes that round
   // with the global passes and the graph continues from there.
   // The graph of a round pair for `bound` active rows with these buffers:
-  // from the context's cache when an earlier build had the same layout,
-  // else captured and cached.
+  // from the context's cache when an earlier build had the same layout and
+  // the same round knobs, else captured and cached.
   const sufgpu_ctx::CachedGraph& round_graph(u32* act, u32* other, u64 bound) {
     const std::vector<u64> key = {reinterpret_cast<u64>(c.arena.base), n, segs, bound,
                                   reinterpret_cast<u64>(act), reinterpret_cast<u64>(other),
-                                  run_count, reinterpret_cast<u64>(L.seg_begin)};
+                                  run_count, reinterpret_cast<u64>(L.seg_begin),
+                                  u64(fused_rounds()), u64(c.tune.seg_small_group)};
     auto& cache = c.round_graphs;
     for (size_t i = 0; i < cache.size(); ++i) {
       if (cache[i].key == key) {
@@ -1295,9 +1380,15 @@ struct Engine {
       for (int r = 0; r < 2; ++r) {
         const RoundState rs = round_state(r == 0 ? kCountA : kCountB, true);
         round_keys(act, other, rs, bound, nullptr, segments());
-        round_seg_sort(other, act, rs, bound, L.scalars + kAbort, r + 1);
-        round_rank(L.k1, act, other, rs, bound);
-        std::swap(act, other);
+        if (fused_rounds()) {
+          // The next active list replaces act: no buffer swap.
+          round_seg_rank(other, act, rs, bound, L.scalars + kAbort, r + 1);
+          round_close(rs);
+        } else {
+          round_seg_sort(other, act, rs, bound, L.scalars + kAbort, r + 1);
+          round_rank(L.k1, act, other, rs, bound);
+          std::swap(act, other);
+        }
       }
     } catch (...) {
       cudaStreamEndCapture(c.stream, &graph);
@@ -1342,7 +1433,8 @@ struct Engine {
         // are complete.  Its active count is in A (first round) or B.
         ++st.seg_sort_fallbacks;
         const int in = abort == 1 ? kCountA : kCountB;
-        if (abort == 2) std::swap(act, other);
+        // Unfused pairs swap the buffers once per round; fused ones never.
+        if (abort == 2 && !fused_rounds()) std::swap(act, other);
         const u64 count = c.host_scalars[in];
         fallback_rows += count;
         ++fallback_rounds;
@@ -1966,6 +2058,8 @@ sufgpu_status sufgpu_create(sufgpu_ctx** out, int device) {
     for (auto& ev : ctx->ev) SG_CUDA(cudaEventCreate(&ev));
     SG_CUDA(cudaFuncSetAttribute(seg_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(sizeof(SegSortSmem))));
+    SG_CUDA(cudaFuncSetAttribute(seg_rank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(sizeof(SegRankSmem))));
     SG_CUDA(cudaFuncSetAttribute(seed_sorted_kernel<true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(sizeof(SeedSortSmem))));

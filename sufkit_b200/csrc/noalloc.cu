@@ -87,7 +87,7 @@ cudaError_t scratch_for_current_device(unsigned char** out) {
     if (err != cudaSuccess) return err;
     err = cudaFuncSetAttribute(radix_onesweep_kernel<true, kSortBlock, kSortItems>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(sizeof(OnesweepSmem<kSortBlock, kSortTile>)));
+                               static_cast<int>(sizeof(OnesweepSmem<kSortBlock, kSortTile, true>)));
     if (err != cudaSuccess) return err;
     g_scratch_ptr[device] = static_cast<unsigned char*>(ptr);
   }
@@ -190,7 +190,7 @@ extern "C" sufgpu_status sufgpu_lcp_noalloc(const uint8_t* text, const uint32_t*
       NA_CUDA(cudaMemsetAsync(status, 0, u64(tiles) * kRadixDigits * 8, stream));
       NA_CUDA(cudaMemsetAsync(counters, 0, 4, stream));
       radix_onesweep_kernel<true, kSortBlock, kSortItems>
-          <<<tiles, kSortBlock, sizeof(OnesweepSmem<kSortBlock, kSortTile>), stream>>>(
+          <<<tiles, kSortBlock, sizeof(OnesweepSmem<kSortBlock, kSortTile, true>), stream>>>(
           kin, vin, kout, vout, ss, p * kRadixBits, p, passes, digits, status, counters, flags);
       NA_CUDA(cudaGetLastError());
       u64* tk = kin; kin = kout; kout = tk;

@@ -115,18 +115,21 @@ radix_offsets_kernel(const u32* __restrict__ hist, const u64* __restrict__ begin
 
 // One LSD pass over bits [shift, shift+8), for a tile of kSortTile pairs
 // handled by kBlock threads x kItems items.  Shared memory holds the tile's
-// keys and values in sorted-slot order and per-warp digit counters.
-template <int kBlock, int kTile = kSortTile>
+// keys and values (kVals) in sorted-slot order and per-warp digit counters.
+// The counters are 16-bit (a warp ranks at most 32 x kItems <= 512 keys, and
+// a tile-local slot is below 4096), which keeps a 4096-pair tile at 56 KB: three
+// blocks per SM instead of two.
+template <int kBlock, int kTile = kSortTile, bool kVals = true>
 struct OnesweepSmem {
   u64 keys[kTile];
-  u32 vals[kTile];
-  u32 staged[kTile];  // values in tile order (asynchronous copies)
-  u32 warp_hist[kBlock / 32][kRadixDigits];
+  u32 vals[kVals ? kTile : 1];
+  unsigned short warp_hist[kBlock / 32][kRadixDigits];
   long long digit_gbase[kRadixDigits];
   u64 warp_scan[kBlock / 32];
   u64 mbar;  // completion barrier of the bulk tile load (kTma)
   u32 tile;
 };
+static_assert(kSortTile <= 65535, "16-bit tile-local slots");
 
 // Bulk (TMA engine) copy of `bytes` contiguous bytes from this GPU's global
 // memory into the CTA's shared memory, completing on an mbarrier: one
@@ -167,26 +170,15 @@ __device__ __forceinline__ bool mbar_wait0(u64* mbar) {
   return false;
 }
 
-// Asynchronous 4-byte copy global -> shared (no register round trip); the
-// issuing thread sees the data after cp_async_wait_all().
-// dst is a shared-memory address (__cvta_generic_to_shared).
-__device__ __forceinline__ void cp_async4(u32 dst, const void* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" :: "r"(dst), "l"(src) : "memory");
-}
-
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
-}
-
 // kVals = false sorts keys only (vals_in/vals_out unused): the packed seed
 // carries each suffix's instance-local index in the low key bits.
-// Blocks per SM: three 256x16, four 256x8, two 512x8.  Registers are capped so
-// that occupancy, not the allocator, decides.
+// Blocks per SM: three 256x16, four 256x8, two 512x8 (three without values).
+// Registers are capped so that occupancy, not the allocator, decides.
 // kTma: the tile's keys arrive by one bulk copy into shared memory (single-
 // segment sorts, whose tiles start on 4096-key boundaries) instead of
 // per-thread loads; the rest is the same.
 template <bool kBallot, int kBlock, int kItems, bool kVals = true, bool kTma = false>
-static __global__ void __launch_bounds__(kBlock, kBlock == 512 ? 2 : (kItems <= 8 ? 4 : 3))
+static __global__ void __launch_bounds__(kBlock, kBlock == 512 ? (kVals ? 2 : 3) : (kItems <= 8 ? 4 : 3))
 radix_onesweep_kernel(const u64* __restrict__ keys_in,
                       const u32* __restrict__ vals_in,
                       u64* __restrict__ keys_out, u32* __restrict__ vals_out,
@@ -195,8 +187,8 @@ radix_onesweep_kernel(const u64* __restrict__ keys_in,
                       u32* tile_counter, DeviceFlags* flags) {
   static_assert(kBlock >= kRadixDigits, "one thread per digit");
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  OnesweepSmem<kBlock, kBlock * kItems>& sm =
-      *reinterpret_cast<OnesweepSmem<kBlock, kBlock * kItems>*>(smem_raw);
+  OnesweepSmem<kBlock, kBlock * kItems, kVals>& sm =
+      *reinterpret_cast<OnesweepSmem<kBlock, kBlock * kItems, kVals>*>(smem_raw);
   constexpr int kWarps = kBlock / 32;
   const u32 lane = threadIdx.x & 31;
   const u32 warp = threadIdx.x >> 5;
@@ -215,17 +207,6 @@ radix_onesweep_kernel(const u64* __restrict__ keys_in,
   u64 key[kItems];
   u32 rank[kItems];
   const u32 warp_base = warp * 32 * kItems;
-  // Values travel by asynchronous copies into sm.staged now, so that their
-  // latency overlaps the ranking and the look-back; each thread moves its
-  // own slots to sorted order afterwards.
-  if (kVals) {
-    const u32 dst = static_cast<u32>(__cvta_generic_to_shared(&sm.staged[warp_base + lane]));
-    const u32* src = vals_in + first + warp_base + lane;
-#pragma unroll
-    for (int i = 0; i < kItems; ++i) {
-      if (warp_base + i * 32 + lane < count) cp_async4(dst + i * 32 * 4, src + i * 32);
-    }
-  }
   u32 bulk = 0;  // keys that arrived by the bulk copy (an even count: 16-byte multiple)
   if (kTma) {
     // The bulk copy needs a 16-byte aligned source; some callers sort
@@ -276,7 +257,7 @@ radix_onesweep_kernel(const u64* __restrict__ keys_in,
     u32 base = 0;
     if (valid && lane == leader) {
       base = sm.warp_hist[warp][digit];
-      sm.warp_hist[warp][digit] = base + __popc(peers);
+      sm.warp_hist[warp][digit] = static_cast<unsigned short>(base + __popc(peers));
     }
     base = __shfl_sync(0xffffffffu, base, leader);
     rank[i] = base + __popc(peers & lanemask_lt);
@@ -300,7 +281,7 @@ radix_onesweep_kernel(const u64* __restrict__ keys_in,
 #pragma unroll
     for (int w = 0; w < kWarps; ++w) {
       const u32 c = sm.warp_hist[w][d];
-      sm.warp_hist[w][d] = running;
+      sm.warp_hist[w][d] = static_cast<unsigned short>(running);
       running += c;
     }
   }
@@ -333,7 +314,6 @@ radix_onesweep_kernel(const u64* __restrict__ keys_in,
   __syncthreads();
 
   // Keys and values to their tile-local sorted slot, then runs out.
-  if (kVals) cp_async_wait_all();  // this thread's own staged slots
 #pragma unroll
   for (int i = 0; i < kItems; ++i) {
     const u32 slot = warp_base + i * 32 + lane;
@@ -341,7 +321,7 @@ radix_onesweep_kernel(const u64* __restrict__ keys_in,
       const u32 digit = static_cast<u32>((key[i] >> shift) & 0xff);
       const u32 local_slot = sm.warp_hist[warp][digit] + rank[i];
       sm.keys[local_slot] = key[i];
-      if (kVals) sm.vals[local_slot] = sm.staged[slot];
+      if (kVals) sm.vals[local_slot] = vals_in[first + slot];
     }
   }
   __syncthreads();

@@ -199,6 +199,22 @@ def test_rank_write_by_slots_or_passes(ctx, slots):
         ctx.set_tuning("rank_slots", 1)
 
 
+@pytest.mark.parametrize("shape", [("sort_block", 256, 512), ("keys_sort_block", 256, 512),
+                                   ("sort_tile", 4096, 2048)])
+def test_onesweep_tile_shapes(ctx, shape):
+    """Onesweep passes of 256 x 16, 512 x 8 and 256 x 8 keys per block, for
+    key-value sorts (unpacked seed) and keys-only sorts (packed seed, rank
+    grouping): the same (oracle-equal) build."""
+    knob, default, other = shape
+    ctx.set_tuning(knob, other)
+    try:
+        for t in (synth.repeat_rich_100mbp(scale=0.03).logical_text(),   # unpacked seed
+                  synth.plain_4mbp(scale=0.5).logical_text()):          # packed seed
+            check_full(ctx, t, isa_bits=32, lcp=sg.LcpEncoding.RAW32)
+    finally:
+        ctx.set_tuning(knob, default)
+
+
 @pytest.mark.parametrize("fused", [0, 1])
 @pytest.mark.parametrize("two_bit", [0, 1])
 def test_seed_first_pass_fused_or_separate(ctx, fused, two_bit):

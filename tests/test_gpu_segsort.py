@@ -1,6 +1,8 @@
 """GPU: doubling rounds sort their groups in shared memory; rounds with a group
 too large for one block take the global passes.  Both give the oracle's
-output word for word, and the two strategies agree with each other."""
+output word for word, and the two strategies agree with each other.  Every
+test runs with the round's second step fused into the shared-memory sort
+(seg_rank) and as the separate round_rank pass over sorted keys."""
 import numpy as np
 import pytest
 
@@ -16,6 +18,13 @@ def expected(text):
         sa, isa, lcp, _ = oracle.ref_adapter(text, 64)
         return sa, isa, lcp
     return oracle.full_build(text)
+
+
+@pytest.fixture(autouse=True, params=[1, 0], ids=["seg_rank", "seg_sort+round_rank"])
+def round_step2(request, ctx):
+    ctx.set_tuning("seg_rank", request.param)
+    yield request.param
+    ctx.set_tuning("seg_rank", 1)
 
 
 def build(ctx, text, seg_sort=1):
