@@ -30,7 +30,7 @@ from . import synth
 
 # Candidate values per knob (0 for seed_symbols = choose from size/entropy).
 CANDIDATES = {
-    "seed_symbols": [0, 16, 18, 21],
+    "seed_symbols": [0, 15, 16, 18, 19, 21],
     "sort_tile": [4096, 2048],
     "sort_block": [256, 512],
     "ballot_min_elems": [1 << 23, 0, 1 << 62],
@@ -38,10 +38,12 @@ CANDIDATES = {
     "two_bit_seed": [1, 0],
     "rank_slots": [1, 0, 2],
     "graph_shrink": [4, 2, 16],
+    "keys_sort_block": [256, 512],
+    "seg_rank": [0, 1],
 }
 DEFAULTS = {"seed_symbols": 0, "sort_tile": 4096, "sort_block": 256,
             "ballot_min_elems": 1 << 23, "packed_max_bits": 24, "two_bit_seed": 1,
-            "rank_slots": 1, "graph_shrink": 4}
+            "rank_slots": 1, "graph_shrink": 4, "keys_sort_block": 256, "seg_rank": 0}
 
 
 def workloads(quick: bool):
