@@ -13,6 +13,8 @@
 // still-unsorted positions are ever touched after the seed.
 #pragma once
 
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 #include "scan.cuh"
 
@@ -616,6 +618,49 @@ window_scatter_kernel(const u64* __restrict__ pairs, u64 n, u32* __restrict__ ra
   }
   __syncthreads();
   for (u32 i = threadIdx.x; i < count; i += 256) rank[first + i] = window[i];
+}
+
+// rank[pos] = head for pairs grouped by windows of 2^16 positions (one
+// grouping pass fewer than 2048-position windows for texts of 2^28 to 2^32
+// symbols, and of 2^17 to 2^24), written through a cluster of two blocks:
+// each block holds half the window (2^15 words, 128 KB of shared memory),
+// reads half the window's pairs and stores each head into the owning
+// block's shared memory (distributed shared memory), then writes its half
+// out coalesced.
+constexpr u32 kClusterWindowBits = 16;
+constexpr u32 kClusterSliceBits = kClusterWindowBits - 1;
+constexpr u32 kClusterSlice = 1u << kClusterSliceBits;
+constexpr u32 kClusterBlock = 1024;
+
+static __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kClusterBlock, 1)
+cluster_window_scatter_kernel(const u64* __restrict__ pairs, u64 n, u32* __restrict__ rank,
+                              DeviceFlags* flags) {
+  extern __shared__ u32 slice[];
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  const u32 me = cluster.block_rank();
+  const u64 w = blockIdx.x >> 1;
+  const u64 first = w << kClusterWindowBits;
+  const u64 count = n - first < (1ull << kClusterWindowBits) ? n - first
+                                                               : (1ull << kClusterWindowBits);
+  cluster.sync();  // both blocks' shared memory is live before remote stores
+  const u64 lo = static_cast<u64>(me) * kClusterSlice;
+  const u64 hi = lo + kClusterSlice < count ? lo + kClusterSlice : count;
+  u32* const half0 = cluster.map_shared_rank(slice, 0);
+  u32* const half1 = cluster.map_shared_rank(slice, 1);
+  for (u64 i = lo + threadIdx.x; i < hi; i += kClusterBlock) {
+    const u64 v = pairs[first + i];
+    const u64 pos = v >> 32;
+    const u64 local = pos - first;
+    if ((pos >> kClusterWindowBits) != w || local >= count) {
+      flag_error(flags, kErrBounds);  // not a permutation
+      continue;
+    }
+    u32* const half = (local >> kClusterSliceBits) ? half1 : half0;
+    half[local & (kClusterSlice - 1)] = static_cast<u32>(v);
+  }
+  cluster.sync();
+  for (u64 i = lo + threadIdx.x; i < hi; i += kClusterBlock) rank[first + i] = slice[i - lo];
 }
 
 // Rank write by window slots (one instance).  Each (position << 32 | head)

@@ -248,6 +248,10 @@ struct Tuning {
   // ranks and next active list (seg_rank_kernel) instead of leaving sorted
   // keys to round_rank.
   bool seg_rank = false;
+  // Rank write of one instance through 2^16-position windows held by a
+  // cluster of two blocks (cluster_window_scatter_kernel) when that saves a
+  // grouping pass over 2048-position windows.
+  bool rank_cluster = true;
   // Run the rounds as captured CUDA graphs of two rounds (needs seg_sort;
   // builds with the per-kernel profile on are driven round by round).
   bool graph_rounds = true;
@@ -309,6 +313,8 @@ std::string apply_tuning(Tuning& t, const std::string& k, int64_t value) {
     t.seg_sort = value != 0;
   } else if (k == "seg_rank") {
     t.seg_rank = value != 0;
+  } else if (k == "rank_cluster") {
+    t.rank_cluster = value != 0;
   } else if (k == "graph_rounds") {
     t.graph_rounds = value != 0;
   } else if (k == "run_split") {
@@ -1098,6 +1104,12 @@ struct Engine {
     // per 8 bits of the longest instance above 11, not of the whole batch).
     const u32 pos_bits = std::max<u32>(1, bits_for(n - 1));
     u64* grouped = pairs;
+    // Windows of 2^16 positions (a cluster of two blocks) when they take
+    // fewer grouping passes than 2048-position windows.
+    auto group_passes = [&](u32 w) { return pos_bits > w ? (pos_bits - w + 7) / 8 : 0u; };
+    const bool cluster_window = segs == 1 && c.tune.rank_cluster && c.tune.rank_slots != 2 &&
+                                group_passes(kClusterWindowBits) < group_passes(kWindowBits);
+    const u32 window_bits = cluster_window ? kClusterWindowBits : kWindowBits;
     if (segs > 1 && c.tune.rank_slots >= 1) {
       // Window slots per instance (rank_slot_segments_kernel): no grouping passes.
       std::vector<u64> wbegin(segs + 1, 0);
@@ -1150,7 +1162,7 @@ struct Engine {
              static_cast<const u64*>(pairs), n, fill, slotted, L.flags);
       launch("window_scatter", n * 12, slot_window_scatter_kernel, windows, 256,
              kSlotWindow * 4, static_cast<const u64*>(slotted), n, L.rank, L.flags);
-    } else if (pos_bits > kWindowBits) {
+    } else if (pos_bits > window_bits) {
       const u64 b2[2] = {0, n};
       const u32 t = static_cast<u32>((n + c.tune.sort_tile - 1) / c.tune.sort_tile);
       const u32 t2[2] = {0, t};
@@ -1160,13 +1172,17 @@ struct Engine {
       SG_CUDA(cudaMemcpyAsync(L.sort_begin, c.host_small + 4096, 16, cudaMemcpyHostToDevice, c.stream));
       SG_CUDA(cudaMemcpyAsync(L.sort_tiles, c.host_small + 4096 + 16, 8, cudaMemcpyHostToDevice, c.stream));
       u64* other_keys = pairs == L.k0 ? L.k1 : L.k0;
-      upload_permutation_hist(n, 32 + kWindowBits, 32 + pos_bits);
+      upload_permutation_hist(n, 32 + window_bits, 32 + pos_bits);
       const bool sw = radix_sort("rank_group", pairs, nullptr, other_keys, nullptr, L.sort_begin,
-                                 L.sort_tiles, 1, t, n, 32 + kWindowBits, 32 + pos_bits, false,
+                                 L.sort_tiles, 1, t, n, 32 + window_bits, 32 + pos_bits, false,
                                  true);
       grouped = sw ? other_keys : pairs;
     }
-    if (segs == 1 && !(pos_bits > kWindowBits && c.tune.rank_slots == 2)) {
+    if (cluster_window) {
+      const u64 windows = (n + (u64(1) << kClusterWindowBits) - 1) >> kClusterWindowBits;
+      launch("window_scatter", n * 12, cluster_window_scatter_kernel, windows * 2, kClusterBlock,
+             kClusterSlice * 4, static_cast<const u64*>(grouped), n, L.rank, L.flags);
+    } else if (segs == 1 && !(pos_bits > kWindowBits && c.tune.rank_slots == 2)) {
       launch("window_scatter", n * 12, window_scatter_kernel, (n + kWindow - 1) / kWindow, 256, 0,
              static_cast<const u64*>(grouped), n, L.rank, L.flags);
     }
@@ -2060,6 +2076,9 @@ sufgpu_status sufgpu_create(sufgpu_ctx** out, int device) {
                                  static_cast<int>(sizeof(SegSortSmem))));
     SG_CUDA(cudaFuncSetAttribute(seg_rank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(sizeof(SegRankSmem))));
+    SG_CUDA(cudaFuncSetAttribute(cluster_window_scatter_kernel,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(kClusterSlice * 4)));
     SG_CUDA(cudaFuncSetAttribute(seed_sorted_kernel<true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(sizeof(SeedSortSmem))));

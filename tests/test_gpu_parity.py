@@ -215,6 +215,23 @@ def test_onesweep_tile_shapes(ctx, shape):
         ctx.set_tuning(knob, default)
 
 
+@pytest.mark.parametrize("cluster", [0, 1])
+def test_rank_write_cluster_windows(ctx, cluster):
+    """The single-text rank write through 65536-position windows held by a
+    two-block cluster (one grouping pass for 22 position bits, none for 16)
+    or through 2048-position windows (two passes, one): the same
+    (oracle-equal) build."""
+    rng = np.random.default_rng(16)
+    ctx.set_tuning("rank_cluster", cluster)
+    try:
+        for t in (synth.repeat_rich_100mbp(scale=0.03).logical_text(),   # 3 Mbp: 22 bits
+                  synth.random_text(rng, 60_000, 4),                     # 16 bits
+                  synth.random_text(rng, 65_536, 4)):                    # one full window
+            check_full(ctx, t, isa_bits=32, lcp=sg.LcpEncoding.RAW32)
+    finally:
+        ctx.set_tuning("rank_cluster", 1)
+
+
 @pytest.mark.parametrize("fused", [0, 1])
 @pytest.mark.parametrize("two_bit", [0, 1])
 def test_seed_first_pass_fused_or_separate(ctx, fused, two_bit):
