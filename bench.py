@@ -253,7 +253,7 @@ def text_statistics_device(d_lcp, torch, seed: int = 21, chunk: int = 1 << 28):
 
 def load_traffic(kernel: str):
     """DRAM bytes per algorithmic byte of `kernel`, from the committed ncu
-    summary (profiles/traffic.json, measured on a 30 Mbp capture and scaled
+    summary (profiles/traffic.json, measured on a 31 Mbp capture and scaled
     to a full launch by its algorithmic bytes), or None."""
     path = ROOT / "profiles" / "traffic.json"
     if not path.exists():
