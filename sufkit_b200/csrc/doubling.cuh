@@ -622,33 +622,37 @@ window_scatter_kernel(const u64* __restrict__ pairs, u64 n, u32* __restrict__ ra
 
 // rank[pos] = head for pairs grouped by windows of 2^16 positions (one
 // grouping pass fewer than 2048-position windows for texts of 2^28 to 2^32
-// symbols, and of 2^17 to 2^24), written through a cluster of two blocks:
-// each block holds half the window (2^15 words, 128 KB of shared memory),
-// reads half the window's pairs and stores each head into the owning
-// block's shared memory (distributed shared memory), then writes its half
-// out coalesced.
+// symbols, and of 2^17 to 2^24), written through a cluster of kCtas blocks:
+// each block holds its share of the window (2^16 / kCtas words: 128 KB for
+// two blocks, 64 KB for four, so that two clusters share an SM), reads its
+// share of the window's pairs and stores each head into the owning block's
+// shared memory (distributed shared memory), then writes its share out
+// coalesced.
 constexpr u32 kClusterWindowBits = 16;
-constexpr u32 kClusterSliceBits = kClusterWindowBits - 1;
-constexpr u32 kClusterSlice = 1u << kClusterSliceBits;
-constexpr u32 kClusterBlock = 1024;
 
-static __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kClusterBlock, 1)
-cluster_window_scatter_kernel(const u64* __restrict__ pairs, u64 n, u32* __restrict__ rank,
-                              DeviceFlags* flags) {
-  extern __shared__ u32 slice[];
+template <int kCtas>
+struct ClusterWindow {
+  static constexpr u32 kSliceBits = kClusterWindowBits - (kCtas == 4 ? 2 : 1);
+  static constexpr u32 kSlice = 1u << kSliceBits;
+  static constexpr u32 kBlock = kCtas == 4 ? 512 : 1024;
+};
+
+template <int kCtas>
+__device__ __forceinline__ void cluster_window_scatter(const u64* __restrict__ pairs, u64 n,
+                                                       u32* __restrict__ rank,
+                                                       DeviceFlags* flags, u32* slice) {
+  using W = ClusterWindow<kCtas>;
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
   const u32 me = cluster.block_rank();
-  const u64 w = blockIdx.x >> 1;
+  const u64 w = blockIdx.x / kCtas;
   const u64 first = w << kClusterWindowBits;
   const u64 count = n - first < (1ull << kClusterWindowBits) ? n - first
                                                                : (1ull << kClusterWindowBits);
-  cluster.sync();  // both blocks' shared memory is live before remote stores
-  const u64 lo = static_cast<u64>(me) * kClusterSlice;
-  const u64 hi = lo + kClusterSlice < count ? lo + kClusterSlice : count;
-  u32* const half0 = cluster.map_shared_rank(slice, 0);
-  u32* const half1 = cluster.map_shared_rank(slice, 1);
-  for (u64 i = lo + threadIdx.x; i < hi; i += kClusterBlock) {
+  cluster.sync();  // every block's shared memory is live before remote stores
+  const u64 lo = static_cast<u64>(me) * W::kSlice;
+  const u64 hi = lo + W::kSlice < count ? lo + W::kSlice : count;
+  for (u64 i = lo + threadIdx.x; i < hi; i += W::kBlock) {
     const u64 v = pairs[first + i];
     const u64 pos = v >> 32;
     const u64 local = pos - first;
@@ -656,11 +660,25 @@ cluster_window_scatter_kernel(const u64* __restrict__ pairs, u64 n, u32* __restr
       flag_error(flags, kErrBounds);  // not a permutation
       continue;
     }
-    u32* const half = (local >> kClusterSliceBits) ? half1 : half0;
-    half[local & (kClusterSlice - 1)] = static_cast<u32>(v);
+    u32* const owner = cluster.map_shared_rank(slice, static_cast<u32>(local >> W::kSliceBits));
+    owner[local & (W::kSlice - 1)] = static_cast<u32>(v);
   }
   cluster.sync();
-  for (u64 i = lo + threadIdx.x; i < hi; i += kClusterBlock) rank[first + i] = slice[i - lo];
+  for (u64 i = lo + threadIdx.x; i < hi; i += W::kBlock) rank[first + i] = slice[i - lo];
+}
+
+static __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(1024, 1)
+cluster_window_scatter_kernel(const u64* __restrict__ pairs, u64 n, u32* __restrict__ rank,
+                              DeviceFlags* flags) {
+  extern __shared__ u32 slice[];
+  cluster_window_scatter<2>(pairs, n, rank, flags, slice);
+}
+
+static __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(512, 2)
+cluster4_window_scatter_kernel(const u64* __restrict__ pairs, u64 n, u32* __restrict__ rank,
+                               DeviceFlags* flags) {
+  extern __shared__ u32 slice[];
+  cluster_window_scatter<4>(pairs, n, rank, flags, slice);
 }
 
 // Rank write by window slots (one instance).  Each (position << 32 | head)

@@ -249,9 +249,13 @@ struct Tuning {
   // keys to round_rank.
   bool seg_rank = false;
   // Rank write of one instance through 2^16-position windows held by a
-  // cluster of two blocks (cluster_window_scatter_kernel) when that saves a
-  // grouping pass over 2048-position windows.
-  bool rank_cluster = true;
+  // cluster of 2 or 4 blocks (cluster_window_scatter_kernel,
+  // cluster4_window_scatter_kernel) when that saves a grouping pass over
+  // 2048-position windows; 0: never.
+  u32 rank_cluster = 2;
+  // Round sort blocks per SM the kernel's registers are capped for (2 or 3;
+  // measured at 3.1 Gbp: 33.3 ms at three against 37.5 ms at two).
+  u32 seg_blocks = 3;
   // Run the rounds as captured CUDA graphs of two rounds (needs seg_sort;
   // builds with the per-kernel profile on are driven round by round).
   bool graph_rounds = true;
@@ -314,7 +318,11 @@ std::string apply_tuning(Tuning& t, const std::string& k, int64_t value) {
   } else if (k == "seg_rank") {
     t.seg_rank = value != 0;
   } else if (k == "rank_cluster") {
-    t.rank_cluster = value != 0;
+    if (value != 0 && value != 2 && value != 4) return "rank_cluster must be 0, 2 or 4";
+    t.rank_cluster = static_cast<u32>(value);
+  } else if (k == "seg_blocks") {
+    if (value != 2 && value != 3) return "seg_blocks must be 2 or 3";
+    t.seg_blocks = static_cast<u32>(value);
   } else if (k == "graph_rounds") {
     t.graph_rounds = value != 0;
   } else if (k == "run_split") {
@@ -1180,8 +1188,15 @@ struct Engine {
     }
     if (cluster_window) {
       const u64 windows = (n + (u64(1) << kClusterWindowBits) - 1) >> kClusterWindowBits;
-      launch("window_scatter", n * 12, cluster_window_scatter_kernel, windows * 2, kClusterBlock,
-             kClusterSlice * 4, static_cast<const u64*>(grouped), n, L.rank, L.flags);
+      if (c.tune.rank_cluster == 4) {
+        launch("window_scatter", n * 12, cluster4_window_scatter_kernel, windows * 4,
+               ClusterWindow<4>::kBlock, ClusterWindow<4>::kSlice * 4,
+               static_cast<const u64*>(grouped), n, L.rank, L.flags);
+      } else {
+        launch("window_scatter", n * 12, cluster_window_scatter_kernel, windows * 2,
+               ClusterWindow<2>::kBlock, ClusterWindow<2>::kSlice * 4,
+               static_cast<const u64*>(grouped), n, L.rank, L.flags);
+      }
     } else if (segs == 1 && !(pos_bits > kWindowBits && c.tune.rank_slots == 2)) {
       launch("window_scatter", n * 12, window_scatter_kernel, (n + kWindow - 1) / kWindow, 256, 0,
              static_cast<const u64*>(grouped), n, L.rank, L.flags);
@@ -1244,7 +1259,8 @@ struct Engine {
   void round_seg_sort(const u32* other, u32* act, const RoundState& rs, u64 bound, u64* abort,
                       u64 tag) {
     zero(L.counters + 48, 4);
-    launch("seg_sort", bound * 24, seg_sort_kernel, (bound + kSegWindow - 1) / kSegWindow,
+    launch("seg_sort", bound * 24, c.tune.seg_blocks == 3 ? seg_sort_kernel<3> : seg_sort_kernel<2>,
+           (bound + kSegWindow - 1) / kSegWindow,
            kSegBlock, sizeof(SegSortSmem), static_cast<const u64*>(L.k0), other, rs.count,
            static_cast<const u32*>(gstart()), static_cast<const u64*>(L.scalars + 1),
            bits_for(n), L.k1, act, L.counters + 48, abort, tag, L.flags, c.tune.seg_small_group);
@@ -1381,7 +1397,8 @@ struct Engine {
     const std::vector<u64> key = {reinterpret_cast<u64>(c.arena.base), n, segs, bound,
                                   reinterpret_cast<u64>(act), reinterpret_cast<u64>(other),
                                   run_count, reinterpret_cast<u64>(L.seg_begin),
-                                  u64(fused_rounds()), u64(c.tune.seg_small_group)};
+                                  u64(fused_rounds()), u64(c.tune.seg_small_group),
+                                  u64(c.tune.seg_blocks)};
     auto& cache = c.round_graphs;
     for (size_t i = 0; i < cache.size(); ++i) {
       if (cache[i].key == key) {
@@ -2072,13 +2089,18 @@ sufgpu_status sufgpu_create(sufgpu_ctx** out, int device) {
     SG_CUDA(cudaMallocHost(reinterpret_cast<void**>(&ctx->host_scalars), 64 * 8));
     SG_CUDA(cudaMallocHost(reinterpret_cast<void**>(&ctx->host_small), 1u << 20));
     for (auto& ev : ctx->ev) SG_CUDA(cudaEventCreate(&ev));
-    SG_CUDA(cudaFuncSetAttribute(seg_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    SG_CUDA(cudaFuncSetAttribute(seg_sort_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(sizeof(SegSortSmem))));
+    SG_CUDA(cudaFuncSetAttribute(seg_sort_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(sizeof(SegSortSmem))));
     SG_CUDA(cudaFuncSetAttribute(seg_rank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(sizeof(SegRankSmem))));
     SG_CUDA(cudaFuncSetAttribute(cluster_window_scatter_kernel,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(kClusterSlice * 4)));
+                                 static_cast<int>(ClusterWindow<2>::kSlice * 4)));
+    SG_CUDA(cudaFuncSetAttribute(cluster4_window_scatter_kernel,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(ClusterWindow<4>::kSlice * 4)));
     SG_CUDA(cudaFuncSetAttribute(seed_sorted_kernel<true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(sizeof(SeedSortSmem))));

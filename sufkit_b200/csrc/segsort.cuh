@@ -145,7 +145,10 @@ __device__ __forceinline__ u32 segsort_radix_passes(SegSortSmem& sm, u32 n_rows,
 // count_ptr: the round's active rows (the grid covers an upper bound).  With
 // abort set, a window too large for a block also writes abort_tag there so
 // that the rest of a host-free round sequence stands still.
-static __global__ void __launch_bounds__(kSegBlock, 2)
+// kMinBlocks: blocks per SM the register budget is capped for (the tile's
+// 75 KB of shared memory fits three).
+template <int kMinBlocks>
+static __global__ void __launch_bounds__(kSegBlock, kMinBlocks)
 seg_sort_kernel(const u64* __restrict__ ckey, const u32* __restrict__ cval,
                 const u64* __restrict__ count_ptr,
                 const u32* __restrict__ gstart, const u64* __restrict__ group_count,

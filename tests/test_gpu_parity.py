@@ -215,11 +215,11 @@ def test_onesweep_tile_shapes(ctx, shape):
         ctx.set_tuning(knob, default)
 
 
-@pytest.mark.parametrize("cluster", [0, 1])
+@pytest.mark.parametrize("cluster", [0, 2, 4])
 def test_rank_write_cluster_windows(ctx, cluster):
     """The single-text rank write through 65536-position windows held by a
-    two-block cluster (one grouping pass for 22 position bits, none for 16)
-    or through 2048-position windows (two passes, one): the same
+    cluster of two or four blocks (one grouping pass for 22 position bits,
+    none for 16) or through 2048-position windows (two passes, one): the same
     (oracle-equal) build."""
     rng = np.random.default_rng(16)
     ctx.set_tuning("rank_cluster", cluster)
@@ -229,7 +229,7 @@ def test_rank_write_cluster_windows(ctx, cluster):
                   synth.random_text(rng, 65_536, 4)):                    # one full window
             check_full(ctx, t, isa_bits=32, lcp=sg.LcpEncoding.RAW32)
     finally:
-        ctx.set_tuning("rank_cluster", 1)
+        ctx.set_tuning("rank_cluster", 2)
 
 
 @pytest.mark.parametrize("fused", [0, 1])

@@ -123,3 +123,21 @@ def test_rank_by_counting_or_passes(ctx, small):
     finally:
         ctx.set_tuning("seg_small_group", 96)
         ctx.set_tuning("graph_rounds", 1)
+
+
+@pytest.mark.parametrize("blocks", [2, 3])
+def test_round_sort_register_caps(ctx, blocks):
+    """The round sort compiled for two or three blocks per SM (register cap):
+    the same oracle-equal build on repeat-rich text and tandem repeats."""
+    rng = np.random.default_rng(8)
+    texts = [synth.repeat_rich_100mbp(scale=0.01).logical_text(),
+             np.concatenate([np.tile(synth.random_text(rng, 9, 4)[:8], 2000),
+                             synth.random_text(rng, 30000, 4)])]
+    ctx.set_tuning("seg_blocks", blocks)
+    try:
+        for t in texts:
+            r = build(ctx, t)
+            sa, isa, lcp = expected(t)
+            assert (r.sa_low == sa).all() and (r.isa_low == isa).all() and (r.lcp == lcp).all()
+    finally:
+        ctx.set_tuning("seg_blocks", 3)
