@@ -339,8 +339,10 @@ __device__ __forceinline__ u32 window_lcp(const u8* text, u64 n, u64 p, u64 q, u
 // keys are exact and handled here; rows of t = 0 / t = 2 keys (rare rows) get
 // placeholder pairs and SA entries, no LCP (nor the row after them), and stay
 // off the active list: rare_place_kernel and rare_active_kernel finish them.
+// Registers capped for five blocks per SM (measured: 43.6 against 46.2 ms at
+// 3.1 Gbp; the round kernels lose at that cap).
 template <bool kTwoBit>
-static __global__ void __launch_bounds__(kScanBlock)
+static __global__ void __launch_bounds__(kScanBlock, 5)
 seed_rank_kernel(const u64* __restrict__ keys, u32* __restrict__ sa,
                  u64 n, Segments segs, u32 packed_shift, u32 bits, u32 symbols,
                  u64* __restrict__ pairs, u32* __restrict__ lcp,
