@@ -97,13 +97,22 @@ constexpr int kSeedRun = 16;
 constexpr int kSeedTile = kSeedBlock * kSeedRun;
 constexpr int kSeedHalo = 64;
 constexpr int kMaxSeedPasses = 8;  // 64-bit keys, 8-bit digits
+// Keys per thread when the kernel only counts (the fused first pass writes
+// the keys): no key buffer in shared memory, so each thread can slide its
+// window over four times as many positions, and the window it builds from
+// scratch at its first position (s symbols) is paid once per 64 keys.
+constexpr int kSeedCountRun = 64;
 
-struct SeedSmem {
-  u64 keys[kSeedTile];
+// kRun keys per thread; the key buffer exists for the position-order write
+// (kRun == kSeedRun) only.
+template <int kRun>
+struct SeedSmemT {
+  u64 keys[kRun == kSeedRun ? kSeedBlock * kRun : 1];
   u32 hist[8][256];
   u16 code[256];
-  __align__(16) u8 window[kSeedTile + kSeedHalo];
+  __align__(16) u8 window[kSeedBlock * kRun + kSeedHalo];
 };
+using SeedSmem = SeedSmemT<kSeedRun>;
 
 // Two-bit seed for texts of four consecutive regular symbols (A, C, G, T in
 // the logical text) and few others.  A window's key is the 2-bit codes of its
@@ -174,19 +183,21 @@ __host__ __device__ __forceinline__ u64 two_bit_of_exact(u64 exact, u32 s, u32 b
 // over bits [packed_shift, packed_shift + 8*passes).
 // kTwoBit: sort keys are two-bit keys (one instance); rare rows also append
 // (exact key, position) to tb's list.
-template <bool kTwoBit>
+// kRun = kSeedCountRun: histograms and rare list only (keys must be null).
+template <bool kTwoBit, int kRun = kSeedRun>
 static __global__ void __launch_bounds__(kSeedBlock)
 seed_keys_kernel(const u8* __restrict__ text, u64 n, Segments segs,
                  const u16* __restrict__ code_table, u32 bits, u32 symbols,
                  u32 passes, u32* __restrict__ hist_out, u32 packed_shift,
                  u64* __restrict__ keys, u32* __restrict__ vals, TwoBitSeed tb) {
+  constexpr int kTile = kSeedBlock * kRun;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  SeedSmem& sm = *reinterpret_cast<SeedSmem*>(smem_raw);
+  SeedSmemT<kRun>& sm = *reinterpret_cast<SeedSmemT<kRun>*>(smem_raw);
   sm.code[threadIdx.x] = code_table[threadIdx.x];
   for (int i = threadIdx.x; i < 8 * 256; i += kSeedBlock) (&sm.hist[0][0])[i] = 0;
-  const u64 tile_first = static_cast<u64>(blockIdx.x) * kSeedTile;
+  const u64 tile_first = static_cast<u64>(blockIdx.x) * kTile;
   // Stage tile + halo as 16-byte vectors (the text buffer is padded).
-  for (int i = threadIdx.x; i < (kSeedTile + kSeedHalo) / 16; i += kSeedBlock) {
+  for (int i = threadIdx.x; i < (kTile + kSeedHalo) / 16; i += kSeedBlock) {
     const u64 at = tile_first + static_cast<u64>(i) * 16;
     uint4 v = make_uint4(0, 0, 0, 0);
     if (at < n) v = *reinterpret_cast<const uint4*>(text + at);
@@ -197,7 +208,7 @@ seed_keys_kernel(const u8* __restrict__ text, u64 n, Segments segs,
   const u64 mask = symbols * bits >= 64 ? ~0ull : ((1ull << (symbols * bits)) - 1);
   const u64 mask2 = 2 * symbols >= 64 ? ~0ull : ((1ull << (2 * symbols)) - 1);
   const u32 smask = symbols >= 32 ? ~0u : ((1u << symbols) - 1);
-  const u32 local0 = threadIdx.x * kSeedRun;
+  const u32 local0 = threadIdx.x * kRun;
   u64 pos = tile_first + local0;
   u32 seg = segs.count == 1 ? 0 : (pos < n ? find_segment(segs.begin, segs.count, pos) : block_seg);
   u64 end = pos < n ? segs.begin[seg + 1] : n;
@@ -217,7 +228,8 @@ seed_keys_kernel(const u8* __restrict__ text, u64 n, Segments segs,
   u32 run_digit[kMaxSeedPasses], run_len[kMaxSeedPasses];
 #pragma unroll
   for (int p = 0; p < kMaxSeedPasses; ++p) run_digit[p] = run_len[p] = 0;
-  for (int r = 0; r < kSeedRun; ++r, ++pos) {
+#pragma unroll 1
+  for (int r = 0; r < kRun; ++r, ++pos) {
     const bool valid = pos < n;
     if (valid && pos >= end) {  // crossed into the next instance
       seg = find_segment(segs.begin, segs.count, pos);
@@ -243,7 +255,9 @@ seed_keys_kernel(const u8* __restrict__ text, u64 n, Segments segs,
         sort_key = two_bit_key(key, k2, irregular, symbols, bits, tb);
         rare = (sort_key & 1) == 0;
       }
-      sm.keys[local] = packed_shift ? (sort_key << packed_shift) | (pos - seg_lo) : sort_key;
+      if constexpr (kRun == kSeedRun) {
+        sm.keys[local] = packed_shift ? (sort_key << packed_shift) | (pos - seg_lo) : sort_key;
+      }
     }
     if (kTwoBit) {
       const u64 slot = warp_append(tb.rare_count, rare);
@@ -283,11 +297,13 @@ seed_keys_kernel(const u8* __restrict__ text, u64 n, Segments segs,
   __syncthreads();
   // keys == null: histograms (and the rare list) only; seed_sorted_kernel
   // generates the keys again and writes them partitioned by the first digit.
-  for (u32 i = threadIdx.x; keys && i < kSeedTile; i += kSeedBlock) {
-    const u64 at = tile_first + i;
-    if (at < n) {
-      keys[at] = sm.keys[i];
-      if (!packed_shift) vals[at] = static_cast<u32>(at);
+  if constexpr (kRun == kSeedRun) {
+    for (u32 i = threadIdx.x; keys && i < kTile; i += kSeedBlock) {
+      const u64 at = tile_first + i;
+      if (at < n) {
+        keys[at] = sm.keys[i];
+        if (!packed_shift) vals[at] = static_cast<u32>(at);
+      }
     }
   }
   for (u32 i = threadIdx.x; i < passes * 256; i += kSeedBlock) {
@@ -339,10 +355,11 @@ __device__ __forceinline__ u32 window_lcp(const u8* text, u64 n, u64 p, u64 q, u
 // keys are exact and handled here; rows of t = 0 / t = 2 keys (rare rows) get
 // placeholder pairs and SA entries, no LCP (nor the row after them), and stay
 // off the active list: rare_place_kernel and rare_active_kernel finish them.
-// Registers capped for five blocks per SM (measured: 43.6 against 46.2 ms at
-// 3.1 Gbp; the round kernels lose at that cap).
-template <bool kTwoBit>
-static __global__ void __launch_bounds__(kScanBlock, 5)
+// kMinBlocks: blocks per SM the registers are capped for (measured: five
+// for one text, 43.6 against 46.2 ms at 3.1 Gbp; four for batches, 16.8
+// against 19.2 ms for 256 bacterial references).
+template <bool kTwoBit, int kMinBlocks>
+static __global__ void __launch_bounds__(kScanBlock, kMinBlocks)
 seed_rank_kernel(const u64* __restrict__ keys, u32* __restrict__ sa,
                  u64 n, Segments segs, u32 packed_shift, u32 bits, u32 symbols,
                  u64* __restrict__ pairs, u32* __restrict__ lcp,

@@ -256,6 +256,9 @@ struct Tuning {
   // Round sort blocks per SM the kernel's registers are capped for (2 or 3;
   // measured at 3.1 Gbp: 33.3 ms at three against 37.5 ms at two).
   u32 seg_blocks = 3;
+  // Seed histograms with kSeedCountRun keys per thread when the fused first
+  // pass writes the keys (instead of kSeedRun).
+  bool seed_count_run = true;
   // Run the rounds as captured CUDA graphs of two rounds (needs seg_sort;
   // builds with the per-kernel profile on are driven round by round).
   bool graph_rounds = true;
@@ -320,6 +323,8 @@ std::string apply_tuning(Tuning& t, const std::string& k, int64_t value) {
   } else if (k == "rank_cluster") {
     if (value != 0 && value != 2 && value != 4) return "rank_cluster must be 0, 2 or 4";
     t.rank_cluster = static_cast<u32>(value);
+  } else if (k == "seed_count_run") {
+    t.seed_count_run = value != 0;
   } else if (k == "seg_blocks") {
     if (value != 2 && value != 3) return "seg_blocks must be 2 or 3";
     t.seg_blocks = static_cast<u32>(value);
@@ -983,6 +988,9 @@ struct Engine {
       // Seed keys and the segmented seed sort.
       seed_bits = sym_bits * symbols + tag;
       const bool fused = c.tune.seed_fused && c.tune.sort_tile == kSortTile;
+      // With the fused first pass this kernel only counts: long runs per thread.
+      const bool counts_only = fused && c.tune.seed_count_run;
+      const u64 count_blocks = (n + u64(kSeedBlock) * kSeedCountRun - 1) / (u64(kSeedBlock) * kSeedCountRun);
       const u32 seed_passes = (seed_bits + kRadixBits - 1) / kRadixBits;
       zero(L.hist, u64(segs) * seed_passes * kRadixDigits * 4);
       if (two_bit) {
@@ -994,13 +1002,25 @@ struct Engine {
         tb.rare_count = L.scalars + 44;
         tb.inst_shift = segs > 1 ? bits * symbols : 0;
         zero(L.scalars + 44, 8);
-        launch("seed_keys", fused ? n : (packed_shift ? n * 9 : n * 13), seed_keys_kernel<true>,
-               (n + kSeedTile - 1) / kSeedTile, kSeedBlock, sizeof(SeedSmem), L.text, n,
-               segments(), static_cast<const u16*>(L.code), bits, symbols, seed_passes, L.hist,
-               packed_shift, fused ? nullptr : L.k0, fused ? nullptr : L.v0, tb);
+        if (counts_only) {
+          launch("seed_keys", n, seed_keys_kernel<true, kSeedCountRun>, count_blocks, kSeedBlock,
+                 sizeof(SeedSmemT<kSeedCountRun>), L.text, n, segments(),
+                 static_cast<const u16*>(L.code), bits, symbols, seed_passes, L.hist, packed_shift,
+                 nullptr, nullptr, tb);
+        } else {
+          launch("seed_keys", fused ? n : (packed_shift ? n * 9 : n * 13), seed_keys_kernel<true>,
+                 (n + kSeedTile - 1) / kSeedTile, kSeedBlock, sizeof(SeedSmem), L.text, n,
+                 segments(), static_cast<const u16*>(L.code), bits, symbols, seed_passes, L.hist,
+                 packed_shift, fused ? nullptr : L.k0, fused ? nullptr : L.v0, tb);
+        }
         // Read back with the sort's pass check below (one synchronisation).
         SG_CUDA(cudaMemcpyAsync(c.host_scalars + 44, L.scalars + 44, 8, cudaMemcpyDeviceToHost,
                                 c.stream));
+      } else if (counts_only) {
+        launch("seed_keys", n, seed_keys_kernel<false, kSeedCountRun>, count_blocks, kSeedBlock,
+               sizeof(SeedSmemT<kSeedCountRun>), L.text, n, segments(),
+               static_cast<const u16*>(L.code), bits, symbols, seed_passes, L.hist, packed_shift,
+               nullptr, nullptr, TwoBitSeed{});
       } else {
         launch("seed_keys", fused ? n : (packed_shift ? n * 9 : n * 13),
                seed_keys_kernel<false>, (n + kSeedTile - 1) / kSeedTile, kSeedBlock,
@@ -1087,7 +1107,9 @@ struct Engine {
     u64* status_max = L.status;
     u64* status_sum = L.status + scan_tiles + 1;
     u64* pairs = keys == L.k0 ? L.k1 : L.k0;
-    launch("seed_rank", n * 24, two_bit ? seed_rank_kernel<true> : seed_rank_kernel<false>,
+    auto seed_rank_fn = segs > 1 ? (two_bit ? seed_rank_kernel<true, 4> : seed_rank_kernel<false, 4>)
+                                 : (two_bit ? seed_rank_kernel<true, 5> : seed_rank_kernel<false, 5>);
+    launch("seed_rank", n * 24, seed_rank_fn,
            scan_tiles, kScanBlock, 0, static_cast<const u64*>(keys), sa, n, segments(),
            packed_shift, bits, symbols, pairs, L.lcp, L.x, status_max, status_sum, L.counters,
            L.scalars + 0, L.flags, runs_on ? 1u : 0u, segs > 1 ? 1u : 0u);

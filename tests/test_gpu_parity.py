@@ -262,3 +262,26 @@ def test_onesweep_bulk_tile_load(ctx, tma):
         check_full(ctx, synth.random_text(np.random.default_rng(3), 9_999, 2))
     finally:
         ctx.set_tuning("tma_tile", 0)
+
+
+@pytest.mark.parametrize("long_run", [0, 1])
+def test_seed_histograms_short_or_long_runs(ctx, long_run):
+    """Seed digit histograms counted with 16 or 64 keys per thread (the
+    counting kernel of the fused first pass): the same (oracle-equal) build
+    for two-bit and code-table seeds, packed or not, and for a batch whose
+    tiles cross instance boundaries."""
+    rng = np.random.default_rng(64)
+    ctx.set_tuning("seed_count_run", long_run)
+    try:
+        for t in (synth.repeat_rich_100mbp(scale=0.02).logical_text(),
+                  synth.human_scale_3gbp(scale=0.002).logical_text(),
+                  synth.plain_4mbp(scale=0.5).logical_text(),
+                  synth.random_text(rng, 70_000, 20)):
+            check_full(ctx, t, isa_bits=32, lcp=sg.LcpEncoding.RAW32)
+        texts = [synth.random_text(rng, int(m), 4) for m in rng.integers(1, 30_000, size=12)]
+        rs = ctx.build_batch(texts, sa_bits=32, isa_bits=0, lcp=sg.LcpEncoding.RAW32)
+        for t, r in zip(texts, rs):
+            sa, _, lcp = expected(t)
+            assert (r.sa == sa).all() and (r.lcp.astype(np.uint64) == lcp).all()
+    finally:
+        ctx.set_tuning("seed_count_run", 1)
