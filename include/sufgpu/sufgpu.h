@@ -272,7 +272,28 @@ SUFGPU_API sufgpu_status sufgpu_profile_entry(const sufgpu_ctx *ctx, uint32_t in
  *                   G, T) and few others sorts 2-bit seed keys, the windows
  *                   that hold another symbol placed exactly from a side
  *                   list; 0 = keys of the text's own code width always;
- *   "two_bit_min"   smallest text (symbols) that uses the two-bit seed.
+ *   "two_bit_min"   smallest text (symbols) that uses the two-bit seed;
+ *   "two_bit_batch" 1 = batches use two-bit seeds too (per-instance side
+ *                   lists);
+ *   "seed_fused"    1 = the first seed pass generates its keys from the text
+ *                   (no key write in position order);
+ *   "seed_count_run" 1 = the histogram pass before a fused first pass counts
+ *                   64 keys per thread, 0 = 16;
+ *   "keys_sort_block" onesweep threads per 4096-key tile of keys-only sorts:
+ *                   256 or 512;
+ *   "rank_slots"    seed rank write by window slots: 0 never, 1 batches
+ *                   only, 2 always (else by grouping passes);
+ *   "rank_cluster"  0, 2 or 4: blocks per cluster that hold a 65536-position
+ *                   window of a single text's rank write (0 = 2048-position
+ *                   windows in one block);
+ *   "seg_small_group" round tiles whose groups have at most this many rows
+ *                   rank by counting (0 = always radix passes);
+ *   "seg_blocks"    round sort compiled for 2 or 3 blocks per SM;
+ *   "seg_rank"      1 = the round sort also writes SA rows, ranks and the
+ *                   next active list (no round_rank pass);
+ *   "graph_shrink"  the graph rounds switch to a smaller bound once the
+ *                   active rows fall below bound / graph_shrink;
+ *   "tma_tile"      1 = single-segment onesweep tiles arrive by one bulk copy.
  * Results are identical for every setting; only speed changes. */
 SUFGPU_API sufgpu_status sufgpu_set_tuning(sufgpu_ctx *ctx, const char *key, int64_t value);
 
