@@ -286,6 +286,9 @@ SUFGPU_API sufgpu_status sufgpu_profile_entry(const sufgpu_ctx *ctx, uint32_t in
  *   "rank_cluster"  0, 2 or 4: blocks per cluster that hold a 65536-position
  *                   window of a single text's rank write (0 = 2048-position
  *                   windows in one block);
+ *   "batch_cluster" 1 = batches write ranks through 65536-position windows
+ *                   per instance held by two-block clusters, 0 = by window
+ *                   slots or 2048-position windows;
  *   "seg_small_group" round tiles whose groups have at most this many rows
  *                   rank by counting (0 = always radix passes);
  *   "seg_blocks"    round sort compiled for 2 or 3 blocks per SM;

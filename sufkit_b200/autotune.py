@@ -43,12 +43,13 @@ CANDIDATES = {
     "rank_cluster": [2, 0, 4],
     "seg_blocks": [3, 2],
     "seed_count_run": [1, 0],
+    "batch_cluster": [1, 0],
 }
 DEFAULTS = {"seed_symbols": 0, "sort_tile": 4096, "sort_block": 256,
             "ballot_min_elems": 1 << 23, "packed_max_bits": 24, "two_bit_seed": 1,
             "rank_slots": 1, "graph_shrink": 4, "keys_sort_block": 256, "seg_rank": 0,
             "rank_cluster": 2, "seg_blocks": 3,
-            "seed_count_run": 1}
+            "seed_count_run": 1, "batch_cluster": 1}
 
 
 def workloads(quick: bool):

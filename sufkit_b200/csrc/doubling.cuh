@@ -355,11 +355,10 @@ __device__ __forceinline__ u32 window_lcp(const u8* text, u64 n, u64 p, u64 q, u
 // keys are exact and handled here; rows of t = 0 / t = 2 keys (rare rows) get
 // placeholder pairs and SA entries, no LCP (nor the row after them), and stay
 // off the active list: rare_place_kernel and rare_active_kernel finish them.
-// kMinBlocks: blocks per SM the registers are capped for (measured: five
-// for one text, 43.6 against 46.2 ms at 3.1 Gbp; four for batches, 16.8
-// against 19.2 ms for 256 bacterial references).
-template <bool kTwoBit, int kMinBlocks>
-static __global__ void __launch_bounds__(kScanBlock, kMinBlocks)
+// Registers capped for five blocks per SM (measured: 43.6 against 46.2 ms at
+// 3.1 Gbp; 19.1 against 19.9 ms for 256 bacterial references).
+template <bool kTwoBit>
+static __global__ void __launch_bounds__(kScanBlock, 5)
 seed_rank_kernel(const u64* __restrict__ keys, u32* __restrict__ sa,
                  u64 n, Segments segs, u32 packed_shift, u32 bits, u32 symbols,
                  u64* __restrict__ pairs, u32* __restrict__ lcp,
@@ -698,6 +697,53 @@ cluster4_window_scatter_kernel(const u64* __restrict__ pairs, u64 n, u32* __rest
                                DeviceFlags* flags) {
   extern __shared__ u32 slice[];
   cluster_window_scatter<4>(pairs, n, rank, flags, slice);
+}
+
+// The same per instance of a batch: pairs carry instance-local positions
+// and are grouped by 2^16-position window inside each instance's rows, so
+// instance j's window w is rows begin[j] + [w << 16, min((w + 1) << 16, n_j)).
+// wbegin[j] = windows of the instances before j (count + 1 entries).  Both
+// blocks of a cluster serve the same window.
+static __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(1024, 1)
+cluster_segment_window_scatter_kernel(const u64* __restrict__ pairs, Segments segs,
+                                      const u64* __restrict__ wbegin, u32* __restrict__ rank,
+                                      DeviceFlags* flags) {
+  using W = ClusterWindow<2>;
+  extern __shared__ u32 slice[];
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  const u32 me = cluster.block_rank();
+  const u64 window = blockIdx.x >> 1;
+  u32 lo_j = 0, hi_j = segs.count;  // instance j with wbegin[j] <= window < wbegin[j + 1]
+  while (hi_j - lo_j > 1) {
+    const u32 mid = (lo_j + hi_j) >> 1;
+    if (wbegin[mid] <= window) lo_j = mid;
+    else hi_j = mid;
+  }
+  const u64 w = window - wbegin[lo_j];
+  const u64 base = segs.begin[lo_j];
+  const u64 len = segs.begin[lo_j + 1] - base;
+  const u64 first = w << kClusterWindowBits;
+  const u64 count = first >= len ? 0
+                    : (len - first < (1ull << kClusterWindowBits) ? len - first
+                                                                  : (1ull << kClusterWindowBits));
+  if (count == 0 && threadIdx.x == 0 && me == 0) flag_error(flags, kErrBounds);
+  cluster.sync();  // every block's shared memory is live before remote stores
+  const u64 lo = static_cast<u64>(me) * W::kSlice;
+  const u64 hi = lo + W::kSlice < count ? lo + W::kSlice : count;
+  for (u64 i = lo + threadIdx.x; i < hi; i += W::kBlock) {
+    const u64 v = pairs[base + first + i];
+    const u64 pos = v >> 32;
+    const u64 local = pos - first;
+    if ((pos >> kClusterWindowBits) != w || local >= count) {
+      flag_error(flags, kErrBounds);  // not a permutation of the instance
+      continue;
+    }
+    u32* const owner = cluster.map_shared_rank(slice, static_cast<u32>(local >> W::kSliceBits));
+    owner[local & (W::kSlice - 1)] = static_cast<u32>(v);
+  }
+  cluster.sync();
+  for (u64 i = lo + threadIdx.x; i < hi; i += W::kBlock) rank[base + first + i] = slice[i - lo];
 }
 
 // Rank write by window slots (one instance).  Each (position << 32 | head)

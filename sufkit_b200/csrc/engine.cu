@@ -259,6 +259,9 @@ struct Tuning {
   // Seed histograms with kSeedCountRun keys per thread when the fused first
   // pass writes the keys (instead of kSeedRun).
   bool seed_count_run = true;
+  // Batches write ranks through 2^16-position windows per instance held by
+  // clusters of two blocks (one grouping pass) instead of window slots.
+  bool batch_cluster = true;
   // Run the rounds as captured CUDA graphs of two rounds (needs seg_sort;
   // builds with the per-kernel profile on are driven round by round).
   bool graph_rounds = true;
@@ -323,6 +326,8 @@ std::string apply_tuning(Tuning& t, const std::string& k, int64_t value) {
   } else if (k == "rank_cluster") {
     if (value != 0 && value != 2 && value != 4) return "rank_cluster must be 0, 2 or 4";
     t.rank_cluster = static_cast<u32>(value);
+  } else if (k == "batch_cluster") {
+    t.batch_cluster = value != 0;
   } else if (k == "seed_count_run") {
     t.seed_count_run = value != 0;
   } else if (k == "seg_blocks") {
@@ -642,18 +647,23 @@ struct Engine {
   // digit of position bits [b, b + 8), each period of 2^(b+8) positions gives
   // every digit 2^b of them, and the remainder fills digits from 0 upwards.
   // Written to L.hist for one segment, so the sort needs no histogram pass.
-  void upload_permutation_hist(u64 count, u32 begin_bit, u32 end_bit) {
+  // counts: one entry per segment (a batch: each instance's local positions
+  // are a permutation of [0, its length)); layout [segment][pass][digit].
+  void upload_permutation_hist(const std::vector<u64>& counts, u32 begin_bit, u32 end_bit) {
     const u32 passes = (end_bit - begin_bit + kRadixBits - 1) / kRadixBits;
-    std::vector<u32> h(u64(passes) * kRadixDigits);
-    for (u32 p = 0; p < passes; ++p) {
-      const u32 b = begin_bit + p * kRadixBits - 32;
-      const u64 width = u64(1) << b;
-      const u64 period = width << kRadixBits;
-      const u64 full = count / period, rem = count % period;
-      for (u32 d = 0; d < kRadixDigits; ++d) {
-        const u64 lo = u64(d) * width;
-        const u64 extra = rem > lo ? std::min<u64>(width, rem - lo) : 0;
-        h[u64(p) * kRadixDigits + d] = static_cast<u32>(full * width + extra);
+    std::vector<u32> h(counts.size() * passes * kRadixDigits);
+    for (size_t j = 0; j < counts.size(); ++j) {
+      const u64 count = counts[j];
+      for (u32 p = 0; p < passes; ++p) {
+        const u32 b = begin_bit + p * kRadixBits - 32;
+        const u64 width = u64(1) << b;
+        const u64 period = width << kRadixBits;
+        const u64 full = count / period, rem = count % period;
+        for (u32 d = 0; d < kRadixDigits; ++d) {
+          const u64 lo = u64(d) * width;
+          const u64 extra = rem > lo ? std::min<u64>(width, rem - lo) : 0;
+          h[(j * passes + p) * kRadixDigits + d] = static_cast<u32>(full * width + extra);
+        }
       }
     }
     upload(L.hist, h.data(), h.size() * 4);
@@ -1107,9 +1117,7 @@ struct Engine {
     u64* status_max = L.status;
     u64* status_sum = L.status + scan_tiles + 1;
     u64* pairs = keys == L.k0 ? L.k1 : L.k0;
-    auto seed_rank_fn = segs > 1 ? (two_bit ? seed_rank_kernel<true, 4> : seed_rank_kernel<false, 4>)
-                                 : (two_bit ? seed_rank_kernel<true, 5> : seed_rank_kernel<false, 5>);
-    launch("seed_rank", n * 24, seed_rank_fn,
+    launch("seed_rank", n * 24, two_bit ? seed_rank_kernel<true> : seed_rank_kernel<false>,
            scan_tiles, kScanBlock, 0, static_cast<const u64*>(keys), sa, n, segments(),
            packed_shift, bits, symbols, pairs, L.lcp, L.x, status_max, status_sum, L.counters,
            L.scalars + 0, L.flags, runs_on ? 1u : 0u, segs > 1 ? 1u : 0u);
@@ -1140,7 +1148,39 @@ struct Engine {
     const bool cluster_window = segs == 1 && c.tune.rank_cluster && c.tune.rank_slots != 2 &&
                                 group_passes(kClusterWindowBits) < group_passes(kWindowBits);
     const u32 window_bits = cluster_window ? kClusterWindowBits : kWindowBits;
-    if (segs > 1 && c.tune.rank_slots >= 1) {
+    // A batch by 2^16-position windows per instance (clusters of two blocks)
+    // when that saves a grouping pass over 2048-position windows.
+    u64 batch_longest = 1;
+    for (u32 j = 0; j < segs; ++j) batch_longest = std::max<u64>(batch_longest, begin[j + 1] - begin[j]);
+    const u32 batch_bits = std::max<u32>(1, bits_for(batch_longest - 1));
+    auto batch_passes = [&](u32 w) { return batch_bits > w ? (batch_bits - w + 7) / 8 : 0u; };
+    const bool batch_cluster = segs > 1 && c.tune.batch_cluster && c.tune.rank_cluster &&
+                               batch_passes(kClusterWindowBits) < batch_passes(kWindowBits);
+    if (batch_cluster) {
+      std::vector<u64> wbegin(segs + 1, 0);
+      for (u32 j = 0; j < segs; ++j) {
+        const u64 len = begin[j + 1] - begin[j];
+        wbegin[j + 1] = wbegin[j] + ((len + (u64(1) << kClusterWindowBits) - 1) >> kClusterWindowBits);
+      }
+      if (batch_bits > kClusterWindowBits) {
+        u64* other_keys = pairs == L.k0 ? L.k1 : L.k0;
+        std::vector<u64> lens(segs);
+        for (u32 j = 0; j < segs; ++j) lens[j] = begin[j + 1] - begin[j];
+        upload_permutation_hist(lens, 32 + kClusterWindowBits, 32 + batch_bits);
+        const bool sw = radix_sort("rank_group", pairs, nullptr, other_keys, nullptr, L.seg_begin,
+                                   L.seg_tiles, segs, seed_tiles, n, 32 + kClusterWindowBits,
+                                   32 + batch_bits, false, true);
+        grouped = sw ? other_keys : pairs;
+      }
+      sync();
+      std::memcpy(c.host_small, wbegin.data(), (segs + 1) * 8);
+      SG_CUDA(cudaMemcpyAsync(L.digit_start, c.host_small, (segs + 1) * 8, cudaMemcpyHostToDevice,
+                              c.stream));
+      launch("window_scatter", n * 12, cluster_segment_window_scatter_kernel, wbegin[segs] * 2,
+             ClusterWindow<2>::kBlock, ClusterWindow<2>::kSlice * 4,
+             static_cast<const u64*>(grouped), segments(), static_cast<const u64*>(L.digit_start),
+             L.rank, L.flags);
+    } else if (segs > 1 && c.tune.rank_slots >= 1) {
       // Window slots per instance (rank_slot_segments_kernel): no grouping passes.
       std::vector<u64> wbegin(segs + 1, 0);
       for (u32 j = 0; j < segs; ++j) {
@@ -1202,7 +1242,7 @@ struct Engine {
       SG_CUDA(cudaMemcpyAsync(L.sort_begin, c.host_small + 4096, 16, cudaMemcpyHostToDevice, c.stream));
       SG_CUDA(cudaMemcpyAsync(L.sort_tiles, c.host_small + 4096 + 16, 8, cudaMemcpyHostToDevice, c.stream));
       u64* other_keys = pairs == L.k0 ? L.k1 : L.k0;
-      upload_permutation_hist(n, 32 + window_bits, 32 + pos_bits);
+      upload_permutation_hist({n}, 32 + window_bits, 32 + pos_bits);
       const bool sw = radix_sort("rank_group", pairs, nullptr, other_keys, nullptr, L.sort_begin,
                                  L.sort_tiles, 1, t, n, 32 + window_bits, 32 + pos_bits, false,
                                  true);
@@ -2118,6 +2158,9 @@ sufgpu_status sufgpu_create(sufgpu_ctx** out, int device) {
     SG_CUDA(cudaFuncSetAttribute(seg_rank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(sizeof(SegRankSmem))));
     SG_CUDA(cudaFuncSetAttribute(cluster_window_scatter_kernel,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(ClusterWindow<2>::kSlice * 4)));
+    SG_CUDA(cudaFuncSetAttribute(cluster_segment_window_scatter_kernel,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(ClusterWindow<2>::kSlice * 4)));
     SG_CUDA(cudaFuncSetAttribute(cluster4_window_scatter_kernel,

@@ -81,3 +81,23 @@ def test_batch_rank_write_by_slots_or_passes(ctx, slots):
             assert_oracle(b, t, sg.LcpEncoding.RAW32)
     finally:
         ctx.set_tuning("rank_slots", 1)
+
+
+@pytest.mark.parametrize("cluster", [0, 1])
+def test_batch_rank_write_cluster_windows(ctx, cluster):
+    """A batch's rank write through 65536-position windows per instance held
+    by two-block clusters (no grouping pass for instances of at most 2^16
+    symbols, one for 2^20 and more), or through window slots: every instance
+    equals the oracle."""
+    rng = np.random.default_rng(65)
+    small = [synth.random_text(rng, int(m), 4) for m in rng.integers(3000, 65_536, size=10)]
+    large = [synth.random_text(rng, int(m), 4) for m in rng.integers(600_000, 1_100_000, size=3)]
+    ctx.set_tuning("batch_cluster", cluster)
+    try:
+        for texts in (small, large + small[:3]):
+            batch = ctx.build_batch(texts, sa_bits=32, isa_bits=32, lcp=sg.LcpEncoding.RAW32,
+                                    validate=True)
+            for t, b in zip(texts, batch):
+                assert_oracle(b, t, sg.LcpEncoding.RAW32)
+    finally:
+        ctx.set_tuning("batch_cluster", 1)
