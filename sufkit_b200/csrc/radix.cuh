@@ -117,7 +117,7 @@ radix_offsets_kernel(const u32* __restrict__ hist, const u64* __restrict__ begin
 // handled by kBlock threads x kItems items.  Shared memory holds the tile's
 // keys and values (kVals) in sorted-slot order and per-warp digit counters.
 // The counters are 16-bit (a warp ranks at most 32 x kItems <= 512 keys, and
-// a tile-local slot is below 4096), which keeps a 4096-pair tile at 56 KB: three
+// a tile-local slot is below 4096), which keeps a 4096-pair tile at 56 KB: four
 // blocks per SM instead of two.
 template <int kBlock, int kTile = kSortTile, bool kVals = true>
 struct OnesweepSmem {
@@ -172,13 +172,15 @@ __device__ __forceinline__ bool mbar_wait0(u64* mbar) {
 
 // kVals = false sorts keys only (vals_in/vals_out unused): the packed seed
 // carries each suffix's instance-local index in the low key bits.
-// Blocks per SM: three 256x16, four 256x8, two 512x8 (three without values).
+// Blocks per SM: four 256x16 (a 56 KB pair tile: four fit the SM's shared
+// memory; 64 registers, measured faster than three blocks at 80 despite a
+// few spilled words), four 256x8, two 512x8 (three without values).
 // Registers are capped so that occupancy, not the allocator, decides.
 // kTma: the tile's keys arrive by one bulk copy into shared memory (single-
 // segment sorts, whose tiles start on 4096-key boundaries) instead of
 // per-thread loads; the rest is the same.
 template <bool kBallot, int kBlock, int kItems, bool kVals = true, bool kTma = false>
-static __global__ void __launch_bounds__(kBlock, kBlock == 512 ? (kVals ? 2 : 3) : (kItems <= 8 ? 4 : 3))
+static __global__ void __launch_bounds__(kBlock, kBlock == 512 ? (kVals ? 2 : 3) : 4)
 radix_onesweep_kernel(const u64* __restrict__ keys_in,
                       const u32* __restrict__ vals_in,
                       u64* __restrict__ keys_out, u32* __restrict__ vals_out,
